@@ -1,0 +1,194 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Run here (where the reference tree and its CPU build exist), never on a GPU
+box:
+
+    make -C oracle/ref_build REF=/root/reference
+    python tests/golden/make_golden.py --ref /root/reference
+
+Sources of truth:
+  * ranlx_kat.npz      -- Luscher's published ranlxs/ranlxd sequences, parsed
+                          from the reference's own test (tests/ranlx/main.C).
+  * ludcmp_kat.json    -- the reference's 10x10 Hilbert LU test
+                          (tests/ludcmp_test/main.C) as printed by its binary.
+  * everything else    -- outputs of the reference's CPU path compiled from
+                          its unchanged sources (oracle/_ref/nrcps_ref, see
+                          oracle/ref_build/ref_driver.cc).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "nrcps_ref")
+
+
+def run_ref(*args: str) -> str:
+    out = subprocess.run([REF_BIN, *args], check=True, capture_output=True, text=True)
+    return out.stdout
+
+
+def parse_ranlx_kat(ref: str) -> dict:
+    src = open(os.path.join(ref, "tests", "ranlx", "main.C")).read()
+    xs = {int(k): float(v) for k, v in re.findall(r"xsn\[(\d+)\]=([0-9.]+)f;", src)}
+    xd = {int(k): float(v) for k, v in re.findall(r"xdn\[(\d+)\]=([0-9.]+);", src)}
+    assert sorted(xs) == list(range(96)) and sorted(xd) == list(range(48))
+    return {
+        # ranlxs lux 0 seed 32767: 20 blocks of 204 draws, compare xs[k+60]
+        # of the last block -> 0-based stream outputs 19*204+60 .. +155.
+        "ranlxs0_seed32767_first_index": np.int64(19 * 204 + 60),
+        "ranlxs0_seed32767_times_2p24": np.array([xs[k] for k in range(96)]),
+        # ranlxd lux 1 seed 32767: 20 blocks of 99 draws, compare xd[k+39].
+        "ranlxd1_seed32767_first_index": np.int64(19 * 99 + 39),
+        "ranlxd1_seed32767_times_2p48": np.array([xd[k] for k in range(48)]),
+    }
+
+
+def parse_ludcmp_kat(ref: str) -> dict:
+    out = subprocess.run([os.path.join(REPO, "oracle", "_ref", "kat_ludcmp")], check=True,
+                         capture_output=True, text=True).stdout
+    det = re.search(r"^det = \(([-0-9.e+]+), ([-0-9.e+]+)\)", out, re.M)
+    ldet = re.search(r"^log\(det\) = \(([-0-9.e+]+), ([-0-9.e+]+)\)", out, re.M)
+    src = open(os.path.join(ref, "tests", "ludcmp_test", "main.C")).read()
+    mdet = re.search(r"det = ([0-9.]+) \* 10\^(-?\d+) \(Mathematica", src)
+    mldet = re.search(r"ldet = (-?[0-9.]+) \(Mathematica", src)
+    return {
+        "n": 10,
+        "reference_det_printed": [float(det.group(1)), float(det.group(2))],
+        "reference_logdet_printed": [float(ldet.group(1)), float(ldet.group(2))],
+        "mathematica_det": float(mdet.group(1)) * 10.0 ** int(mdet.group(2)),
+        "mathematica_logdet": float(mldet.group(1)),
+    }
+
+
+def rng_streams(tmp: str) -> dict:
+    out = {}
+    for kind in ["RANLXS0", "RANLXS1", "RANLXS2", "RANLXD1", "RANLXD2", "RAN2"]:
+        for skip, count in [(0, 600), (200_000, 200)]:
+            fn = os.path.join(tmp, f"{kind}_{skip}.bin")
+            run_ref("rng", f"rng={kind}", "seed=1234", f"skip={skip}", f"count={count}", f"out={fn}")
+            out[f"{kind}_seed1234_skip{skip}"] = np.fromfile(fn)
+    fn = os.path.join(tmp, "gauss.bin")
+    run_ref("gauss", "rng=RANLXS2", "seed=99", "skip=0", "count=400", f"out={fn}")
+    out["gauss_RANLXS2_seed99"] = np.fromfile(fn)
+    return out
+
+
+def fields(tmp: str) -> dict:
+    out = {}
+    cases = [("ZTWO", "RANLXS2", 1234, 4, 3), ("ZTWO", "RANLXD1", 7, 6, 2), ("GAUSS", "RANLXS2", 99, 4, 2),
+             ("COMPLEXGAUSS", "RANLXS1", 5, 4, 1), ("ZTHREE", "RANLXS0", 11, 4, 2), ("ZTWO", "RAN2", 3, 4, 2)]
+    for field, kind, seed, L, slices in cases:
+        fn = os.path.join(tmp, "f.bin")
+        run_ref("field", f"field={field}", f"rng={kind}", f"seed={seed}", f"L={L}", f"slices={slices}",
+                f"out={fn}")
+        out[f"{field}_{kind}_seed{seed}_L{L}"] = np.fromfile(fn).reshape(slices, L ** 3, 2)
+    return out
+
+
+def ensemble(tmp: str, name: str, **kv) -> dict:
+    d = os.path.join(tmp, name)
+    os.makedirs(d, exist_ok=True)
+    args = [f"{k}={v}" for k, v in kv.items()] + [f"out={d}"]
+    info = json.loads(run_ref("ensemble", *args).strip().splitlines()[-1])
+    L, T = int(kv["L"]), int(kv["T"])
+    N = info["N"]
+    nmeas = 2 * N if kv.get("mode") == "slater2" else N
+    res = {
+        "dets": np.fromfile(os.path.join(d, "dets.bin"), dtype=np.complex128).reshape(-1, T, nmeas),
+        "sources": np.fromfile(os.path.join(d, "sources.bin"), dtype=np.complex128).reshape(N, L ** 3),
+        "args": json.dumps(kv),
+    }
+    if os.path.exists(os.path.join(d, "momenta.txt")):
+        res["momenta"] = np.loadtxt(os.path.join(d, "momenta.txt"), dtype=np.int64).reshape(-1, 4)
+    if os.path.exists(os.path.join(d, "props.bin")):
+        res["props"] = np.fromfile(os.path.join(d, "props.bin"), dtype=np.complex128).reshape(-1, N, L ** 3)
+    if os.path.exists(os.path.join(d, "fields.bin")):
+        res["fields"] = np.fromfile(os.path.join(d, "fields.bin")).reshape(-1, L ** 3, 2)
+    return res
+
+
+def lu_cases(tmp: str) -> dict:
+    rs = np.random.default_rng(20251203)
+    mats, dets = [], []
+    for n in range(1, 13):
+        for _ in range(2):
+            m = rs.standard_normal((n, n)) + 1j * rs.standard_normal((n, n))
+            if _ == 1 and n > 2:
+                m[1] = m[0] * (1 + 1e-9)  # nearly singular: pivoting matters
+            fn = os.path.join(tmp, "m.bin")
+            with open(fn, "wb") as f:
+                np.array([1, n], dtype=np.int32).tofile(f)
+                m.astype(np.complex128).tofile(f)
+            run_ref("lu", f"in={fn}", f"out={fn}.det")
+            dets.append(np.fromfile(fn + ".det", dtype=np.complex128)[0])
+            mats.append(m)
+    out = {f"m{i}": m for i, m in enumerate(mats)}
+    out["dets"] = np.array(dets)
+    return out
+
+
+def sho_coefficients(ref: str) -> dict:
+    d = os.path.join(ref, "production", "slater_det2_trapped", "sources")
+    out = {}
+    for n in range(10):
+        lines = []
+        for line in open(os.path.join(d, f"source.{n}")):
+            p = line.split()
+            if len(p) == 5:
+                lines.append([int(p[0]), int(p[1]), int(p[2]), float(p[3]), float(p[4])])
+        out[str(n)] = lines
+    return out
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    a = ap.parse_args()
+    if not os.path.exists(REF_BIN):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "oracle", "ref_build"), f"REF={a.ref}"])
+    np.savez_compressed(os.path.join(HERE, "ranlx_kat.npz"), **parse_ranlx_kat(a.ref))
+    json.dump(parse_ludcmp_kat(a.ref), open(os.path.join(HERE, "ludcmp_kat.json"), "w"), indent=1)
+    sho = sho_coefficients(a.ref)
+    json.dump(sho, open(os.path.join(HERE, "sho_coefficients.json"), "w"))
+    with tempfile.TemporaryDirectory() as tmp:
+        np.savez_compressed(os.path.join(HERE, "rng_streams.npz"), **rng_streams(tmp))
+        np.savez_compressed(os.path.join(HERE, "fields.npz"), **fields(tmp))
+        np.savez_compressed(os.path.join(HERE, "lu_cases.npz"), **lu_cases(tmp))
+        # config 1 of the benchmark: L=16, T=32, N=7 (E_F=0.1), Z2 a=0.5, seed 1234
+        np.savez_compressed(os.path.join(HERE, "ensemble_config1.npz"), **ensemble(
+            tmp, "c1", L=16, T=32, ef=0.1, seed=1234, rng="RANLXS2", field="ZTWO",
+            couplings="0.019894367886486918", cutoff=2.0, configs=2, dump_fields=3))
+        # small lattice, p-dependent interaction (3 couplings), ranlxd, props dumped
+        np.savez_compressed(os.path.join(HERE, "ensemble_multicoupling.npz"), **ensemble(
+            tmp, "mc", L=8, T=8, ef=0.35, seed=5, rng="RANLXD1", field="ZTWO",
+            couplings="0.02,0.004,0.001", cutoff=0.99999, configs=2, dump_props=4))
+        # Gaussian field, a=0.3
+        np.savez_compressed(os.path.join(HERE, "ensemble_gauss.npz"), **ensemble(
+            tmp, "g", L=8, T=8, ef=0.35, seed=99, rng="RANLXS2", field="GAUSS",
+            couplings=repr(0.09 / (4 * np.pi)), cutoff=2.0, configs=2))
+        # trapped, SHO sources, pair sink (production/slater_det2_trapped shape)
+        shodir = os.path.join(tmp, "sho")
+        os.makedirs(shodir)
+        for n, lines in sho.items():
+            with open(os.path.join(shodir, f"source.{n}"), "w") as f:
+                for l in lines:
+                    f.write(f"{l[0]} {l[1]} {l[2]} {l[3]!r} {l[4]!r}\n")
+        np.savez_compressed(os.path.join(HERE, "ensemble_trapped.npz"), **ensemble(
+            tmp, "tr", L=8, T=6, sources="sho", N=4, sho_dir=shodir, lambda1=2.0, lambda2=2.0,
+            lambda3=2.0, mode="slater2", potential=1, kappa=0.005, ptype="EXP", wavefunc="TGND",
+            tb_disp="STANDARD", tb_lambda=0.176776695, seed=31, rng="RANLXS2", field="ZTWO",
+            couplings="0.019894367886486918", cutoff=0.99999, configs=2, dump_props=3))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,323 @@
+"""Benchmark: batched auxiliary-field transfer-matrix ensemble on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (the batched precision form): L=32^3 periodic lattice, T=64 time
+slices, N=19 plane-wave orbitals (E_F = 0.045, closed shells |n|^2 <= 2),
+Z2 fields with a = 0.5 (C0 = 0.25/(4 pi)) drawn on the device from RANLXS2
+seed 7 (+491*rank), 4096 configurations per step, complex FP32 propagation,
+FP64 LU of every leading minor.  One step = one pass of the production loop
+over the 4096 configurations: field draw, 64 x (measure all N minors + one
+transfer-matrix step), and the reference's per-block sum of |det|^2 over
+configurations (and over ranks, as Comms::GlobalSum does).
+
+Metric: config*slices/s (whole job).  Inputs: none but seeds and the source
+list, so the orbitals (20 GB) and fields (1 GB) are generated on the device
+and exceed L2 (126 MB) every step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "L=32³ N=19+19 config·slices/s vs plain FP64; stat. error per GPU-second"
+UNIT = "config·slices/s"
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "nrcps_ref")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--L", type=int, default=32)
+    ap.add_argument("--T", type=int, default=64)
+    ap.add_argument("--ef", type=float, default=0.045)
+    ap.add_argument("--configs", type=int, default=4096)
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--cpu-sample-slices", type=int, default=32, help="slices per host process for cpu_baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(a, n_orb):
+    return {"workload": f"batched ensemble L={a.L}^3 T={a.T} N={n_orb} Z2 a=0.5 RANLXS2 seed {a.seed}, "
+                        f"{a.configs} configs/step, {a.precision} propagation + FP64 LU",
+            "L": a.L, "T": a.T, "N": n_orb, "configs_per_step": a.configs, "field": "ZTWO", "rng": "RANLXS2",
+            "seed": a.seed, "precision": a.precision, "sources": "plane waves (Fermi sea E_F=%g)" % a.ef,
+            "l2": "inputs larger than L2 (orbitals %.1f GB)" % (a.configs * n_orb * a.L ** 3 * (8 if a.precision == "f32" else 16) / 1e9)}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 8 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 8 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) > 8 for i in range(4) if s[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------ cpu baseline
+def cpu_baseline(a, slices_per_proc: int, n_orb: int):
+    """The reference's CPU path (oracle/_ref, built from its own sources) on
+    every host core: one single-threaded process per core, seeds seed+491*r
+    as the reference's MPI ranks (src/random/random.C:88)."""
+    cores = os.cpu_count() or 1
+    if os.path.exists(REF_BIN):
+        procs = [subprocess.Popen([REF_BIN, "bench", f"L={a.L}", f"T={a.T}", f"ef={a.ef}", f"seed={a.seed + 491 * r}",
+                                   "rng=RANLXS2", "field=ZTWO", f"max_slices={slices_per_proc}", "cutoff=2.0"],
+                                  stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True) for r in range(cores)]
+        rates = []
+        for p in procs:
+            out, _ = p.communicate()
+            rates.append(json.loads(out.strip().splitlines()[-1])["config_slices_per_s"])
+        return {"value": sum(rates), "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"{slices_per_proc} slices of one L={a.L}^3 N={n_orb} configuration per process, "
+                          f"{cores} processes (reference CPU FP64 path, FFTW replaced by the oracle's FFT)"}
+    # fall back to the oracle port, single thread
+    from oracle import oracle as O
+    import numpy as np
+    idx, _, _ = O.momenta((a.L,) * 3, "PERFECT", 1.0, a.ef, (2 * O.PI) ** 2)
+    job = O.Job(L=a.L, T=min(a.T, 4), configs=1, seed=a.seed)
+    t = time.perf_counter()
+    O.run_ensemble(job, O.plane_wave_sources(job.dims, idx))
+    el = time.perf_counter() - t
+    return {"value": job.T / el, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{job.T} slices of one configuration, oracle restatement, 1 thread"}
+
+
+def run_reference(a):
+    """--impl reference: the reference's own CPU implementation timed on the host."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np  # noqa: F401
+    n_orb = 19
+    samples = []
+    for i in range(a.warmup + a.steps):
+        t = time.perf_counter()
+        cb = cpu_baseline(a, max(4, a.cpu_sample_slices // 4), n_orb)
+        el = time.perf_counter() - t
+        if i >= a.warmup:
+            samples.append((cb, el))
+    vals = [s[0]["value"] for s in samples]
+    v = statistics.median(vals)
+    cb = dict(samples[-1][0])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1000 * statistics.median([s[1] for s in samples]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload(a, n_orb), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# -------------------------------------------------------------------- b200
+def run_b200(a):
+    import ctypes
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import nrcps_b200 as nb
+    from nrcps_b200 import _capi as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    ctx = nb.Context(local)
+
+    dims = (a.L,) * 3
+    idx, _, _ = nb.momenta(dims, "PERFECT", 1.0, a.ef, 2.0)
+    n_orb = len(idx)
+    job = nb.EnsembleJob(L=a.L, T=a.T, n_conf=a.configs, seed=a.seed, rank=rank, precision=a.precision,
+                         fermi_energy=a.ef)
+    ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
+    corr = torch.zeros((a.T, n_orb), dtype=torch.float64, device=dev)
+
+    def step(i):
+        dets = ens.run(i * a.configs)
+        # production/slater_det/main.C:208-211 and :226: corr[n][t] += |det|^2, summed over ranks
+        corr.copy_((dets.real ** 2 + dets.imag ** 2).sum(0))
+        if world > 1:
+            dist.all_reduce(corr)
+        return dets
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for i in range(a.warmup):
+        step(i)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    launches0 = ctx_launches = None
+    start.record()
+    for i in range(a.steps):
+        step(a.warmup + i)
+    stop.record()
+    barrier()
+    clocks.stop()
+    ms = start.elapsed_time(stop)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    launches_per_step = ens.launches() + 1  # graph body + field draw
+    value = world * a.configs * a.T * a.steps / (ms / 1000.0)
+
+    # ---- roofline of the dominant kernel: the fused transfer-matrix step
+    # (psi <- K B w F K psi), algorithmic bytes = one read + one write of every
+    # orbital = 2 * V * sizeof(complex) per orbital.
+    rconf = min(a.configs, 1024)
+    esize = 8 if a.precision == "f32" else 16
+    psi = torch.randn((rconf * n_orb,) + dims, dtype=torch.complex64 if a.precision == "f32" else torch.complex128,
+                      device=dev)
+    bits = nb.draw_z2_bits("RANLXS2", a.seed, 0, rconf * a.L ** 3, ctx)
+    kinv = torch.from_numpy(1.0 / nb.kinetic_table(dims, "PERFECT", 1.0, 0.5, 2.0)).to(dev)
+    pf = C.PositionFactor()
+    pf.field_mode, pf.dev_field, pf.bit0, pf.conf_stride = 1, bits.data_ptr(), 0, a.L ** 3
+    pf.a, pf.dev_pos = 0.5, None
+    d3 = np.array(dims, dtype=np.int32)
+    prec = C.F32 if a.precision == "f32" else C.F64
+
+    def prop():
+        ctx.check(nb.lib().nrcps_propagate(ctx.handle, ctypes.c_void_p(psi.data_ptr()), n_orb, rconf,
+                                           d3.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                           ctypes.c_void_p(kinv.data_ptr()), ctypes.byref(pf), prec), "propagate")
+
+    for _ in range(3):
+        prop()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record()
+    for _ in range(reps):
+        prop()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    kms = e0.elapsed_time(e1) / reps
+    alg_bytes = 2.0 * a.L ** 3 * esize * rconf * n_orb
+    achieved = alg_bytes / (kms / 1000.0) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "kernel": "fused transfer-matrix step (nrcps_propagate), %d configs x %d orbitals, %.3f ms/launch"
+                          % (rconf, n_orb, kms),
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    del psi, bits
+
+    # ---- end to end through the public API with host buffers: the step's
+    # input (source list, pinned) goes host->device, the raw determinants come
+    # back device->host into pinned memory.
+    idx_host = torch.from_numpy(np.asarray(idx, dtype=np.int32)).pin_memory()
+    idx_dev = torch.empty_like(idx_host, device=dev)
+    dets_host = torch.empty(ens.dets.shape, dtype=ens.dets.dtype).pin_memory()
+    barrier()
+    e0.record()
+    for i in range(a.steps):
+        idx_dev.copy_(idx_host, non_blocking=True)
+        dets = step(a.warmup + a.steps + i)
+        dets_host.copy_(dets, non_blocking=True)
+    e1.record()
+    barrier()
+    ems = e0.elapsed_time(e1)
+    t = torch.tensor([ems], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e = {"value": world * a.configs * a.T * a.steps / (float(t.item()) / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": idx_host.numel() * 4, "d2h_bytes_per_step": dets_host.numel() * 16}
+
+    if rank == 0:
+        cb = None if a.no_cpu_baseline else cpu_baseline(a, a.cpu_sample_slices, n_orb)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": a.precision, "data": "synthetic (device-drawn fields, plane-wave sources)",
+                "config": workload(a, n_orb), "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
+                "gpu_launches": launches_per_step * a.steps, "clocks": clocks.summary()}
+        print(json.dumps(line))
+    ens.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_b200(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

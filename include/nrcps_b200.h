@@ -1,0 +1,275 @@
+/*
+ * nrcps_b200.h -- C ABI of libnrcps_b200.so, the B200 (sm_100a) implementation
+ * of nrCPS's auxiliary-field transfer-matrix hot path.
+ *
+ * The reference (mgendres/nrCPS v2_7_6) swaps its CPU and GPU backends per
+ * translation unit behind fixed class headers (include/fourier.h,
+ * include/hamiltonian.h, include/propagator.h, include/one_body.h,
+ * include/two_body.h, include/slater_det*.h, include/lattice.h,
+ * include/random.h, include/cuda_utils.h).  Every entry point below replaces
+ * one of those GPU translation units' methods (cited beside it); the C++
+ * shims that re-implement the class methods over this ABI live in
+ * nrcps_b200/shim/.  Plain pointers and sizes only: device pointers are
+ * CUDA device addresses, host pointers are ordinary host memory.
+ *
+ * Conventions shared with the reference:
+ *   - lattice site (x,y,z) has index z + Z*(y + Y*x) (src/utils/vector3.C:190-215);
+ *   - an orbital is V = X*Y*Z complex numbers in momentum space, interleaved
+ *     (re, im); a batch of orbitals is contiguous, orbital n at offset n*V;
+ *   - sign -1 is FFTW_FORWARD (momentum -> position), +1 FFTW_BACKWARD;
+ *     transforms are unnormalised (src/fourier/noarch/fourier.C:34-35).
+ *
+ * Errors: every call returns nrcps_status; nothing in the library exits or
+ * traps.  The reference instead prints and calls exit() (src/utils/error.C:36-46);
+ * the shims translate a non-OK status into ERR.General to keep that behaviour.
+ * nrcps_last_error() describes the most recent failure on a context.
+ *
+ * Threading: a context is used by one host thread at a time; all its work is
+ * queued on the context's stream (nrcps_set_stream).
+ */
+#ifndef NRCPS_B200_H
+#define NRCPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Every entry point below is exported even when the library is built with
+ * hidden default visibility. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef enum {
+  NRCPS_OK = 0,
+  NRCPS_ERR_INVALID_ARGUMENT = 1,
+  NRCPS_ERR_UNSUPPORTED = 2,
+  NRCPS_ERR_CUDA = 3,
+  NRCPS_ERR_OUT_OF_MEMORY = 4,
+  NRCPS_ERR_SINGULAR = 5,  /* ludcmp's "singular matrix" (src/utils/ludcmp.C:31-34) */
+  NRCPS_ERR_NONFINITE = 6,
+  NRCPS_ERR_TIMEOUT = 7
+} nrcps_status;
+
+typedef enum { NRCPS_F64 = 0, NRCPS_F32 = 1 } nrcps_precision;
+
+/* Generator kinds, numbered as the reference's RandomType (include/enum.h:7-18). */
+typedef enum {
+  NRCPS_RAN0 = 0, NRCPS_RAN1 = 1, NRCPS_RAN2 = 2, NRCPS_RAN3 = 3,
+  NRCPS_RANLXS0 = 4, NRCPS_RANLXS1 = 5, NRCPS_RANLXS2 = 6,
+  NRCPS_RANLXD1 = 7, NRCPS_RANLXD2 = 8
+} nrcps_rng_kind;
+
+/* Field kinds, numbered as the reference's FieldType (include/enum.h:27-33). */
+typedef enum {
+  NRCPS_FIELD_GAUSS = 0, NRCPS_FIELD_COMPLEXGAUSS = 1,
+  NRCPS_FIELD_ZTWO = 2, NRCPS_FIELD_ZTHREE = 3
+} nrcps_field_kind;
+
+typedef struct nrcps_context nrcps_context;
+
+/* ------------------------------------------------------------ lifecycle */
+nrcps_status nrcps_create(int device, nrcps_context **ctx);
+nrcps_status nrcps_destroy(nrcps_context *ctx);
+const char *nrcps_last_error(const nrcps_context *ctx);
+/* cudaStream_t passed as void*; NULL selects the legacy default stream. */
+nrcps_status nrcps_set_stream(nrcps_context *ctx, void *stream);
+nrcps_status nrcps_synchronize(nrcps_context *ctx);
+/* Library version string, e.g. "nrcps_b200 0.1 sm_100a". */
+const char *nrcps_version(void);
+
+/* ----------------------------------------------------- host-side tables
+ * Replace the reference's host constructors' table builds so that callers
+ * without the reference classes get identical tables.  All outputs are host
+ * arrays of V doubles unless stated. cutoff_sq = (DoArg.cutoff * pi)^2. */
+
+/* Dispersion ctor (src/alg/dispersion.C:11-75); type = DispersionType,
+ * hard_cutoff = CutoffType.  Periodic boundaries. */
+nrcps_status nrcps_dispersion_table(const int dims[3], int type, double mass, int hard_cutoff,
+                                    double cutoff_sq, double *out);
+/* Kinetic ctor (src/hamiltonian/hamiltonian.C:260-281): xi = 1 + disp(m/dt). */
+nrcps_status nrcps_kinetic_table(const int dims[3], int type, double mass, double dt,
+                                 double cutoff_sq, double *xi);
+/* Interaction ctor (src/hamiltonian/hamiltonian.C:77-147): momentum factor
+ * c(p) incl. 1/V and dt; itype = InteractionType. */
+nrcps_status nrcps_interaction_table(const int dims[3], double mass, int itype,
+                                     const double *couplings, int ncoup, double dt,
+                                     double cutoff_sq, double *out);
+/* Potential ctor (src/hamiltonian/hamiltonian.C:165-244), harmonic form;
+ * ptype = PotentialType (0 LIN, 1 EXP).  Includes 1/V. */
+nrcps_status nrcps_potential_table(const int dims[3], int ptype, double k1, double k2, double k3,
+                                   double dt, double *out);
+/* Momenta ctor (src/alg/momenta.C:12-139).  Writes up to cap entries of the
+ * energy-sorted momenta (lattice index, energy, opposite-parity slot) and
+ * stores the total count in *count. */
+nrcps_status nrcps_momenta(const int dims[3], int disp_type, double mass, double fermi_energy,
+                           double cutoff_sq, int cap, int *index, double *energy, int *parity,
+                           int *count);
+/* OneBody::Set() SHO branch (src/one_body/one_body.C:66-166): coeffs = V
+ * complex with each file coefficient (n1,n2,n3,re,im) at its lattice index;
+ * psi = V complex. */
+nrcps_status nrcps_sho_source(const int dims[3], double lambda1, double lambda2, double lambda3,
+                              const double *coeffs, double *psi);
+/* TwoBody ctor (src/two_body/two_body.C:21-141): pair wave function w (V
+ * doubles) and opposite-parity index (V ints).  wf_type = WavefuncType. */
+nrcps_status nrcps_two_body_tables(const int dims[3], int wf_type, int disp1, int disp2, double m1,
+                                   double m2, double lambda, double cutoff_sq, double *w,
+                                   int *opposite);
+
+/* ------------------------------------------------------------------ RNG
+ * UniformDeviate/Random replacements (src/random/*.C).  The stream is the
+ * reference's: generator `kind` seeded with `seed` (the reference adds
+ * 491*rank first, src/random/random.C:88). */
+
+/* Reference binary state after Init(seed) (105 longs for ranlux,
+ * src/random/ranlxs.C:193-213; 36 for ran2, src/random/ran2.C:85-95). */
+nrcps_status nrcps_rng_seed_state(int kind, long seed, long *state, int *state_size);
+/* Advance a ranlux state by n uniforms without generating them (exact
+ * skip-ahead through the generator's equivalent linear congruential form). */
+nrcps_status nrcps_rng_skip(int kind, long *state, uint64_t n);
+/* `count` uniforms from stream position `offset` of (kind, seed), generated
+ * on the GPU into dev_out (doubles).  Bit-identical to Random::Uniform. */
+nrcps_status nrcps_rng_uniforms(nrcps_context *ctx, int kind, long seed, uint64_t offset,
+                                uint64_t count, double *dev_out);
+
+/* Lattice::Refresh (src/alg/lattice.C:60-109) on the GPU: `slices`
+ * consecutive field slices of `vol` sites starting at uniform position
+ * *offset of (kind, seed); writes interleaved complex doubles (2*vol per
+ * slice) to dev_out and advances *offset past the uniforms consumed.
+ * Z2/Z3 consume one uniform per site; Gauss consumes a data-dependent number
+ * (polar rejection, src/random/random.C:105-116). */
+nrcps_status nrcps_draw_fields(nrcps_context *ctx, int kind, long seed, int field_kind, long vol,
+                               long slices, uint64_t *offset, double *dev_out);
+/* Z2 fields as packed sign bits: bit u of dev_bits (32-bit words) is set when
+ * the site drawn from uniform u of the stream window has phi = +1, for
+ * u in [first, first + count). */
+nrcps_status nrcps_draw_z2_bits(nrcps_context *ctx, int kind, long seed, uint64_t first,
+                                uint64_t count, uint32_t *dev_bits);
+
+/* --------------------------------------------------------------- Fourier
+ * Fourier::Forward/Backward (src/fourier/cuda/fourier.cu:43-79): in-place
+ * unnormalised 3-D DFT of `batch` orbitals. */
+nrcps_status nrcps_fft3d(nrcps_context *ctx, void *data, int batch, const int dims[3],
+                         nrcps_precision prec, int sign);
+
+/* ------------------------------------------------------------ Hamiltonian
+ * Kinetic::Evolve (src/hamiltonian/cuda/hamiltonian_evolve.cu:95-104):
+ * psi /= xi on `batch` orbitals; xi is a device array of V doubles. */
+nrcps_status nrcps_kinetic_evolve(nrcps_context *ctx, void *psi, int batch, long vol,
+                                  const double *dev_xi, nrcps_precision prec);
+/* Potential::Evolve (hamiltonian_evolve.cu:73-92): FFT, psi *= v(x), IFFT. */
+nrcps_status nrcps_potential_evolve(nrcps_context *ctx, void *psi, int batch, const int dims[3],
+                                    const double *dev_pot, nrcps_precision prec);
+/* Interaction::Initialize (src/hamiltonian/cuda/hamiltonian_initialize.cu:17-35):
+ * fld = (1 + IFFT_fwd[c(p) * FFT_bwd[phi]]) / V, all FP64 device arrays. */
+nrcps_status nrcps_interaction_initialize(nrcps_context *ctx, const double *dev_lat,
+                                          const double *dev_itab, const int dims[3],
+                                          double *dev_fld);
+/* Interaction::Evolve (hamiltonian_evolve.cu:42-69): FFT, psi *= fld, IFFT. */
+nrcps_status nrcps_interaction_evolve(nrcps_context *ctx, void *psi, int batch, const int dims[3],
+                                      const double *dev_fld, nrcps_precision prec);
+
+/* Fused Propagator::Run (src/alg/propagator.C:35-45) over the ordering
+ * [K, (V), I, (V), K] for `nconf` independent configurations of `batch`
+ * orbitals each (psi[conf][orb][V]).  One pass: psi <- k .* B[w .* F[k .* psi]]
+ * with k = 1/xi (dev_kin, V doubles), w(x) = P(x) * fld_conf(x), where
+ * P (dev_pos, V doubles, may be NULL) folds the potential steps and the
+ * position-space factor fld_conf is chosen by field_mode (k = bit0 +
+ * conf*conf_stride + site):
+ *   0: complex FP64 fld (Interaction::Initialize output), element k of dev_field;
+ *   1: Z2 bits: fld = (1 + a*phi)/V with phi = +1 when bit k of dev_field is set;
+ *   2: interleaved complex FP64 phi (Lattice::Get layout), fld = (1 + a*phi)/V.
+ * Mathematically identical to the reference's sequence (F*B = V). */
+typedef struct {
+  int field_mode;
+  const void *dev_field;
+  uint64_t bit0;        /* element (mode 0/2) or bit (mode 1) offset of configuration 0 */
+  uint64_t conf_stride; /* elements (mode 0/2) or bits (mode 1) between configurations */
+  double a;
+  const double *dev_pos; /* may be NULL */
+} nrcps_position_factor;
+nrcps_status nrcps_propagate(nrcps_context *ctx, void *psi, int batch, int nconf, const int dims[3],
+                             const double *dev_kin, const nrcps_position_factor *w,
+                             nrcps_precision prec);
+
+/* --------------------------------------------------------- measurement */
+/* SlaterDet fill (src/slater_det/slater_det.C:33-37) via OneBody::Project
+ * (src/one_body/noarch/one_body_project.C:14-27) and Cuda::InnerProduct
+ * (src/utils/cuda/cuda_utils.cu:88-127): S[c][s][t] = sum_p conj(src_s(p))
+ * psi_{c,t}(p), for nconf configurations; src (ns x V, FP64 complex) shared,
+ * psi (nconf x nt x V, precision prec), S FP64 complex, row-major per conf. */
+nrcps_status nrcps_overlap(nrcps_context *ctx, const double *dev_src, int ns, const void *dev_psi,
+                           int nt, int nconf, long vol, nrcps_precision prec, double *dev_S);
+/* Plane-wave sources (OneBody::Set(n1,n2,n3), src/one_body/one_body.C:215-228):
+ * S[c][s][t] = psi_{c,t}(p_s), an exact gather; dev_index = ns lattice indices. */
+nrcps_status nrcps_overlap_planewave(nrcps_context *ctx, const int *dev_index, int ns,
+                                     const void *dev_psi, int nt, int nconf, long vol,
+                                     nrcps_precision prec, double *dev_S);
+/* TwoBody::Run (src/two_body/noarch/two_body_run.C:16-43): phi[c][s][t] =
+ * sum_i w_i psi1_{c,s}(i) psi2_{c,t}(opp(i)), no conjugation. */
+nrcps_status nrcps_pair_matrix(nrcps_context *ctx, const void *dev_psi1, const void *dev_psi2, int n,
+                               int nconf, long vol, const double *dev_w, const int *dev_opposite,
+                               nrcps_precision prec, double *dev_phi);
+/* SlaterDet::Run / SlaterDet2::Run (src/slater_det/slater_det.C:59-115,
+ * slater_det2.C:78-148) with ludcmp (src/utils/ludcmp.C:9-65) in FP64 for
+ * every leading minor n = 1..N of nconf matrices S (N x N complex):
+ *   mode 0: out[c][n-1] = det S_n (N values per matrix);
+ *   mode 1: out[c][2(n-1)] = det with column n-1 from dev_psi1 (struck
+ *           column), out[c][2(n-1)+1] = det S_n (2N values per matrix).
+ * log_det != 0 returns log det instead (DET_TYPE_LOG). */
+nrcps_status nrcps_slater_dets(nrcps_context *ctx, const double *dev_S, const double *dev_psi1,
+                               int N, int nconf, int mode, int log_det, double *dev_out);
+
+/* ------------------------------------------------------------ ensemble
+ * The production loop (production/slater_det/main.C:185-220, mode 0;
+ * production/slater_det2_trapped/main-no_cum.C:185-210, mode 1) for many
+ * independent configurations at once, the time loop captured in a CUDA
+ * graph.  Tables are host arrays (see the table builders above). */
+typedef struct {
+  int dims[3];
+  int T;
+  int n_orb;             /* N: orbitals = sources */
+  int n_conf;            /* configurations in one run() */
+  int rng_kind;
+  long seed;             /* already including 491*rank */
+  int field_kind;
+  int mode;              /* 0 slater (N minors), 1 slater2 (2N) */
+  int precision;         /* nrcps_precision of the orbital propagation */
+  int plane_wave;        /* 1: sources are plane waves given by index */
+  int use_potential;
+  int qr_period;         /* 0: never re-orthonormalise */
+  double a;              /* (1 + a*phi) coupling when the interaction is local */
+  int local_interaction; /* 1: c(p) constant, use a; 0: full Interaction::Initialize */
+} nrcps_job;
+
+typedef struct nrcps_ensemble nrcps_ensemble;
+
+/* kin_xi = xi table (V), itab = interaction c(p) table (V), pot = potential
+ * table (V, or NULL), sources = n_orb x V complex (ignored when plane_wave),
+ * pw_index = n_orb lattice indices (plane_wave only), w/opposite = pair tables
+ * (mode 1 only). */
+nrcps_status nrcps_ensemble_create(nrcps_context *ctx, const nrcps_job *job, const double *kin_xi,
+                                   const double *itab, const double *pot, const double *sources,
+                                   const int *pw_index, const double *w, const int *opposite,
+                                   nrcps_ensemble **ens);
+/* Runs configurations [first_conf, first_conf + n_conf) of the stream:
+ * configuration c uses field slices c*T .. c*T+T-1 (slice 0 = the Lattice
+ * constructor's draw).  dets: device array n_conf x T x nmeas complex
+ * doubles, nmeas = N (mode 0) or 2N (mode 1), raw determinants before any
+ * accumulation. */
+nrcps_status nrcps_ensemble_run(nrcps_ensemble *ens, uint64_t first_conf, double *dev_dets);
+nrcps_status nrcps_ensemble_destroy(nrcps_ensemble *ens);
+/* Kernel launches issued by the last run (for launch accounting). */
+nrcps_status nrcps_ensemble_launches(const nrcps_ensemble *ens, long *launches);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,577 @@
+"""Python host API over the C ABI, mirroring the reference's class API.
+
+The reference (mgendres/nrCPS v2_7_6) exposes its hot path as C++ classes
+(include/fourier.h, hamiltonian.h, propagator.h, lattice.h, random.h,
+one_body.h, two_body.h, slater_det.h).  The classes below keep those names,
+argument meanings and call order so that scripts and tests read like the
+reference's drivers; every numerical operation is a call into
+libnrcps_b200.so.  Device memory is held in torch tensors (complex128 /
+complex64 are interleaved (re, im), the layout the library expects).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field as dc_field
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _capi as C
+from ._capi import check, lib
+
+PI = 3.1415926535897932  # include/constants.h:12
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _dims(dims) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(dims, dtype=np.int32).reshape(3))
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def cutoff_sq(cutoff: float) -> float:
+    """GJP.CutoffSq() for DoArg.cutoff in units of pi (global_job_parameter.C:48,112)."""
+    c = cutoff * PI
+    return c * c
+
+
+# --------------------------------------------------------------------- context
+class Context:
+    """One device, one stream (torch's current stream by default)."""
+
+    def __init__(self, device: int = 0):
+        if not torch.cuda.is_available():
+            raise RuntimeError("nrcps_b200 needs a CUDA device")
+        self.device = torch.device("cuda", device)
+        h = ctypes.c_void_p()
+        check(lib().nrcps_create(device, ctypes.byref(h)), None, "nrcps_create")
+        self.handle = h
+        self.use_current_stream()
+
+    def use_current_stream(self) -> None:
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        check(lib().nrcps_set_stream(self.handle, ctypes.c_void_p(s)), self.handle, "nrcps_set_stream")
+
+    def check(self, status: int, what: str = "") -> None:
+        check(status, self.handle, what)
+
+    def synchronize(self) -> None:
+        self.check(lib().nrcps_synchronize(self.handle), "synchronize")
+
+    def close(self) -> None:
+        if self.handle:
+            lib().nrcps_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(torch.cuda.current_device())
+    return _default_ctx
+
+
+# ---------------------------------------------------------------- host tables
+def dispersion_table(dims, dtype: str = "PERFECT", mass: float = 1.0, hard_cutoff: bool = True,
+                     cutoff: float = 2.0) -> np.ndarray:
+    """Dispersion (src/alg/dispersion.C:11-75)."""
+    d = _dims(dims)
+    out = np.zeros(int(np.prod(d)))
+    check(lib().nrcps_dispersion_table(_ip(d), C.DISP_TYPES[dtype], mass, int(hard_cutoff), cutoff_sq(cutoff),
+                                       _dp(out)), None, "dispersion_table")
+    return out
+
+
+def kinetic_table(dims, dtype: str = "PERFECT", mass: float = 1.0, dt: float = 0.5, cutoff: float = 2.0) -> np.ndarray:
+    """Kinetic's xi(p) = 1 + disp(m/dt) (src/hamiltonian/hamiltonian.C:260-281)."""
+    d = _dims(dims)
+    out = np.zeros(int(np.prod(d)))
+    check(lib().nrcps_kinetic_table(_ip(d), C.DISP_TYPES[dtype], mass, dt, cutoff_sq(cutoff), _dp(out)), None,
+          "kinetic_table")
+    return out
+
+
+def interaction_table(dims, mass: float = 1.0, couplings: Sequence[float] = (0.019894367886486918,),
+                      dt: float = 1.0, cutoff: float = 2.0, itype: str = "ONEMINUSXIINVSQ") -> np.ndarray:
+    """Interaction's momentum factor c(p) (src/hamiltonian/hamiltonian.C:77-147)."""
+    d = _dims(dims)
+    c = np.ascontiguousarray(np.asarray(couplings, dtype=np.float64))
+    out = np.zeros(int(np.prod(d)))
+    check(lib().nrcps_interaction_table(_ip(d), mass, C.INTERACTION_TYPES[itype], _dp(c), len(c), dt,
+                                        cutoff_sq(cutoff), _dp(out)), None, "interaction_table")
+    return out
+
+
+def potential_table(dims, kappa=0.005, dt: float = 0.5, ptype: str = "EXP") -> np.ndarray:
+    """Harmonic Potential incl. 1/V (src/hamiltonian/hamiltonian.C:165-244)."""
+    d = _dims(dims)
+    k = list(kappa) if np.ndim(kappa) else [kappa] * 3
+    out = np.zeros(int(np.prod(d)))
+    check(lib().nrcps_potential_table(_ip(d), C.POTENTIAL_TYPES[ptype], k[0], k[1], k[2], dt, _dp(out)), None,
+          "potential_table")
+    return out
+
+
+def momenta(dims, dtype: str = "PERFECT", mass: float = 1.0, fermi_energy: float = 0.1, cutoff: float = 2.0):
+    """Momenta below the Fermi energy, energy-sorted (src/alg/momenta.C:12-139)."""
+    d = _dims(dims)
+    cap = int(np.prod(d))
+    idx = np.zeros(cap, dtype=np.int32)
+    en = np.zeros(cap)
+    par = np.zeros(cap, dtype=np.int32)
+    n = ctypes.c_int()
+    check(lib().nrcps_momenta(_ip(d), C.DISP_TYPES[dtype], mass, fermi_energy, cutoff_sq(cutoff), cap, _ip(idx),
+                              _dp(en), _ip(par), ctypes.byref(n)), None, "momenta")
+    k = n.value
+    return idx[:k].copy(), en[:k].copy(), par[:k].copy()
+
+
+def sho_source(dims, lambdas, coeff_lines) -> np.ndarray:
+    """OneBody::Set(file) for SHO sources (src/one_body/one_body.C:53-213)."""
+    d = _dims(dims)
+    X, Y, Z = (int(v) for v in d)
+    vol = X * Y * Z
+    co = np.zeros(2 * vol)
+    for n1, n2, n3, re, im in coeff_lines:
+        j = (int(n3) % Z) + Z * ((int(n2) % Y) + Y * (int(n1) % X))
+        co[2 * j], co[2 * j + 1] = re, im
+    out = np.zeros(2 * vol)
+    check(lib().nrcps_sho_source(_ip(d), lambdas[0], lambdas[1], lambdas[2], _dp(co), _dp(out)), None, "sho_source")
+    return out.view(np.complex128)
+
+
+def two_body_tables(dims, wavefunc: str = "TGND", disp: str = "STANDARD", mass: float = 1.0,
+                    lam: float = 0.176776695, cutoff: float = 0.99999):
+    """TwoBody's pair wave function and opposite-parity index (src/two_body/two_body.C:21-141)."""
+    d = _dims(dims)
+    vol = int(np.prod(d))
+    w = np.zeros(vol)
+    opp = np.zeros(vol, dtype=np.int32)
+    check(lib().nrcps_two_body_tables(_ip(d), C.WAVEFUNC_TYPES[wavefunc], C.DISP_TYPES[disp], C.DISP_TYPES[disp],
+                                      mass, mass, lam, cutoff_sq(cutoff), _dp(w), _ip(opp)), None, "two_body_tables")
+    return w, opp
+
+
+# ------------------------------------------------------------------------ RNG
+def rng_seed_state(kind: str, seed: int) -> np.ndarray:
+    st = np.zeros(105, dtype=np.int64)
+    n = ctypes.c_int()
+    check(lib().nrcps_rng_seed_state(C.RNG_KINDS[kind], seed, st.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                                     ctypes.byref(n)), None, "rng_seed_state")
+    return st[: n.value].copy()
+
+
+def rng_skip(kind: str, state: np.ndarray, n: int) -> np.ndarray:
+    st = np.ascontiguousarray(state, dtype=np.int64).copy()
+    check(lib().nrcps_rng_skip(C.RNG_KINDS[kind], st.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), n), None,
+          "rng_skip")
+    return st
+
+
+def uniforms(kind: str, seed: int, count: int, offset: int = 0, ctx: Optional[Context] = None) -> torch.Tensor:
+    ctx = ctx or default_context()
+    out = torch.empty(count, dtype=torch.float64, device=ctx.device)
+    ctx.check(lib().nrcps_rng_uniforms(ctx.handle, C.RNG_KINDS[kind], seed, offset, count, _ptr(out)), "uniforms")
+    return out
+
+
+def draw_fields(kind: str, seed: int, field: str, vol: int, slices: int, offset: int = 0,
+                ctx: Optional[Context] = None):
+    """Lattice::Refresh slices on the GPU: ([slices, vol, 2] float64, next stream offset)."""
+    ctx = ctx or default_context()
+    out = torch.empty((slices, vol, 2), dtype=torch.float64, device=ctx.device)
+    off = ctypes.c_uint64(offset)
+    ctx.check(lib().nrcps_draw_fields(ctx.handle, C.RNG_KINDS[kind], seed, C.FIELD_KINDS[field], vol, slices,
+                                      ctypes.byref(off), _ptr(out)), "draw_fields")
+    return out, off.value
+
+
+def draw_z2_bits(kind: str, seed: int, first: int, count: int, ctx: Optional[Context] = None) -> torch.Tensor:
+    ctx = ctx or default_context()
+    out = torch.empty((count + 31) // 32, dtype=torch.int32, device=ctx.device)
+    ctx.check(lib().nrcps_draw_z2_bits(ctx.handle, C.RNG_KINDS[kind], seed, first, count, _ptr(out)), "draw_z2_bits")
+    return out
+
+
+# ------------------------------------------------------------- class mirrors
+def _cdtype(precision: str):
+    return torch.complex128 if precision == "f64" else torch.complex64
+
+
+def _prec(precision: str) -> int:
+    return C.F64 if precision == "f64" else C.F32
+
+
+class Random:
+    """Random (src/random/random.C:12-93): generator kind, seed (+491*rank) and stream position."""
+
+    def __init__(self, kind: str = "RANLXS2", seed: int = 1234, rank: int = 0):
+        self.kind = kind
+        self.seed = seed + 491 * rank
+        self.offset = 0
+
+
+class Lattice:
+    """Lattice (src/alg/lattice.C): one field slice, drawn on the GPU from the Random stream."""
+
+    def __init__(self, dims, rng: Random, field: str = "ZTWO", ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.dims = tuple(int(v) for v in dims)
+        self.vol = int(np.prod(self.dims))
+        self.rng = rng
+        self.field_type = field
+        self.field = None
+        self.refresh()  # the constructor draws the first slice (lattice.C:15-31)
+
+    def refresh(self) -> None:
+        f, self.rng.offset = draw_fields(self.rng.kind, self.rng.seed, self.field_type, self.vol, 1,
+                                         self.rng.offset, self.ctx)
+        self.field = f[0]
+
+    def get(self) -> torch.Tensor:
+        return self.field
+
+
+class Fourier:
+    """Fourier (src/fourier/cuda/fourier.cu): a batch of orbitals with in-place 3-D DFTs."""
+
+    def __init__(self, batch: int, dims, precision: str = "f64", ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.dims = tuple(int(v) for v in dims)
+        self.precision = precision
+        self.b = torch.zeros((batch,) + self.dims, dtype=_cdtype(precision), device=self.ctx.device)
+
+    def batch_size(self) -> int:
+        return self.b.shape[0]
+
+    def forward(self) -> None:  # FFTW_FORWARD: momentum -> position
+        self.ctx.check(lib().nrcps_fft3d(self.ctx.handle, _ptr(self.b), self.batch_size(), _ip(_dims(self.dims)),
+                                         _prec(self.precision), -1), "Fourier::Forward")
+
+    def backward(self) -> None:  # FFTW_BACKWARD: position -> momentum
+        self.ctx.check(lib().nrcps_fft3d(self.ctx.handle, _ptr(self.b), self.batch_size(), _ip(_dims(self.dims)),
+                                         _prec(self.precision), +1), "Fourier::Backward")
+
+    def get(self, n: int) -> torch.Tensor:
+        if n < 0 or n >= self.batch_size():
+            raise ValueError("Fourier::Get: argument out of range")  # fourier_common.C:14-15
+        return self.b[n]
+
+
+class Kinetic:
+    """Kinetic (src/hamiltonian/hamiltonian.C:260-281): psi(p) /= xi(p)."""
+
+    def __init__(self, dims, dispersion: str = "PERFECT", mass: float = 1.0, dt: float = 0.5, cutoff: float = 2.0,
+                 ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.xi_host = kinetic_table(dims, dispersion, mass, dt, cutoff)
+        self.xi = torch.from_numpy(self.xi_host).to(self.ctx.device)
+
+    def initialize(self) -> None:
+        pass
+
+    def evolve(self, b: Fourier) -> None:
+        self.ctx.check(lib().nrcps_kinetic_evolve(self.ctx.handle, _ptr(b.b), b.batch_size(), self.xi.numel(),
+                                                  _ptr(self.xi), _prec(b.precision)), "Kinetic::Evolve")
+
+
+class Potential:
+    """Potential (src/hamiltonian/hamiltonian.C:165-244): FFT, psi(x) *= v(x), IFFT."""
+
+    def __init__(self, dims, kappa=0.005, dt: float = 0.5, ptype: str = "EXP", ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.dims = tuple(int(v) for v in dims)
+        self.pot_host = potential_table(dims, kappa, dt, ptype)
+        self.pot = torch.from_numpy(self.pot_host).to(self.ctx.device)
+
+    def initialize(self) -> None:
+        pass
+
+    def evolve(self, b: Fourier) -> None:
+        self.ctx.check(lib().nrcps_potential_evolve(self.ctx.handle, _ptr(b.b), b.batch_size(), _ip(_dims(self.dims)),
+                                                    _ptr(self.pot), _prec(b.precision)), "Potential::Evolve")
+
+
+class Interaction:
+    """Interaction (src/hamiltonian/hamiltonian.C:77-147): smeared aux-field factor."""
+
+    def __init__(self, lattice: Lattice, mass: float = 1.0, couplings=(0.019894367886486918,), dt: float = 1.0,
+                 cutoff: float = 2.0, itype: str = "ONEMINUSXIINVSQ"):
+        self.ctx = lattice.ctx
+        self.lattice = lattice
+        self.dims = lattice.dims
+        self.itab_host = interaction_table(self.dims, mass, couplings, dt, cutoff, itype)
+        self.itab = torch.from_numpy(self.itab_host).to(self.ctx.device)
+        self.fld = torch.zeros((lattice.vol, 2), dtype=torch.float64, device=self.ctx.device)
+
+    def initialize(self) -> None:
+        self.ctx.check(lib().nrcps_interaction_initialize(self.ctx.handle, _ptr(self.lattice.get()), _ptr(self.itab),
+                                                          _ip(_dims(self.dims)), _ptr(self.fld)),
+                       "Interaction::Initialize")
+
+    def evolve(self, b: Fourier) -> None:
+        self.ctx.check(lib().nrcps_interaction_evolve(self.ctx.handle, _ptr(b.b), b.batch_size(),
+                                                      _ip(_dims(self.dims)), _ptr(self.fld), _prec(b.precision)),
+                       "Interaction::Evolve")
+
+
+class Propagator:
+    """Propagator (src/alg/propagator.C): N orbitals advanced by a Hamiltonian list."""
+
+    def __init__(self, n_fermions: int, dims, precision: str = "f64", ctx: Optional[Context] = None):
+        self.b = Fourier(n_fermions, dims, precision, ctx)
+        self.ctx = self.b.ctx
+
+    def run(self, hamiltonians) -> None:
+        for h in hamiltonians:
+            h.evolve(self.b)
+
+    def set(self, psi, n: int) -> None:
+        src = psi if isinstance(psi, torch.Tensor) else torch.from_numpy(np.asarray(psi))
+        self.b.get(n).copy_(src.reshape(self.b.dims).to(self.b.b.dtype).to(self.ctx.device))
+
+    def get(self, n: Optional[int] = None):
+        return self.b if n is None else self.b.get(n)
+
+
+class OneBody:
+    """OneBody (src/one_body/one_body.C): a source vector in momentum space."""
+
+    def __init__(self, dims, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.dims = tuple(int(v) for v in dims)
+        self.vol = int(np.prod(self.dims))
+        self.psi = torch.zeros(self.vol, dtype=torch.complex128, device=self.ctx.device)
+
+    def set_momentum(self, n1: int, n2: int, n3: int) -> None:  # OneBody::Set(int,int,int)
+        X, Y, Z = self.dims
+        self.psi.zero_()
+        self.psi[(n3 % Z) + Z * ((n2 % Y) + Y * (n1 % X))] = 1.0
+
+    def set_vector(self, v) -> None:  # OneBody::Set(Float*)
+        self.psi.copy_(torch.as_tensor(np.asarray(v), dtype=torch.complex128).reshape(-1))
+
+    def get(self) -> torch.Tensor:
+        return self.psi
+
+    def project(self, phi: torch.Tensor) -> complex:  # OneBody::Project
+        S = overlap(self.psi.reshape(1, -1), phi.reshape(1, -1), self.ctx)
+        return complex(S[0, 0, 0].item())
+
+
+class TwoBody:
+    """TwoBody (src/two_body/two_body.C): pair sink sum_p w(p) psi1(p) psi2(-p)."""
+
+    def __init__(self, dims, wavefunc: str = "TGND", disp: str = "STANDARD", mass: float = 1.0,
+                 lam: float = 0.176776695, cutoff: float = 0.99999, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.w_host, self.opp_host = two_body_tables(dims, wavefunc, disp, mass, lam, cutoff)
+        self.w = torch.from_numpy(self.w_host).to(self.ctx.device)
+        self.opp = torch.from_numpy(self.opp_host).to(self.ctx.device)
+
+    def run_matrix(self, props1: torch.Tensor, props2: torch.Tensor) -> torch.Tensor:
+        """TwoBody::Run(Float**, Float**, complex*, int): [nconf, n, n] pair matrices."""
+        p1 = props1.reshape(-1, props1.shape[-2] if props1.dim() > 2 else props1.shape[0], self.w.numel())
+        p2 = props2.reshape(p1.shape)
+        nconf, n, vol = p1.shape
+        out = torch.empty((nconf, n, n), dtype=torch.complex128, device=self.ctx.device)
+        prec = C.F64 if p1.dtype == torch.complex128 else C.F32
+        self.ctx.check(lib().nrcps_pair_matrix(self.ctx.handle, _ptr(p1), _ptr(p2), n, nconf, vol, _ptr(self.w),
+                                               _ptr(self.opp), prec, _ptr(out)), "TwoBody::Run")
+        return out
+
+    def run(self, prop1: torch.Tensor, prop2: torch.Tensor) -> complex:
+        """TwoBody::Run(Float*, Float*)."""
+        return complex(self.run_matrix(prop1.reshape(1, 1, -1), prop2.reshape(1, 1, -1))[0, 0, 0].item())
+
+
+def overlap(src: torch.Tensor, psi: torch.Tensor, ctx: Optional[Context] = None) -> torch.Tensor:
+    """S[c][s][t] = <src_s | psi_{c,t}>; src [ns, V] complex128, psi [nconf, nt, V] or [nt, V]."""
+    ctx = ctx or default_context()
+    src = src.reshape(src.shape[0], -1).contiguous()
+    vol = src.shape[1]
+    p = psi.reshape(-1, psi.shape[-2] if psi.dim() >= 3 else psi.shape[0], vol).contiguous()
+    nconf, nt, _ = p.shape
+    S = torch.empty((nconf, src.shape[0], nt), dtype=torch.complex128, device=ctx.device)
+    prec = C.F64 if p.dtype == torch.complex128 else C.F32
+    ctx.check(lib().nrcps_overlap(ctx.handle, _ptr(src), src.shape[0], _ptr(p), nt, nconf, vol, prec, _ptr(S)),
+              "overlap")
+    return S
+
+
+def overlap_planewave(index, psi: torch.Tensor, ctx: Optional[Context] = None) -> torch.Tensor:
+    ctx = ctx or default_context()
+    idx = torch.as_tensor(np.asarray(index, dtype=np.int32), device=ctx.device)
+    p = psi.contiguous()
+    nconf, nt, vol = p.shape
+    S = torch.empty((nconf, idx.numel(), nt), dtype=torch.complex128, device=ctx.device)
+    prec = C.F64 if p.dtype == torch.complex128 else C.F32
+    ctx.check(lib().nrcps_overlap_planewave(ctx.handle, _ptr(idx), idx.numel(), _ptr(p), nt, nconf, vol, prec,
+                                            _ptr(S)), "overlap_planewave")
+    return S
+
+
+def slater_dets(S: torch.Tensor, psi1: Optional[torch.Tensor] = None, mode: int = 0, log: bool = False,
+                ctx: Optional[Context] = None) -> torch.Tensor:
+    """All leading-minor determinants of [nconf, N, N] Slater matrices (SlaterDet::Run / SlaterDet2::Run)."""
+    ctx = ctx or default_context()
+    S = S.contiguous()
+    nconf, N, _ = S.shape
+    nmeas = 2 * N if mode else N
+    out = torch.empty((nconf, nmeas), dtype=torch.complex128, device=ctx.device)
+    p1 = psi1.contiguous() if psi1 is not None else None
+    ctx.check(lib().nrcps_slater_dets(ctx.handle, _ptr(S), _ptr(p1), N, nconf, mode, int(log), _ptr(out)),
+              "slater_dets")
+    return out
+
+
+class SlaterDet:
+    """SlaterDet (src/slater_det/slater_det.C): S[s][t] = <src_s|prop_t>, det of leading minors."""
+
+    def __init__(self, props: torch.Tensor, one_bodies: Sequence[OneBody]):
+        self.ctx = one_bodies[0].ctx
+        src = torch.stack([ob.get() for ob in one_bodies])
+        self.mat = overlap(src, props.reshape(1, len(one_bodies), -1), self.ctx)
+        self._dets = None
+        self.log = False
+
+    def set_det_type(self, log: bool) -> None:
+        self.log = log
+        self._dets = None
+
+    def slater_mat(self, s: int, t: int) -> complex:
+        return complex(self.mat[0, s, t].item())
+
+    def run(self, n: int) -> complex:
+        if n > self.mat.shape[1]:
+            raise ValueError("Submatrix exceeds size of matrix.")  # slater_det.C:66-68
+        if n < 1:
+            return 1.0
+        if self._dets is None:
+            self._dets = slater_dets(self.mat, log=self.log, ctx=self.ctx).cpu()
+        return complex(self._dets[0, n - 1])
+
+
+# ------------------------------------------------------------------ ensemble
+@dataclass
+class EnsembleJob:
+    """One batched run of the production loop (production/slater_det/main.C)."""
+    L: int = 16
+    T: int = 32
+    n_conf: int = 200
+    rng: str = "RANLXS2"
+    seed: int = 1234
+    rank: int = 0
+    field: str = "ZTWO"
+    precision: str = "f64"
+    kin_disp: str = "PERFECT"
+    kin_mass: float = 1.0
+    kin_dt: float = 0.5
+    cutoff: float = 2.0
+    int_mass: float = 1.0
+    int_dt: float = 1.0
+    int_type: str = "ONEMINUSXIINVSQ"
+    couplings: list = dc_field(default_factory=lambda: [0.019894367886486918])
+    potential: bool = False
+    pot_type: str = "EXP"
+    kappa: float = 0.005
+    pot_dt: float = 0.5
+    mode: str = "slater"  # "slater" (N minors) or "slater2" (2N, pair sink)
+    wavefunc: str = "TGND"
+    wf_disp: str = "STANDARD"
+    wf_mass: float = 1.0
+    wf_lambda: float = 0.176776695
+    fermi_energy: float = 0.1
+
+    @property
+    def dims(self):
+        return (self.L, self.L, self.L)
+
+
+class Ensemble:
+    """nrcps_ensemble: every configuration of a run advanced together, time loop in a CUDA graph."""
+
+    def __init__(self, job: EnsembleJob, sources: Optional[np.ndarray] = None, plane_wave_index=None,
+                 ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.job = job
+        dims = job.dims
+        vol = int(np.prod(dims))
+        xi = kinetic_table(dims, job.kin_disp, job.kin_mass, job.kin_dt, job.cutoff)
+        itab = interaction_table(dims, job.int_mass, job.couplings, job.int_dt, job.cutoff, job.int_type)
+        pot = potential_table(dims, job.kappa, job.pot_dt, job.pot_type) if job.potential else None
+        local = len(job.couplings) == 1
+        if plane_wave_index is not None:
+            idx = np.ascontiguousarray(np.asarray(plane_wave_index, dtype=np.int32))
+            n_orb = idx.size
+            src = None
+        else:
+            src = np.ascontiguousarray(np.asarray(sources, dtype=np.complex128).reshape(-1, vol))
+            n_orb = src.shape[0]
+            idx = None
+        self.n_orb = n_orb
+        self.nmeas = 2 * n_orb if job.mode == "slater2" else n_orb
+        w = opp = None
+        if job.mode == "slater2":
+            w, opp = two_body_tables(dims, job.wavefunc, job.wf_disp, job.wf_mass, job.wf_lambda, job.cutoff)
+        j = C.Job()
+        j.dims[:] = dims
+        j.T, j.n_orb, j.n_conf = job.T, n_orb, job.n_conf
+        j.rng_kind, j.seed = C.RNG_KINDS[job.rng], job.seed + 491 * job.rank
+        j.field_kind = C.FIELD_KINDS[job.field]
+        j.mode = 1 if job.mode == "slater2" else 0
+        j.precision = _prec(job.precision)
+        j.plane_wave = int(idx is not None)
+        j.use_potential = int(pot is not None)
+        j.qr_period = 0
+        j.a = float(itab[0] * vol)  # c(p) * V: the local (1 + a phi) coupling
+        j.local_interaction = int(local)
+        self._keep = (xi, itab, pot, src, idx, w, opp)
+        h = ctypes.c_void_p()
+        dp = lambda a: None if a is None else _dp(a.view(np.float64) if a.dtype == np.complex128 else a)
+        ipn = lambda a: None if a is None else _ip(a)
+        self.ctx.check(lib().nrcps_ensemble_create(self.ctx.handle, ctypes.byref(j), dp(xi), dp(itab), dp(pot),
+                                                   dp(src), ipn(idx), dp(w), ipn(opp), ctypes.byref(h)),
+                       "ensemble_create")
+        self.handle = h
+        self.dets = torch.empty((job.n_conf, job.T, self.nmeas), dtype=torch.complex128, device=self.ctx.device)
+
+    def run(self, first_conf: int = 0) -> torch.Tensor:
+        """Raw determinants [n_conf, T, nmeas] of configurations first_conf.. (device tensor)."""
+        self.ctx.check(lib().nrcps_ensemble_run(self.handle, first_conf, _ptr(self.dets)), "ensemble_run")
+        return self.dets
+
+    def launches(self) -> int:
+        n = ctypes.c_long()
+        self.ctx.check(lib().nrcps_ensemble_launches(self.handle, ctypes.byref(n)), "ensemble_launches")
+        return n.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().nrcps_ensemble_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

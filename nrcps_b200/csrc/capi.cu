@@ -1,0 +1,93 @@
+// capi.cu -- context lifecycle, error reporting and scratch memory of the C ABI.
+#include <cstdarg>
+#include <cstdio>
+
+#include "common.cuh"
+
+namespace nrcps {
+
+nrcps_status set_error(nrcps_context* ctx, nrcps_status st, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return st;
+}
+
+nrcps_status check_cuda(nrcps_context* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return NRCPS_OK;
+  nrcps_status st = (e == cudaErrorMemoryAllocation) ? NRCPS_ERR_OUT_OF_MEMORY : NRCPS_ERR_CUDA;
+  return set_error(ctx, st, "%s: %s", what, cudaGetErrorString(e));
+}
+
+nrcps_status check_launch(nrcps_context* ctx, const char* what) {
+  return check_cuda(ctx, cudaGetLastError(), what);
+}
+
+void* scratch(nrcps_context* ctx, size_t bytes, nrcps_status* st) {
+  *st = NRCPS_OK;
+  if (bytes <= ctx->scratch_bytes) return ctx->scratch;
+  if (ctx->scratch) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->scratch);
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+  }
+  size_t want = bytes + bytes / 4;
+  cudaError_t e = cudaMalloc(&ctx->scratch, want);
+  if (e != cudaSuccess) {
+    *st = check_cuda(ctx, e, "cudaMalloc(scratch)");
+    ctx->scratch = nullptr;
+    return nullptr;
+  }
+  ctx->scratch_bytes = want;
+  return ctx->scratch;
+}
+
+}  // namespace nrcps
+
+using namespace nrcps;
+
+extern "C" const char* nrcps_version(void) { return "nrcps_b200 0.1 sm_100a"; }
+
+extern "C" nrcps_status nrcps_create(int device, nrcps_context** out) {
+  if (!out) return NRCPS_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return NRCPS_ERR_CUDA;
+  if (device < 0 || device >= n) return NRCPS_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return NRCPS_ERR_CUDA;
+  nrcps_context* ctx = new nrcps_context();
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+  *out = ctx;
+  return NRCPS_OK;
+}
+
+extern "C" nrcps_status nrcps_destroy(nrcps_context* ctx) {
+  if (!ctx) return NRCPS_OK;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->scratch) cudaFree(ctx->scratch);
+  if (ctx->gen_args) cudaFree(ctx->gen_args);
+  delete ctx;
+  return NRCPS_OK;
+}
+
+extern "C" const char* nrcps_last_error(const nrcps_context* ctx) {
+  return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+extern "C" nrcps_status nrcps_set_stream(nrcps_context* ctx, void* stream) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  ctx->stream = (cudaStream_t)stream;
+  return NRCPS_OK;
+}
+
+extern "C" nrcps_status nrcps_synchronize(nrcps_context* ctx) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+}

@@ -1,0 +1,99 @@
+// common.cuh -- shared types and helpers of libnrcps_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+
+#include "../../include/nrcps_b200.h"
+
+namespace nrcps {
+
+// ------------------------------------------------------------------ complex
+template <typename R>
+struct cplx {
+  R re, im;
+};
+
+// Vector type carrying one complex number, for 8/16-byte accesses.
+template <typename R>
+struct vec2;
+template <>
+struct vec2<float> {
+  typedef float2 type;
+};
+template <>
+struct vec2<double> {
+  typedef double2 type;
+};
+
+template <typename R>
+__device__ __forceinline__ cplx<R> ld(const void* base, long i) {
+  typedef typename vec2<R>::type V;
+  V v = reinterpret_cast<const V*>(base)[i];
+  return cplx<R>{v.x, v.y};
+}
+template <typename R>
+__device__ __forceinline__ void st(void* base, long i, cplx<R> c) {
+  typedef typename vec2<R>::type V;
+  V v;
+  v.x = c.re;
+  v.y = c.im;
+  reinterpret_cast<V*>(base)[i] = v;
+}
+
+template <typename R>
+__host__ __device__ __forceinline__ cplx<R> cmul(cplx<R> a, cplx<R> b) {
+  return cplx<R>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+// ---------------------------------------------------------------- context
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  int sm_count = 148;
+  // Scratch owned by the context (grown on demand, never shrunk).
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  long launches = 0;  // kernels queued through this context
+  // Device copy of the ranlux generation arguments for (gen_kind, gen_seed).
+  void* gen_args = nullptr;
+  int gen_kind = -1;
+  long gen_seed = 0;
+};
+
+}  // namespace nrcps
+
+struct nrcps_context : public nrcps::Context {};
+
+namespace nrcps {
+
+nrcps_status set_error(nrcps_context* ctx, nrcps_status st, const char* fmt, ...);
+nrcps_status check_cuda(nrcps_context* ctx, cudaError_t e, const char* what);
+nrcps_status check_launch(nrcps_context* ctx, const char* what);
+void* scratch(nrcps_context* ctx, size_t bytes, nrcps_status* st);
+
+inline long vol_of(const int dims[3]) { return (long)dims[0] * dims[1] * dims[2]; }
+
+inline unsigned grid_for(long n, int block, long cap = 148L * 64) {
+  long g = (n + block - 1) / block;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+}  // namespace nrcps
+
+#define NRCPS_TRY(expr)                       \
+  do {                                        \
+    nrcps_status _s = (expr);                 \
+    if (_s != NRCPS_OK) return _s;            \
+  } while (0)
+
+#define NRCPS_REQUIRE(ctx, cond, ...)                                            \
+  do {                                                                           \
+    if (!(cond)) return nrcps::set_error((ctx), NRCPS_ERR_INVALID_ARGUMENT, __VA_ARGS__); \
+  } while (0)

@@ -1,0 +1,192 @@
+// fft.cuh -- register-resident DFTs of compile-time length for 3-D lattice FFTs.
+//
+// A pencil of N complex values lives in one thread's registers; the
+// transform is a fully unrolled mixed-radix (4, 2, 3) decimation-in-time
+// Cooley-Tukey.  Twiddles W_N^k = exp(SIGN * 2*pi*i * k / N) are
+// compile-time constants: every loop index that reaches a twiddle is a
+// template parameter (static_for), and the constants come from a constexpr
+// sine/cosine written here from their Taylor series after exact octant
+// reduction of the rational angle k/N (no runtime math library involved).
+// Conventions match FFTW's (src/fourier/noarch/fourier.C:34-35 of the
+// reference): SIGN = -1 is FFTW_FORWARD, +1 FFTW_BACKWARD, unnormalised.
+#pragma once
+
+#include <utility>
+
+#include "common.cuh"
+
+namespace nrcps {
+namespace fft {
+
+// ------------------------------------------------------------- static_for
+template <typename F, int... Is>
+__host__ __device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, Is...>) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, typename F>
+__host__ __device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// --------------------------------------------------- constexpr sin / cos
+// sin and cos of phi in [0, pi/4] by Taylor series (terms to phi^27, below
+// 1e-30 relative), evaluated in double at compile time.
+constexpr double taylor_sin(double x) {
+  double term = x, sum = x;
+  for (int n = 1; n < 14; ++n) {
+    term *= -x * x / ((2.0 * n) * (2.0 * n + 1.0));
+    sum += term;
+  }
+  return sum;
+}
+constexpr double taylor_cos(double x) {
+  double term = 1.0, sum = 1.0;
+  for (int n = 1; n < 14; ++n) {
+    term *= -x * x / ((2.0 * n - 1.0) * (2.0 * n));
+    sum += term;
+  }
+  return sum;
+}
+constexpr double kHalfPi = 1.57079632679489661923132169163975144;
+
+// cos and sin of 2*pi*k/n for integers k, n > 0, reduced exactly to the
+// first octant with integer arithmetic.
+struct CS {
+  double c, s;
+};
+constexpr CS unit_root(long k, long n) {
+  long kk = ((k % n) + n) % n;
+  long q = (4 * kk) / n;        // quadrant
+  long r = 4 * kk - q * n;      // angle within quadrant = (pi/2) * r / n
+  double c = 0, s = 0;
+  if (2 * r <= n) {
+    double phi = kHalfPi * (double)r / (double)n;
+    c = taylor_cos(phi);
+    s = taylor_sin(phi);
+  } else {
+    double phi = kHalfPi * (double)(n - r) / (double)n;
+    c = taylor_sin(phi);
+    s = taylor_cos(phi);
+  }
+  // rotate by q quarter turns
+  for (long i = 0; i < q; ++i) {
+    double t = c;
+    c = -s;
+    s = t;
+  }
+  return CS{c, s};
+}
+
+// x * W_N^K with W_N = exp(SIGN 2 pi i / N); exact for multiples of N/4.
+template <int N, int K, int SIGN, typename R>
+__device__ __forceinline__ cplx<R> twiddle(cplx<R> x) {
+  constexpr int k = ((K % N) + N) % N;
+  if constexpr (k == 0) {
+    return x;
+  } else if constexpr ((4 * k) % N == 0) {
+    constexpr int q = (4 * k) / N;  // quarter turns of exp(+2 pi i k/N)
+    constexpr int qs = SIGN > 0 ? q : (4 - q) % 4;
+    if constexpr (qs == 1) return cplx<R>{-x.im, x.re};
+    else if constexpr (qs == 2) return cplx<R>{-x.re, -x.im};
+    else return cplx<R>{x.im, -x.re};
+  } else {
+    constexpr CS w = unit_root(k, N);
+    constexpr R c = (R)w.c;
+    constexpr R s = (R)(SIGN > 0 ? w.s : -w.s);
+    return cplx<R>{x.re * c - x.im * s, x.re * s + x.im * c};
+  }
+}
+
+template <int SIGN, typename R>
+__device__ __forceinline__ cplx<R> mul_i(cplx<R> z) {  // SIGN * i * z
+  if constexpr (SIGN > 0) return cplx<R>{-z.im, z.re};
+  else return cplx<R>{z.im, -z.re};
+}
+
+template <typename R>
+__device__ __forceinline__ cplx<R> add(cplx<R> a, cplx<R> b) { return cplx<R>{a.re + b.re, a.im + b.im}; }
+template <typename R>
+__device__ __forceinline__ cplx<R> sub(cplx<R> a, cplx<R> b) { return cplx<R>{a.re - b.re, a.im - b.im}; }
+
+// ------------------------------------------------------------ butterflies
+template <int P, int SIGN, typename R>
+struct Butterfly;
+
+template <int SIGN, typename R>
+struct Butterfly<2, SIGN, R> {
+  static __device__ __forceinline__ void run(cplx<R>* t) {
+    cplx<R> a = t[0], b = t[1];
+    t[0] = add(a, b);
+    t[1] = sub(a, b);
+  }
+};
+
+template <int SIGN, typename R>
+struct Butterfly<4, SIGN, R> {
+  static __device__ __forceinline__ void run(cplx<R>* t) {
+    cplx<R> s02 = add(t[0], t[2]), d02 = sub(t[0], t[2]);
+    cplx<R> s13 = add(t[1], t[3]), d13 = mul_i<SIGN>(sub(t[1], t[3]));
+    t[0] = add(s02, s13);
+    t[2] = sub(s02, s13);
+    t[1] = add(d02, d13);
+    t[3] = sub(d02, d13);
+  }
+};
+
+template <int SIGN, typename R>
+struct Butterfly<3, SIGN, R> {
+  static __device__ __forceinline__ void run(cplx<R>* t) {
+    constexpr R c = (R)-0.5;
+    constexpr R s = (R)0.86602540378443864676372317075293618;  // sin(2 pi / 3)
+    cplx<R> u = add(t[1], t[2]);
+    cplx<R> v = sub(t[1], t[2]);
+    cplx<R> m{t[0].re + c * u.re, t[0].im + c * u.im};
+    cplx<R> iv = mul_i<SIGN>(cplx<R>{s * v.re, s * v.im});
+    t[0] = add(t[0], u);
+    t[1] = add(m, iv);
+    t[2] = sub(m, iv);
+  }
+};
+
+template <int N>
+struct Radix {
+  static constexpr int value = (N % 4 == 0) ? 4 : (N % 2 == 0 ? 2 : (N % 3 == 0 ? 3 : N));
+};
+
+// ------------------------------------------------------------------- DFT
+// In-place DFT of x[0..N) (natural order in and out).
+template <int N, int SIGN, typename R>
+struct Dft {
+  static_assert(N == 1 || Radix<N>::value <= 4, "only lengths 2^a 3^b are supported");
+  static __device__ __forceinline__ void run(cplx<R>* x) {
+    constexpr int P = Radix<N>::value;
+    constexpr int M = N / P;
+    if constexpr (N == 1) {
+      return;
+    } else if constexpr (M == 1) {
+      Butterfly<P, SIGN, R>::run(x);
+    } else {
+      cplx<R> s[P][M];
+#pragma unroll
+      for (int q = 0; q < P; ++q)
+#pragma unroll
+        for (int j = 0; j < M; ++j) s[q][j] = x[j * P + q];
+#pragma unroll
+      for (int q = 0; q < P; ++q) Dft<M, SIGN, R>::run(s[q]);
+      static_for<M>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        cplx<R> t[P];
+        static_for<P>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          t[q] = twiddle<N, q * k, SIGN, R>(s[q][k]);
+        });
+        Butterfly<P, SIGN, R>::run(t);
+#pragma unroll
+        for (int ss = 0; ss < P; ++ss) x[k + ss * M] = t[ss];
+      });
+    }
+  }
+};
+
+}  // namespace fft
+}  // namespace nrcps

@@ -1,0 +1,325 @@
+// measure.cu -- Slater-matrix fills and determinants (the measurement half of
+// every time slice): overlaps S = <src|psi>, the pair matrix of TwoBody, and
+// FP64 LU of every leading minor with the reference's pivoting rule.
+#include "common.cuh"
+
+namespace nrcps {
+
+// ---------------------------------------------------------------- overlap
+// One block per (configuration, orbital t); sources in chunks of 8.  FP64
+// accumulation for both orbital precisions.
+template <typename R>
+__global__ void __launch_bounds__(256) overlap_kernel(const double* __restrict__ src, int ns,
+                                                      const void* __restrict__ psi, int nt, long vol,
+                                                      double* __restrict__ S) {
+  const long ct = blockIdx.x;  // conf * nt + t
+  const long conf = ct / nt;
+  const int t = (int)(ct % nt);
+  const char* p = reinterpret_cast<const char*>(psi) + (size_t)ct * vol * 2 * sizeof(R);
+  __shared__ double red[8][2][8];
+  for (int s0 = 0; s0 < ns; s0 += 8) {
+    double ar[8], ai[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ar[k] = ai[k] = 0.0;
+    for (long i = threadIdx.x; i < vol; i += blockDim.x) {
+      cplx<R> q = ld<R>(p, i);
+      double qr = (double)q.re, qi = (double)q.im;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (s0 + k < ns) {
+          double2 a = reinterpret_cast<const double2*>(src)[(long)(s0 + k) * vol + i];
+          ar[k] += a.x * qr + a.y * qi;
+          ai[k] += a.x * qi - a.y * qr;
+        }
+      }
+    }
+    // warp reduce then block reduce
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      for (int off = 16; off > 0; off >>= 1) {
+        ar[k] += __shfl_down_sync(0xffffffffu, ar[k], off);
+        ai[k] += __shfl_down_sync(0xffffffffu, ai[k], off);
+      }
+    }
+    const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    if (ln == 0) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        red[warp][0][k] = ar[k];
+        red[warp][1][k] = ai[k];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 8 && s0 + (int)threadIdx.x < ns) {
+      const int k = threadIdx.x;
+      double sr = 0.0, si = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        sr += red[w][0][k];
+        si += red[w][1][k];
+      }
+      long o = ((conf * ns + (s0 + k)) * (long)nt + t) * 2;
+      S[o] = sr;
+      S[o + 1] = si;
+    }
+    __syncthreads();
+  }
+}
+
+// Plane-wave sources: S[c][s][t] = psi_{c,t}(p_s) exactly.
+template <typename R>
+__global__ void gather_kernel(const int* __restrict__ index, int ns, const void* __restrict__ psi, int nt,
+                              int nconf, long vol, double* __restrict__ S) {
+  long total = (long)nconf * ns * nt;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    long conf = e / ((long)ns * nt);
+    int s = (int)((e / nt) % ns), t = (int)(e % nt);
+    cplx<R> q = ld<R>(psi, ((conf * nt + t) * vol) + index[s]);
+    S[2 * e] = (double)q.re;
+    S[2 * e + 1] = (double)q.im;
+  }
+}
+
+// ------------------------------------------------------------ pair matrix
+// One block per (configuration, s, t): phi = sum_i w_i psi1_s(i) psi2_t(opp(i)).
+template <typename R>
+__global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1, const void* __restrict__ psi2,
+                                                   int n, long vol, const double* __restrict__ w,
+                                                   const int* __restrict__ opp, double* __restrict__ phi) {
+  const long e = blockIdx.x;  // (conf * n + s) * n + t
+  const long conf = e / ((long)n * n);
+  const int s = (int)((e / n) % n), t = (int)(e % n);
+  const char* a = reinterpret_cast<const char*>(psi1) + (size_t)(conf * n + s) * vol * 2 * sizeof(R);
+  const char* b = reinterpret_cast<const char*>(psi2) + (size_t)(conf * n + t) * vol * 2 * sizeof(R);
+  double re = 0.0, im = 0.0;
+  for (long i = threadIdx.x; i < vol; i += blockDim.x) {
+    cplx<R> x = ld<R>(a, i), y = ld<R>(b, opp[i]);
+    double wi = w[i];
+    re += ((double)x.re * y.re - (double)x.im * y.im) * wi;
+    im += ((double)x.re * y.im + (double)x.im * y.re) * wi;
+  }
+  __shared__ double red[2][8];
+  for (int off = 16; off > 0; off >>= 1) {
+    re += __shfl_down_sync(0xffffffffu, re, off);
+    im += __shfl_down_sync(0xffffffffu, im, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = re;
+    red[1][threadIdx.x >> 5] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sr = 0, si = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      sr += red[0][k];
+      si += red[1][k];
+    }
+    phi[2 * e] = sr;
+    phi[2 * e + 1] = si;
+  }
+}
+
+// ------------------------------------------------------------------- LU
+struct dc {
+  double re, im;
+};
+__device__ __forceinline__ dc dmul(dc a, dc b) { return dc{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ double dabs(dc a) { return hypot(a.re, a.im); }
+__device__ __forceinline__ dc drecip(dc b) {
+  // 1 / b with Smith's scaling
+  if (fabs(b.re) >= fabs(b.im)) {
+    double r = b.im / b.re, d = b.re + b.im * r;
+    return dc{1.0 / d, -r / d};
+  }
+  double r = b.re / b.im, d = b.re * r + b.im;
+  return dc{r / d, -1.0 / d};
+}
+
+// Crout LU with implicit-scaled partial pivoting (src/utils/ludcmp.C:9-65)
+// on the n x n matrix a (row-major, stride n).  Returns the permutation
+// parity d, or 0 when a row is all zero (the reference exits there).
+__device__ double ludcmp_dev(dc* a, int n, double* vv) {
+  double d = 1.0;
+  for (int i = 0; i < n; ++i) {
+    double big = 0.0;
+    for (int j = 0; j < n; ++j) {
+      double t = dabs(a[n * i + j]);
+      if (t > big) big = t;
+    }
+    if (big == 0.0) return 0.0;
+    vv[i] = 1.0 / big;
+  }
+  int imax = 0;
+  for (int j = 0; j < n; ++j) {
+    for (int i = 0; i < j; ++i) {
+      dc sum = a[n * i + j];
+      for (int k = 0; k < i; ++k) {
+        dc p = dmul(a[n * i + k], a[n * k + j]);
+        sum.re -= p.re;
+        sum.im -= p.im;
+      }
+      a[n * i + j] = sum;
+    }
+    double big = 0.0;
+    for (int i = j; i < n; ++i) {
+      dc sum = a[n * i + j];
+      for (int k = 0; k < j; ++k) {
+        dc p = dmul(a[n * i + k], a[n * k + j]);
+        sum.re -= p.re;
+        sum.im -= p.im;
+      }
+      a[n * i + j] = sum;
+      double dum = vv[i] * dabs(sum);
+      if (dum >= big) {
+        big = dum;
+        imax = i;
+      }
+    }
+    if (j != imax) {
+      for (int k = 0; k < n; ++k) {
+        dc t = a[n * imax + k];
+        a[n * imax + k] = a[n * j + k];
+        a[n * j + k] = t;
+      }
+      d = -d;
+      vv[imax] = vv[j];
+    }
+    if (dabs(a[n * j + j]) == 0.0) a[n * j + j] = dc{1.0e-20, 0.0};
+    dc r = drecip(a[n * j + j]);
+    for (int i = j + 1; i < n; ++i) a[n * i + j] = dmul(a[n * i + j], r);
+  }
+  return d;
+}
+
+// One thread per (matrix, measured minor).  Scratch: per thread n*n complex
+// + n doubles in global memory (L2-resident).
+__global__ void slater_dets_kernel(const double* __restrict__ S, const double* __restrict__ psi1, int N, int nconf,
+                                   int mode, int log_det, double* __restrict__ out, double* scratch,
+                                   long out_conf_stride, long out_offset) {
+  const int nmeas = mode ? 2 * N : N;
+  const long total = (long)nconf * nmeas;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long c = e / nmeas;
+    const int m = (int)(e % nmeas);
+    const int n = mode ? m / 2 + 1 : m + 1;
+    const int t0 = (mode && (m % 2 == 0)) ? n - 1 : -1;
+    dc* a = reinterpret_cast<dc*>(scratch + e * (2L * N * N + N));
+    double* vv = scratch + e * (2L * N * N + N) + 2L * N * N;
+    const dc* Sc = reinterpret_cast<const dc*>(S) + c * (long)N * N;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) a[n * i + j] = Sc[(long)N * i + j];
+    if (t0 >= 0) {
+      // SlaterDet2::Run column t0 from psi1[s + t0*N] (slater_det2.C:102-106)
+      const dc* P = reinterpret_cast<const dc*>(psi1) + c * (long)N * N;
+      for (int i = 0; i < n; ++i) a[n * i + t0] = P[i + (long)t0 * N];
+    }
+    double d = ludcmp_dev(a, n, vv);
+    dc r;
+    if (!log_det) {
+      r = dc{d, 0.0};
+      for (int i = 0; i < n; ++i) r = dmul(r, a[n * i + i]);
+    } else {
+      // log(d) + sum log(U_ii), principal branches (slater_det.C:102-109)
+      r = dc{log(fabs(d)), d < 0 ? 3.14159265358979323846 : 0.0};
+      for (int i = 0; i < n; ++i) {
+        r.re += log(dabs(a[n * i + i]));
+        r.im += atan2(a[n * i + i].im, a[n * i + i].re);
+      }
+    }
+    if (d == 0.0) r = dc{nan(""), nan("")};  // singular: flagged to the host
+    double* o = out + c * out_conf_stride + out_offset + 2L * m;
+    o[0] = r.re;
+    o[1] = r.im;
+  }
+}
+
+size_t slater_dets_scratch_bytes(int N, int nconf, int mode) {
+  const int nmeas = mode ? 2 * N : N;
+  return sizeof(double) * (size_t)nconf * nmeas * (2L * N * N + N);
+}
+
+// scr: caller-owned scratch of slater_dets_scratch_bytes(), or NULL for the
+// context's scratch.
+nrcps_status slater_dets_impl(nrcps_context* ctx, const double* S, const double* psi1, int N, int nconf, int mode,
+                              int log_det, double* out, long out_conf_stride, long out_offset, double* scr) {
+  const int nmeas = mode ? 2 * N : N;
+  const long total = (long)nconf * nmeas;
+  if (total == 0) return NRCPS_OK;
+  if (!scr) {
+    nrcps_status st;
+    scr = (double*)scratch(ctx, slater_dets_scratch_bytes(N, nconf, mode), &st);
+    if (!scr) return st;
+  }
+  slater_dets_kernel<<<grid_for(total, 64, 1L << 20), 64, 0, ctx->stream>>>(S, psi1, N, nconf, mode, log_det, out,
+                                                                             scr, out_conf_stride, out_offset);
+  ctx->launches++;
+  return check_launch(ctx, "slater_dets_kernel");
+}
+
+nrcps_status overlap_impl(nrcps_context* ctx, const double* src, int ns, const void* psi, int nt, int nconf,
+                          long vol, nrcps_precision prec, double* S) {
+  long blocks = (long)nconf * nt;
+  if (blocks == 0) return NRCPS_OK;
+  if (prec == NRCPS_F64) overlap_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(src, ns, psi, nt, vol, S);
+  else overlap_kernel<float><<<(unsigned)blocks, 256, 0, ctx->stream>>>(src, ns, psi, nt, vol, S);
+  ctx->launches++;
+  return check_launch(ctx, "overlap_kernel");
+}
+
+nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const void* psi, int nt, int nconf, long vol,
+                         nrcps_precision prec, double* S) {
+  long total = (long)nconf * ns * nt;
+  if (total == 0) return NRCPS_OK;
+  unsigned g = grid_for(total, 256, (long)ctx->sm_count * 8);
+  if (prec == NRCPS_F64) gather_kernel<double><<<g, 256, 0, ctx->stream>>>(index, ns, psi, nt, nconf, vol, S);
+  else gather_kernel<float><<<g, 256, 0, ctx->stream>>>(index, ns, psi, nt, nconf, vol, S);
+  ctx->launches++;
+  return check_launch(ctx, "gather_kernel");
+}
+
+nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
+                       const double* w, const int* opp, nrcps_precision prec, double* phi) {
+  long blocks = (long)nconf * n * n;
+  if (blocks == 0) return NRCPS_OK;
+  if (prec == NRCPS_F64) pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
+  else pair_kernel<float><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
+  ctx->launches++;
+  return check_launch(ctx, "pair_kernel");
+}
+
+}  // namespace nrcps
+
+using namespace nrcps;
+
+extern "C" nrcps_status nrcps_overlap(nrcps_context* ctx, const double* dev_src, int ns, const void* dev_psi, int nt,
+                                      int nconf, long vol, nrcps_precision prec, double* dev_S) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  NRCPS_REQUIRE(ctx, dev_src && dev_psi && dev_S && ns >= 0 && nt >= 0 && nconf >= 0 && vol > 0,
+                "nrcps_overlap: bad arguments");
+  return overlap_impl(ctx, dev_src, ns, dev_psi, nt, nconf, vol, prec, dev_S);
+}
+
+extern "C" nrcps_status nrcps_overlap_planewave(nrcps_context* ctx, const int* dev_index, int ns, const void* dev_psi,
+                                                int nt, int nconf, long vol, nrcps_precision prec, double* dev_S) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  NRCPS_REQUIRE(ctx, dev_index && dev_psi && dev_S && ns >= 0 && nt >= 0 && nconf >= 0 && vol > 0,
+                "nrcps_overlap_planewave: bad arguments");
+  return gather_impl(ctx, dev_index, ns, dev_psi, nt, nconf, vol, prec, dev_S);
+}
+
+extern "C" nrcps_status nrcps_pair_matrix(nrcps_context* ctx, const void* dev_psi1, const void* dev_psi2, int n,
+                                          int nconf, long vol, const double* dev_w, const int* dev_opposite,
+                                          nrcps_precision prec, double* dev_phi) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_w && dev_opposite && dev_phi && n >= 0 && nconf >= 0 && vol > 0,
+                "nrcps_pair_matrix: bad arguments");
+  return pair_impl(ctx, dev_psi1, dev_psi2, n, nconf, vol, dev_w, dev_opposite, prec, dev_phi);
+}
+
+extern "C" nrcps_status nrcps_slater_dets(nrcps_context* ctx, const double* dev_S, const double* dev_psi1, int N,
+                                          int nconf, int mode, int log_det, double* dev_out) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  NRCPS_REQUIRE(ctx, dev_S && dev_out && N > 0 && nconf >= 0 && (mode == 0 || (mode == 1 && dev_psi1)),
+                "nrcps_slater_dets: bad arguments");
+  const int nmeas = mode ? 2 * N : N;
+  return slater_dets_impl(ctx, dev_S, dev_psi1, N, nconf, mode, log_det, dev_out, 2L * nmeas, 0, nullptr);
+}

@@ -339,6 +339,7 @@ int run_ensemble(const KV& kv, bool timed_only) {
   long slices_done = 0;
   double t0 = now_s();
   const double budget = getd(kv, "budget_s", 1e30);
+  const long max_slices = getl(kv, "max_slices", -1);  // bounded sample for timing
   vector<complex<double> > row(nmeas);
   vector<complex<double> > smat((size_t)N * N), psi1((size_t)N * N);
 
@@ -377,7 +378,9 @@ int run_ensemble(const KV& kv, bool timed_only) {
       propagator.Run(hamiltonians);
       lattice.Refresh();
       ++slices_done;
+      if (max_slices > 0 && slices_done >= max_slices) break;
     }
+    if (max_slices > 0 && slices_done >= max_slices) break;
     if (timed_only && now_s() - t0 > budget) break;
   }
   double el = now_s() - t0;

@@ -1,0 +1,284 @@
+"""GPU parity: every hot-path operation of libnrcps_b200 against the oracle
+(the CPU restatement pinned to the reference) on identical inputs.
+
+Tolerances: RNG and field integers bit-exact; FP64 propagation, overlaps and
+determinants within 1e-12 relative; FP32 propagation within 1e-5 relative on
+the correlators (the BASELINE target for the fast mode).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+nb = pytest.importorskip("nrcps_b200")
+
+FP64_REL = 1e-12
+FP32_REL = 1e-5
+
+
+def rel_err(got, ref):
+    got, ref = np.asarray(got), np.asarray(ref)
+    return np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300))
+
+
+def max_norm_err(got, ref):
+    got, ref = np.asarray(got), np.asarray(ref)
+    return np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return nb.default_context()
+
+
+# ------------------------------------------------------------------ RNG
+@pytest.mark.parametrize("kind", ["RANLXS0", "RANLXS1", "RANLXS2", "RANLXD1", "RANLXD2", "RAN2"])
+def test_uniforms_bit_exact_vs_reference(golden, ctx, kind):
+    g = golden("rng_streams.npz")
+    assert np.array_equal(nb.uniforms(kind, 1234, 600, 0, ctx).cpu().numpy(), g[f"{kind}_seed1234_skip0"])
+    assert np.array_equal(nb.uniforms(kind, 1234, 200, 200_000, ctx).cpu().numpy(),
+                          g[f"{kind}_seed1234_skip200000"])
+
+
+@pytest.mark.parametrize("kind", ["RANLXS2", "RANLXD1"])
+def test_uniforms_bit_exact_long_windows(ctx, kind):
+    rs = np.random.default_rng(3)
+    for off in [0, 95, 96, 1, 4095, 77777, 1_000_003]:
+        n = int(rs.integers(1, 50_000))
+        got = nb.uniforms(kind, 4321, n, off, ctx).cpu().numpy()
+        assert np.array_equal(got, O.uniforms(kind, 4321, n, skip=off)), off
+
+
+def test_known_answer_on_device(golden, ctx):
+    k = golden("ranlx_kat.npz")
+    u = nb.uniforms("RANLXS0", 32767, 96, int(k["ranlxs0_seed32767_first_index"]), ctx).cpu().numpy()
+    assert np.array_equal(u * 2.0 ** 24, k["ranlxs0_seed32767_times_2p24"])
+    u = nb.uniforms("RANLXD1", 32767, 48, int(k["ranlxd1_seed32767_first_index"]), ctx).cpu().numpy()
+    assert np.array_equal(u * 2.0 ** 48, k["ranlxd1_seed32767_times_2p48"])
+
+
+def test_fields_bit_exact_vs_reference(golden, ctx):
+    g = golden("fields.npz")
+    for key in g.files:
+        field, kind, seed, L = key.split("_")
+        ref = g[key]
+        got, off = nb.draw_fields(kind, int(seed[4:]), field, int(L[1:]) ** 3, ref.shape[0], 0, ctx)
+        assert np.array_equal(got.cpu().numpy(), ref), key
+
+
+@pytest.mark.parametrize("field", ["GAUSS", "COMPLEXGAUSS"])
+def test_gauss_fields_stream_exact(ctx, field):
+    """Uniform consumption is bit-exact; values agree to a few ulp (log on the device)."""
+    vol, slices = 4096, 5
+    got, off = nb.draw_fields("RANLXS2", 99, field, vol, slices, 0, ctx)
+    r = O.Rng("RANLXS2", 99)
+    ref = r.fields(field, vol, slices)
+    assert np.max(np.abs(got.cpu().numpy() - ref)) <= 4e-15 * np.max(np.abs(ref))
+    # the next slice continues from the same stream position
+    nxt, _ = nb.draw_fields("RANLXS2", 99, field, vol, 1, off, ctx)
+    assert np.max(np.abs(nxt.cpu().numpy()[0] - r.fields(field, vol, 1)[0])) < 1e-13
+
+
+def test_z2_bits(ctx):
+    first, count = 96 * 7 + 5, 100_000
+    bits = nb.draw_z2_bits("RANLXS2", 11, first, count, ctx).cpu().numpy().view(np.uint32)
+    u = O.uniforms("RANLXS2", 11, count, skip=first)
+    want = (np.floor(2 * u) >= 1)
+    got = ((bits[np.arange(count) >> 5] >> (np.arange(count) & 31)) & 1).astype(bool)
+    assert np.array_equal(got, want)
+
+
+# ------------------------------------------------------------------ FFT
+@pytest.mark.parametrize("dims", [(4, 4, 4), (8, 6, 12), (16, 16, 16), (24, 24, 24), (32, 32, 32), (48, 16, 2)])
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_fft3d_matches_numpy(ctx, dims, precision):
+    rs = np.random.default_rng(5)
+    a = rs.standard_normal((3,) + dims) + 1j * rs.standard_normal((3,) + dims)
+    f = nb.Fourier(3, dims, precision, ctx)
+    f.b.copy_(torch.from_numpy(a))
+    f.forward()
+    tol = 1e-13 if precision == "f64" else 2e-6
+    assert max_norm_err(f.b.cpu().numpy(), np.fft.fftn(a, axes=(1, 2, 3))) < tol
+    f.b.copy_(torch.from_numpy(a))
+    f.backward()
+    assert max_norm_err(f.b.cpu().numpy(), np.fft.ifftn(a, axes=(1, 2, 3)) * np.prod(dims)) < tol
+
+
+# ---------------------------------------------------------- propagation
+def _steps_reference(golden_name, golden):
+    g = golden(golden_name)
+    args = json.loads(str(g["args"]))
+    return g, args
+
+
+def test_class_api_steps_match_reference_props(golden, ctx):
+    """Propagator::Run([K, I, K]) through the class API against the reference's
+    own per-step orbitals (multi-coupling interaction, ranlxd fields drawn on
+    the device)."""
+    g, args = _steps_reference("ensemble_multicoupling.npz", golden)
+    dims = (8, 8, 8)
+    couplings = [float(c) for c in args["couplings"].split(",")]
+    rng = nb.Random(args["rng"], int(args["seed"]))
+    lat = nb.Lattice(dims, rng, "ZTWO", ctx)
+    inter = nb.Interaction(lat, 1.0, couplings, 1.0, float(args["cutoff"]))
+    kin = nb.Kinetic(dims, "PERFECT", 1.0, 0.5, float(args["cutoff"]), ctx)
+    N = g["sources"].shape[0]
+    prop = nb.Propagator(N, dims, "f64", ctx)
+    for n in range(N):
+        prop.set(g["sources"][n], n)
+    for t in range(g["props"].shape[0]):
+        got = prop.get().b.reshape(N, -1).cpu().numpy()
+        assert max_norm_err(got, g["props"][t]) < FP64_REL, t
+        for h in (kin, inter, kin):
+            h.initialize()
+        prop.run([kin, inter, kin])
+        lat.refresh()
+
+
+def test_potential_steps_match_oracle(ctx):
+    dims = (8, 8, 8)
+    pot = nb.Potential(dims, 0.005, 0.5, "EXP", ctx)
+    kin = nb.Kinetic(dims, "PERFECT", 1.0, 0.5, 0.99999, ctx)
+    rng = nb.Random("RANLXS2", 31)
+    lat = nb.Lattice(dims, rng, "ZTWO", ctx)
+    inter = nb.Interaction(lat, 1.0, [0.019894367886486918], 1.0, 0.99999)
+    rs = np.random.default_rng(9)
+    psi0 = rs.standard_normal((3, 512)) + 1j * rs.standard_normal((3, 512))
+    prop = nb.Propagator(3, dims, "f64", ctx)
+    for n in range(3):
+        prop.set(psi0[n], n)
+    ref = psi0.copy()
+    xi = O.kinetic_xi(dims, "PERFECT", 1.0, 0.5, (0.99999 * O.PI) ** 2)
+    potv = O.potential_table(dims, 0.005, 0.5, "EXP")
+    itab = O.interaction_table(dims, 1.0, [0.019894367886486918], 1.0, (0.99999 * O.PI) ** 2)
+    fields = O.field_slices("RANLXS2", 31, "ZTWO", 512, 4)
+    for t in range(4):
+        inter.initialize()
+        prop.run([kin, pot, inter, pot, kin])
+        lat.refresh()
+        fld = O.interaction_initialize(dims, fields[t], itab)
+        ref = O.kinetic_evolve(ref, xi)
+        ref = O.potential_evolve(dims, ref, potv)
+        ref = O.interaction_evolve(dims, ref, fld)
+        ref = O.potential_evolve(dims, ref, potv)
+        ref = O.kinetic_evolve(ref, xi)
+        assert max_norm_err(prop.get().b.reshape(3, -1).cpu().numpy(), ref) < FP64_REL, t
+
+
+# ---------------------------------------------------------- measurement
+def test_overlap_pair_and_dets_match_oracle(golden, ctx):
+    g = golden("ensemble_trapped.npz")
+    src = g["sources"]
+    N, vol = src.shape
+    psi = g["props"][2]  # reference orbitals after two steps
+    S = nb.overlap(torch.from_numpy(src).to(ctx.device), torch.from_numpy(psi).to(ctx.device).reshape(1, N, vol), ctx)
+    S_ref = O.project(src, psi)
+    assert rel_err(S.cpu().numpy()[0], S_ref) < FP64_REL
+    w, opp = O.two_body_tables((8, 8, 8), "TGND", "STANDARD", 1.0, 0.176776695, (0.99999 * O.PI) ** 2)
+    tb = nb.TwoBody((8, 8, 8), "TGND", "STANDARD", 1.0, 0.176776695, 0.99999, ctx)
+    p = torch.from_numpy(psi).to(ctx.device).reshape(1, N, vol)
+    phi = tb.run_matrix(p, p).cpu().numpy()[0]
+    phi_ref = O.pair_matrix(psi, psi, w, opp)
+    assert max_norm_err(phi, phi_ref) < FP64_REL
+    dets = nb.slater_dets(torch.from_numpy(phi_ref).to(ctx.device).reshape(1, N, N),
+                          torch.from_numpy(S_ref).to(ctx.device).reshape(1, N, N), mode=1, ctx=ctx).cpu().numpy()[0]
+    for n in range(N):
+        assert rel_err(dets[2 * n + 1], O.minor_det(phi_ref, n + 1)) < FP64_REL
+        assert rel_err(dets[2 * n], O.minor_det(phi_ref, n + 1, t0=n, psi1=S_ref)) < FP64_REL
+
+
+def test_lu_cases_match_reference(golden, ctx):
+    g = golden("lu_cases.npz")
+    for i, ref in enumerate(g["dets"]):
+        m = g[f"m{i}"]
+        n = m.shape[0]
+        d = nb.slater_dets(torch.from_numpy(m).to(ctx.device).reshape(1, n, n), ctx=ctx).cpu().numpy()[0, n - 1]
+        assert abs(d - ref) <= 1e-12 * abs(ref) + 1e-300, i
+
+
+def test_log_det(ctx):
+    rs = np.random.default_rng(2)
+    m = rs.standard_normal((6, 6)) + 1j * rs.standard_normal((6, 6))
+    d = nb.slater_dets(torch.from_numpy(m).to(ctx.device).reshape(1, 6, 6), log=True, ctx=ctx).cpu().numpy()[0]
+    for n in range(1, 7):
+        ref = O.minor_det(m, n, log=True)
+        assert abs(np.exp(d[n - 1]) - np.exp(ref)) < 1e-12 * abs(np.exp(ref))
+
+
+# ------------------------------------------------------------- ensemble
+def _job_from_golden(args, precision):
+    j = nb.EnsembleJob(L=int(args["L"]), T=int(args["T"]), n_conf=int(args["configs"]), rng=args.get("rng", "RANLXS2"),
+                       seed=int(args["seed"]), field=args.get("field", "ZTWO"), precision=precision,
+                       cutoff=float(args["cutoff"]), couplings=[float(c) for c in str(args["couplings"]).split(",")])
+    if args.get("potential"):
+        j.potential, j.kappa, j.pot_type = True, float(args["kappa"]), args["ptype"]
+    if args.get("mode") == "slater2":
+        j.mode, j.wavefunc = "slater2", args["wavefunc"]
+        j.wf_disp, j.wf_lambda = args["tb_disp"], float(args["tb_lambda"])
+    return j
+
+
+@pytest.mark.parametrize("name", ["ensemble_config1.npz", "ensemble_multicoupling.npz", "ensemble_gauss.npz",
+                                  "ensemble_trapped.npz"])
+def test_ensemble_fp64_matches_reference(golden, ctx, name):
+    g = golden(name)
+    args = json.loads(str(g["args"]))
+    job = _job_from_golden(args, "f64")
+    if "momenta" in g.files and args.get("sources", "mom") == "mom":
+        idx, _, _ = nb.momenta(job.dims, "PERFECT", 1.0, float(args["ef"]), job.cutoff)
+        ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
+    else:
+        ens = nb.Ensemble(job, sources=g["sources"], ctx=ctx)
+    dets = ens.run(0).cpu().numpy()
+    ref = g["dets"]
+    assert dets.shape == ref.shape
+    assert rel_err(dets, ref) < FP64_REL
+
+
+def test_ensemble_fp32_config1(golden, ctx):
+    g = golden("ensemble_config1.npz")
+    args = json.loads(str(g["args"]))
+    job = _job_from_golden(args, "f32")
+    idx, _, _ = nb.momenta(job.dims, "PERFECT", 1.0, 0.1, job.cutoff)
+    dets = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx).run(0).cpu().numpy()
+    assert rel_err(dets, g["dets"]) < FP32_REL
+
+
+def test_ensemble_later_configurations_use_later_fields(ctx):
+    """Configurations 3..4 of a run from the stream start equal a run that starts at 3."""
+    job = nb.EnsembleJob(L=8, T=6, n_conf=5, fermi_energy=0.35, precision="f64")
+    idx, _, _ = nb.momenta(job.dims, "PERFECT", 1.0, 0.35, job.cutoff)
+    full = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx).run(0).cpu().numpy()
+    job2 = nb.EnsembleJob(L=8, T=6, n_conf=2, fermi_energy=0.35, precision="f64")
+    part = nb.Ensemble(job2, plane_wave_index=idx, ctx=ctx).run(3).cpu().numpy()
+    assert np.array_equal(full[3:5], part)
+
+
+def test_free_gas_analytic_on_device(ctx):
+    """Kinetic only: det S_n(tau) = prod_{i<=n} xi(p_i)^(-tau) (tests/free_gas)."""
+    dims = (16, 16, 16)
+    idx, _, _ = nb.momenta(dims, "PERFECT", 1.0, 0.1, 2.0)
+    xi = nb.kinetic_table(dims, "PERFECT", 1.0, 0.5, 2.0)
+    kin = nb.Kinetic(dims, "PERFECT", 1.0, 0.5, 2.0, ctx)
+    prop = nb.Propagator(len(idx), dims, "f64", ctx)
+    for n, j in enumerate(idx):
+        v = np.zeros(4096, complex)
+        v[j] = 1
+        prop.set(v, n)
+    src = torch.zeros((len(idx), 4096), dtype=torch.complex128, device=ctx.device)
+    src[torch.arange(len(idx)), torch.as_tensor(idx, dtype=torch.long)] = 1
+    for tau in range(1, 5):
+        prop.run([kin, kin])
+        S = nb.overlap(src, prop.get().b.reshape(1, len(idx), -1), ctx)
+        d = nb.slater_dets(S, ctx=ctx).cpu().numpy()[0]
+        for n in range(1, len(idx) + 1):
+            expect = np.prod(xi[idx[:n]] ** (-2.0 * tau))
+            assert abs(d[n - 1] / expect - 1) < 1e-13

@@ -80,6 +80,15 @@ nrcps_status nrcps_set_stream(nrcps_context *ctx, void *stream);
 nrcps_status nrcps_synchronize(nrcps_context *ctx);
 /* Library version string, e.g. "nrcps_b200 0.1 sm_100a". */
 const char *nrcps_version(void);
+/* Tuning options of a context (no counterpart in the reference, whose launch
+ * shape is the compile-time BLOCKS/THREADS of include/config.h:30-33):
+ *   "propagate.fused"  1 (default): single-pass cluster kernel where one
+ *                      exists for the shape; 0: five pencil passes;
+ *   "fused.cluster"    0 (default): autotuned cluster size; else force it. */
+nrcps_status nrcps_set_option(nrcps_context *ctx, const char *name, long value);
+/* Times every fused-kernel cluster size for (prec, L) on this device and
+ * keeps the fastest for later calls; *cluster receives it (may be NULL). */
+nrcps_status nrcps_autotune(nrcps_context *ctx, nrcps_precision prec, int L, int *cluster);
 
 /* ----------------------------------------------------- host-side tables
  * Replace the reference's host constructors' table builds so that callers

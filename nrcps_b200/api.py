@@ -68,6 +68,16 @@ class Context:
     def synchronize(self) -> None:
         self.check(lib().nrcps_synchronize(self.handle), "synchronize")
 
+    def set_option(self, name: str, value: int) -> None:
+        """nrcps_set_option: "propagate.fused" (1/0), "fused.cluster" (0 = autotuned)."""
+        self.check(lib().nrcps_set_option(self.handle, name.encode(), int(value)), "set_option")
+
+    def autotune(self, precision: str, L: int) -> int:
+        """Times the fused kernel's cluster sizes for (precision, L); returns the chosen one."""
+        c = ctypes.c_int()
+        self.check(lib().nrcps_autotune(self.handle, _prec(precision), L, ctypes.byref(c)), "autotune")
+        return c.value
+
     def close(self) -> None:
         if self.handle:
             lib().nrcps_destroy(self.handle)
@@ -402,6 +412,25 @@ class TwoBody:
     def run(self, prop1: torch.Tensor, prop2: torch.Tensor) -> complex:
         """TwoBody::Run(Float*, Float*)."""
         return complex(self.run_matrix(prop1.reshape(1, 1, -1), prop2.reshape(1, 1, -1))[0, 0, 0].item())
+
+
+def propagate(psi: torch.Tensor, batch: int, kinv: torch.Tensor, field: torch.Tensor, a: float,
+              field_mode: int = 1, off0: int = 0, conf_stride: Optional[int] = None,
+              pos: Optional[torch.Tensor] = None, ctx: Optional[Context] = None) -> None:
+    """One fused Propagator::Run step on psi [nconf*batch, X, Y, Z] (in place):
+    psi <- k . B[w . F[k . psi]], k = kinv (FP64, V), w from `field`
+    (field_mode 1: Z2 bits, 2: interleaved complex phi, 0: complex fld)."""
+    ctx = ctx or default_context()
+    dims = tuple(psi.shape[-3:])
+    vol = int(np.prod(dims))
+    nconf = psi.shape[0] // batch
+    pf = C.PositionFactor()
+    pf.field_mode, pf.dev_field, pf.bit0 = field_mode, field.data_ptr(), off0
+    pf.conf_stride = vol if conf_stride is None else conf_stride
+    pf.a, pf.dev_pos = a, (pos.data_ptr() if pos is not None else None)
+    prec = C.F64 if psi.dtype == torch.complex128 else C.F32
+    ctx.check(lib().nrcps_propagate(ctx.handle, _ptr(psi), batch, nconf, _ip(_dims(dims)), _ptr(kinv),
+                                    ctypes.byref(pf), prec), "propagate")
 
 
 def overlap(src: torch.Tensor, psi: torch.Tensor, ctx: Optional[Context] = None) -> torch.Tensor:

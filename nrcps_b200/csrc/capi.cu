@@ -73,6 +73,7 @@ extern "C" nrcps_status nrcps_destroy(nrcps_context* ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->gen_args) cudaFree(ctx->gen_args);
+  if (ctx->kin_f32) cudaFree(ctx->kin_f32);
   delete ctx;
   return NRCPS_OK;
 }
@@ -85,6 +86,30 @@ extern "C" nrcps_status nrcps_set_stream(nrcps_context* ctx, void* stream) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
   ctx->stream = (cudaStream_t)stream;
   return NRCPS_OK;
+}
+
+namespace nrcps {
+nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster);
+}
+
+extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, long value) {
+  if (!ctx || !name) return NRCPS_ERR_INVALID_ARGUMENT;
+  std::string n(name);
+  if (n == "propagate.fused") {
+    ctx->fused_enabled = value != 0;
+  } else if (n == "fused.cluster") {
+    if (value < 0 || value > 16) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.cluster out of range");
+    ctx->fused_cluster = (int)value;
+  } else {
+    return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "unknown option %s", name);
+  }
+  return NRCPS_OK;
+}
+
+extern "C" nrcps_status nrcps_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* cluster) {
+  if (!ctx || L <= 0 || L >= 64) return NRCPS_ERR_INVALID_ARGUMENT;
+  if (cluster) *cluster = 0;
+  return fused_autotune(ctx, prec, L, cluster);
 }
 
 extern "C" nrcps_status nrcps_synchronize(nrcps_context* ctx) {

@@ -63,6 +63,12 @@ struct Context {
   void* gen_args = nullptr;
   int gen_kind = -1;
   long gen_seed = 0;
+  // Tuning options (nrcps_set_option).
+  int fused_enabled = 1;  // single-pass cluster kernel where a variant exists
+  int fused_cluster = 0;  // 0: autotuned / default cluster size
+  // FP32 copy of a kinetic table for nrcps_propagate(F32).
+  float* kin_f32 = nullptr;
+  long kin_f32_len = 0;
 };
 
 }  // namespace nrcps

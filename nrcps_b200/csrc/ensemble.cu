@@ -26,6 +26,9 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
                          nrcps_precision prec, double* S);
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
                        const double* w, const int* opp, nrcps_precision prec, double* phi);
+nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
+                            const float* kin_f32, const nrcps_position_factor* w, nrcps_precision prec);
+nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster);
 }  // namespace nrcps
 
 struct nrcps_ensemble {
@@ -38,6 +41,7 @@ struct nrcps_ensemble {
   double* src = nullptr;
   int* pw_index = nullptr;
   double* kinv = nullptr;
+  float* kinv_f = nullptr;
   double* pos = nullptr;
   double* itab = nullptr;
   double* w = nullptr;
@@ -179,7 +183,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       pf.bit0 = (uint64_t)t * vol;
       pf.conf_stride = (uint64_t)T * vol;
     }
-    NRCPS_TRY(nrcps_propagate(ctx, e->psi, N, nc, d3, e->kinv, &pf, prec));
+    NRCPS_TRY(propagate_impl(ctx, e->psi, N, nc, d3, e->kinv, e->kinv_f, &pf, prec));
   }
   e->launches_per_run = ctx->launches - n0;
   return NRCPS_OK;
@@ -225,6 +229,13 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   std::vector<double> h(V);
   for (long i = 0; i < V; ++i) h[i] = 1.0 / kin_xi[i];
   if ((st = upload(ctx, e->kinv, h.data(), 8 * V))) return fail(st);
+  {
+    std::vector<float> hf(V);
+    for (long i = 0; i < V; ++i) hf[i] = (float)h[i];
+    if ((st = dalloc(ctx, &e->kinv_f, 4 * V)) || (st = upload(ctx, e->kinv_f, hf.data(), 4 * V))) return fail(st);
+  }
+  if (job->dims[0] == job->dims[1] && job->dims[1] == job->dims[2] && job->dims[0] < 64)
+    fused_autotune(ctx, (nrcps_precision)job->precision, job->dims[0], nullptr);
   if (job->use_potential) {
     // [K,V,I,V,K] = K B diag(V^2 v^2 fld) F K since F B = V (unnormalised transforms)
     for (long i = 0; i < V; ++i) h[i] = ((double)V * pot[i]) * ((double)V * pot[i]);
@@ -329,7 +340,7 @@ extern "C" nrcps_status nrcps_ensemble_destroy(nrcps_ensemble* e) {
   if (e->ctx) cudaStreamSynchronize(e->ctx->stream);
   if (e->exec) cudaGraphExecDestroy(e->exec);
   if (e->graph) cudaGraphDestroy(e->graph);
-  void* bufs[] = {e->psi, e->src, e->pw_index, e->kinv, e->pos, e->itab, e->w, e->opp,
+  void* bufs[] = {e->psi, e->src, e->pw_index, e->kinv, e->kinv_f, e->pos, e->itab, e->w, e->opp,
                   e->bits, e->phi, e->fld, e->S, e->P1, e->lu_scr};
   for (void* b : bufs)
     if (b) cudaFree(b);

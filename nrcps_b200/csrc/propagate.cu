@@ -302,6 +302,15 @@ extern "C" nrcps_status nrcps_interaction_initialize(nrcps_context* ctx, const d
 }
 
 namespace nrcps {
+bool fused_supported(nrcps_precision prec, const int d[3]);
+nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const void* kin_table,
+                        nrcps_precision prec, const nrcps_position_factor* w, int cluster);
+
+__global__ void to_f32_kernel(float* dst, const double* src, long n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
 template <typename R>
 static nrcps_status propagate_t(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3],
                                 const double* kin, const FieldArgs& f) {
@@ -316,6 +325,47 @@ static nrcps_status propagate_t(nrcps_context* ctx, void* psi, int batch, int nc
 }
 }  // namespace nrcps
 
+namespace nrcps {
+// Propagator step for the ensemble and the C ABI.  kin_f32 may be NULL (then
+// an FP32 copy of kin is made in the context when the FP32 fused kernel runs).
+nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
+                            const float* kin_f32, const nrcps_position_factor* w, nrcps_precision prec) {
+  if (ctx->fused_enabled && fused_supported(prec, d)) {
+    const void* table = kin;
+    if (prec == NRCPS_F32) {
+      if (!kin_f32) {
+        const long V = vol_of(d);
+        if (ctx->kin_f32_len < V) {
+          if (ctx->kin_f32) cudaFree(ctx->kin_f32);
+          ctx->kin_f32 = nullptr;
+          ctx->kin_f32_len = 0;
+          NRCPS_TRY(check_cuda(ctx, cudaMalloc((void**)&ctx->kin_f32, sizeof(float) * V), "cudaMalloc(kin f32)"));
+          ctx->kin_f32_len = V;
+        }
+        to_f32_kernel<<<grid_for(V, 256), 256, 0, ctx->stream>>>(ctx->kin_f32, kin, V);
+        ctx->launches++;
+        NRCPS_TRY(check_launch(ctx, "to_f32_kernel"));
+        kin_f32 = ctx->kin_f32;
+      }
+      table = kin_f32;
+    }
+    nrcps_status st = fused_step(ctx, psi, batch, nconf, d, table, prec, w, ctx->fused_cluster);
+    if (st != NRCPS_ERR_UNSUPPORTED) return st;
+  }
+  FieldArgs f;
+  f.mode = w->field_mode;
+  f.field = w->dev_field;
+  f.bit0 = w->bit0;
+  f.conf_stride = w->conf_stride;
+  f.a = w->a;
+  f.vol = (double)vol_of(d);
+  f.pos = w->dev_pos;
+  f.orbs_per_conf = batch;
+  return prec == NRCPS_F64 ? propagate_t<double>(ctx, psi, batch, nconf, d, kin, f)
+                           : propagate_t<float>(ctx, psi, batch, nconf, d, kin, f);
+}
+}  // namespace nrcps
+
 // Fused Propagator::Run; dev_kin holds k = 1/xi.
 extern "C" nrcps_status nrcps_propagate(nrcps_context* ctx, void* psi, int batch, int nconf, const int dims[3],
                                        const double* dev_kin, const nrcps_position_factor* w,
@@ -326,15 +376,5 @@ extern "C" nrcps_status nrcps_propagate(nrcps_context* ctx, void* psi, int batch
   NRCPS_REQUIRE(ctx, w->field_mode >= 0 && w->field_mode <= 2, "nrcps_propagate: bad field_mode");
   NRCPS_TRY(check_dims(ctx, dims));
   if (nconf == 0) return NRCPS_OK;
-  FieldArgs f;
-  f.mode = w->field_mode;
-  f.field = w->dev_field;
-  f.bit0 = w->bit0;
-  f.conf_stride = w->conf_stride;
-  f.a = w->a;
-  f.vol = (double)vol_of(dims);
-  f.pos = w->dev_pos;
-  f.orbs_per_conf = batch;
-  return prec == NRCPS_F64 ? propagate_t<double>(ctx, psi, batch, nconf, dims, dev_kin, f)
-                           : propagate_t<float>(ctx, psi, batch, nconf, dims, dev_kin, f);
+  return propagate_impl(ctx, psi, batch, nconf, dims, dev_kin, nullptr, w, prec);
 }

@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--cpu-sample-slices", type=int, default=32, help="slices per host process for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cluster", type=int, default=0, help="force the fused kernel's cluster size (0: autotuned)")
+    ap.add_argument("--no-fused", action="store_true", help="pencil passes instead of the fused kernel")
     return ap.parse_args()
 
 
@@ -185,6 +187,10 @@ def run_b200(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
     ctx = nb.Context(local)
+    if a.no_fused:
+        ctx.set_option("propagate.fused", 0)
+    if a.cluster:
+        ctx.set_option("fused.cluster", a.cluster)
 
     dims = (a.L,) * 3
     idx, _, _ = nb.momenta(dims, "PERFECT", 1.0, a.ef, 2.0)

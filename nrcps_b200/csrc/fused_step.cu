@@ -46,6 +46,7 @@ struct FusedArgs {
   uint64_t conf_stride;
   double a;
   double vol;
+  double w_plus, w_minus;  // (1 + a)/V and (1 - a)/V for Z2 fields
 };
 
 template <typename R>
@@ -54,8 +55,7 @@ __device__ __forceinline__ cplx<R> fused_w(const FusedArgs& f, long conf, long s
   const uint64_t k = f.off0 + (uint64_t)conf * f.conf_stride + (uint64_t)site;
   if (f.field_mode == 1) {
     uint32_t word = __ldg(reinterpret_cast<const uint32_t*>(f.field) + (k >> 5));
-    double phi = ((word >> (k & 31)) & 1u) ? 1.0 : -1.0;
-    w = cplx<R>{(R)((1.0 + f.a * phi) / f.vol), (R)0};
+    w = cplx<R>{(R)(((word >> (k & 31)) & 1u) ? f.w_plus : f.w_minus), (R)0};
   } else if (f.field_mode == 2) {
     double2 phi = __ldg(reinterpret_cast<const double2*>(f.field) + k);
     w = cplx<R>{(R)((1.0 + f.a * phi.x) / f.vol), (R)((f.a * phi.y) / f.vol)};
@@ -164,6 +164,7 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
     // read and written in place through distributed shared memory (CTA c
     // touches only region c of its peers, so the accesses are disjoint).
     if constexpr (C > 1) cluster.sync();
+    else __syncthreads();
     {
       cplx<R>* base[C];
 #pragma unroll
@@ -353,6 +354,8 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   f.field = bits;
   f.a = 0.5;
   f.vol = (double)V;
+  f.w_plus = 1.5 / V;
+  f.w_minus = 0.5 / V;
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -408,6 +411,8 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   f.conf_stride = w->conf_stride;
   f.a = w->a;
   f.vol = (double)d[0] * d[1] * d[2];
+  f.w_plus = (1.0 + f.a) / f.vol;
+  f.w_minus = (1.0 - f.a) / f.vol;
   if (f.n_orb_total == 0) return NRCPS_OK;
   init_choices();
   const int L = d[0];

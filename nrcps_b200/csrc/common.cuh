@@ -12,8 +12,10 @@
 namespace nrcps {
 
 // ------------------------------------------------------------------ complex
+// Aligned to its full size so that shared/global accesses are single
+// 8-byte (FP32) or 16-byte (FP64) transactions.
 template <typename R>
-struct cplx {
+struct alignas(2 * sizeof(R)) cplx {
   R re, im;
 };
 
@@ -49,6 +51,22 @@ __host__ __device__ __forceinline__ cplx<R> cmul(cplx<R> a, cplx<R> b) {
   return cplx<R>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
 
+// x * (hi + lo) for a real factor.  In FP32 the factor is carried as two
+// floats: rounding a factor that is applied every step to one float would
+// bias every mode by the same relative amount each step (a drift of order
+// 2T * 6e-8 in the correlators); the split removes that bias.
+template <typename R>
+__device__ __forceinline__ cplx<R> scale2(cplx<R> x, R hi, R lo) {
+  if constexpr (sizeof(R) == 4) return cplx<R>{fmaf(x.re, lo, x.re * hi), fmaf(x.im, lo, x.im * hi)};
+  else return cplx<R>{x.re * hi, x.im * hi};
+}
+
+template <typename R>
+__device__ __forceinline__ void split(double v, R& hi, R& lo) {
+  hi = (R)v;
+  lo = (sizeof(R) == 4) ? (R)(v - (double)hi) : (R)0;
+}
+
 // ---------------------------------------------------------------- context
 struct Context {
   int device = 0;
@@ -67,7 +85,7 @@ struct Context {
   int fused_enabled = 1;  // single-pass cluster kernel where a variant exists
   int fused_cluster = 0;  // 0: autotuned / default cluster size
   // FP32 copy of a kinetic table for nrcps_propagate(F32).
-  float* kin_f32 = nullptr;
+  float2* kin_f32 = nullptr;  // (hi, lo) split of the last table
   long kin_f32_len = 0;
 };
 

@@ -27,7 +27,7 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
                        const double* w, const int* opp, nrcps_precision prec, double* phi);
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
-                            const float* kin_f32, const nrcps_position_factor* w, nrcps_precision prec);
+                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec);
 nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster);
 }  // namespace nrcps
 
@@ -41,7 +41,7 @@ struct nrcps_ensemble {
   double* src = nullptr;
   int* pw_index = nullptr;
   double* kinv = nullptr;
-  float* kinv_f = nullptr;
+  float2* kinv_f = nullptr;  // (hi, lo) split of kinv
   double* pos = nullptr;
   double* itab = nullptr;
   double* w = nullptr;
@@ -230,9 +230,12 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   for (long i = 0; i < V; ++i) h[i] = 1.0 / kin_xi[i];
   if ((st = upload(ctx, e->kinv, h.data(), 8 * V))) return fail(st);
   {
-    std::vector<float> hf(V);
-    for (long i = 0; i < V; ++i) hf[i] = (float)h[i];
-    if ((st = dalloc(ctx, &e->kinv_f, 4 * V)) || (st = upload(ctx, e->kinv_f, hf.data(), 4 * V))) return fail(st);
+    std::vector<float2> hf(V);
+    for (long i = 0; i < V; ++i) {
+      float hi = (float)h[i];
+      hf[i] = make_float2(hi, (float)(h[i] - (double)hi));
+    }
+    if ((st = dalloc(ctx, &e->kinv_f, 8 * V)) || (st = upload(ctx, e->kinv_f, hf.data(), 8 * V))) return fail(st);
   }
   if (job->dims[0] == job->dims[1] && job->dims[1] == job->dims[2] && job->dims[0] < 64)
     fused_autotune(ctx, (nrcps_precision)job->precision, job->dims[0], nullptr);

@@ -37,7 +37,7 @@ struct FusedArgs {
   void* psi;              // [orbitals][V] complex R
   long n_orb_total;       // nconf * batch
   int batch;              // orbitals per configuration
-  const float* kin_f;     // k(p) in FP32 (R = float)
+  const float2* kin_f;    // k(p) split as (hi, lo) floats, hi + lo = k to ~1e-15 (R = float)
   const double* kin_d;    // k(p) in FP64 (R = double)
   const double* pos;      // optional P(x)
   int field_mode;         // 1 bits, 2 complex phi, 0 complex fld
@@ -49,34 +49,50 @@ struct FusedArgs {
   double w_plus, w_minus;  // (1 + a)/V and (1 - a)/V for Z2 fields
 };
 
+// x * w for the position-space factor of site `site` (general modes).
 template <typename R>
-__device__ __forceinline__ cplx<R> fused_w(const FusedArgs& f, long conf, long site) {
-  cplx<R> w;
-  const uint64_t k = f.off0 + (uint64_t)conf * f.conf_stride + (uint64_t)site;
+__device__ __forceinline__ cplx<R> apply_w_general(const FusedArgs& f, uint64_t kb, int site, cplx<R> x) {
+  double wr, wi;
+  const uint64_t k = kb + (uint64_t)site;
   if (f.field_mode == 1) {
     uint32_t word = __ldg(reinterpret_cast<const uint32_t*>(f.field) + (k >> 5));
-    w = cplx<R>{(R)(((word >> (k & 31)) & 1u) ? f.w_plus : f.w_minus), (R)0};
+    wr = ((word >> (k & 31)) & 1u) ? f.w_plus : f.w_minus;
+    wi = 0.0;
   } else if (f.field_mode == 2) {
     double2 phi = __ldg(reinterpret_cast<const double2*>(f.field) + k);
-    w = cplx<R>{(R)((1.0 + f.a * phi.x) / f.vol), (R)((f.a * phi.y) / f.vol)};
+    wr = (1.0 + f.a * phi.x) / f.vol;
+    wi = (f.a * phi.y) / f.vol;
   } else {
     double2 v = __ldg(reinterpret_cast<const double2*>(f.field) + k);
-    w = cplx<R>{(R)v.x, (R)v.y};
+    wr = v.x;
+    wi = v.y;
   }
   if (f.pos) {
-    R p = (R)__ldg(f.pos + site);
-    w.re *= p;
-    w.im *= p;
+    double p = __ldg(f.pos + site);
+    wr *= p;
+    wi *= p;
   }
-  return w;
+  R rh, rl, ih, il;
+  split<R>(wr, rh, rl);
+  split<R>(wi, ih, il);
+  cplx<R> y = cmul(cplx<R>{rh, ih}, x);
+  if constexpr (sizeof(R) == 4) {
+    y.re = fmaf(x.re, rl, fmaf(-x.im, il, y.re));
+    y.im = fmaf(x.im, rl, fmaf(x.re, il, y.im));
+  }
+  return y;
 }
 
 template <typename R>
-__device__ __forceinline__ R kin_at(const FusedArgs& f, long site);
-template <>
-__device__ __forceinline__ float kin_at<float>(const FusedArgs& f, long site) { return __ldg(f.kin_f + site); }
-template <>
-__device__ __forceinline__ double kin_at<double>(const FusedArgs& f, long site) { return __ldg(f.kin_d + site); }
+__device__ __forceinline__ cplx<R> apply_kin(const FusedArgs& f, int site, cplx<R> x) {
+  if constexpr (sizeof(R) == 4) {
+    float2 k = __ldg(f.kin_f + site);
+    return scale2<R>(x, k.x, k.y);
+  } else {
+    R k = __ldg(f.kin_d + site);
+    return cplx<R>{x.re * k, x.im * k};
+  }
+}
 
 template <typename R, int L, int C>
 struct FusedShape {
@@ -98,7 +114,7 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
     fused_step_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
   constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION, NT = Sh::THREADS;
-  constexpr long V = (long)L * L * L;
+  constexpr int V = L * L * L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* sm = reinterpret_cast<cplx<R>*>(smem_raw);
 
@@ -111,17 +127,24 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
   // local offset of (region r, xl, yl, z); regions are REGION apart
   auto off = [](int r, int xl, int yl, int z) { return r * REGION + (xl * S + yl) * LP + z; };
 
+  // Z2 fields without a static factor take the fast path: one 32-bit word
+  // per pencil element, the bit position fixed per thread (L*L % 32 == 0).
+  const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  R wp_hi, wp_lo, wm_hi, wm_lo;
+  split<R>(f.w_plus, wp_hi, wp_lo);
+  split<R>(f.w_minus, wm_hi, wm_lo);
+
   for (long orb = cluster_id; orb < f.n_orb_total; orb += n_clusters) {
     const long conf = orb / f.batch;
-    char* gpsi = reinterpret_cast<char*>(f.psi) + (size_t)orb * V * sizeof(cplx<R>);
+    const uint64_t kb = f.off0 + (uint64_t)conf * f.conf_stride;  // field offset of this configuration
+    cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> x[L];
     // ---- 1. z-pencils from HBM: thread -> (xl, y), y fastest
     {
       const int y = tid % L, xl = tid / L;
-      const int xg = c * S + xl;
-      const long base = ((long)xg * L + y) * L;
+      const int base = ((c * S + xl) * L + y) * L;
       if constexpr (sizeof(R) == 4) {
-        const float4* src = reinterpret_cast<const float4*>(gpsi) + base / 2;
+        const float4* src = reinterpret_cast<const float4*>(gpsi + base);
 #pragma unroll
         for (int j = 0; j < L / 2; ++j) {
           float4 v = __ldcs(src + j);
@@ -129,7 +152,7 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
           x[2 * j + 1] = cplx<R>{v.z, v.w};
         }
       } else {
-        const double2* src = reinterpret_cast<const double2*>(gpsi) + base;
+        const double2* src = reinterpret_cast<const double2*>(gpsi + base);
 #pragma unroll
         for (int j = 0; j < L; ++j) {
           double2 v = __ldcs(src + j);
@@ -137,20 +160,14 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
         }
       }
 #pragma unroll
-      for (int j = 0; j < L; ++j) {
-        R k = kin_at<R>(f, base + j);
-        x[j].re *= k;
-        x[j].im *= k;
-      }
+      for (int j = 0; j < L; ++j) x[j] = apply_kin<R>(f, base + j, x[j]);
       fft::Dft<L, -1, R>::run(x);
-      const int r = y / S, yl = y % S;
+      cplx<R>* row = sm + off(y / S, xl, y % S, 0);
 #pragma unroll
-      for (int j = 0; j < L; ++j) sm[off(r, xl, yl, j)] = x[j];
+      for (int j = 0; j < L; ++j) row[j] = x[j];
     }
     __syncthreads();
-    // ---- 2. forward DFT along y: thread -> (xl, z), z fastest (the same
-    // thread-to-pencil map as the z-pass, so no barrier is needed between
-    // them beyond the one above)
+    // ---- 2. forward DFT along y: thread -> (xl, z), z fastest
     {
       const int z = tid % L, xl = tid / L;
 #pragma unroll
@@ -159,7 +176,7 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
 #pragma unroll
       for (int y = 0; y < L; ++y) sm[off(y / S, xl, y % S, z)] = x[y];
     }
-    // ---- 3./4./5. x: forward DFT, times w, backward DFT on the pencils of
+    // ---- 3. x: forward DFT, times w, backward DFT on the pencils of
     // y-slab c.  The pencil's element x lives in region c of CTA x/S; it is
     // read and written in place through distributed shared memory (CTA c
     // touches only region c of its peers, so the accesses are disjoint).
@@ -170,14 +187,22 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
 #pragma unroll
       for (int r = 0; r < C; ++r) base[r] = (C > 1 ? cluster.map_shared_rank(sm, r) : sm) + c * REGION;
       const int z = tid % L, yl = tid / L;
-      const int yg = c * S + yl;
+      const int site0 = (c * S + yl) * L + z;  // site of x = 0
 #pragma unroll
       for (int xx = 0; xx < L; ++xx) x[xx] = base[xx / S][((xx % S) * S + yl) * LP + z];
       fft::Dft<L, -1, R>::run(x);
+      if (z2_fast) {
+        const uint64_t k0 = kb + (uint64_t)site0;
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
+        const int bit = (int)(k0 & 31);
 #pragma unroll
-      for (int xx = 0; xx < L; ++xx) {
-        const long site = ((long)xx * L + yg) * L + z;
-        x[xx] = cmul(fused_w<R>(f, conf, site), x[xx]);
+        for (int xx = 0; xx < L; ++xx) {
+          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+          x[xx] = scale2<R>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+        }
+      } else {
+#pragma unroll
+        for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
       }
       fft::Dft<L, +1, R>::run(x);
 #pragma unroll
@@ -198,24 +223,20 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
     // ---- 5. backward DFT along z, times k, store
     {
       const int y = tid % L, xl = tid / L;
-      const int xg = c * S + xl;
-      const long base = ((long)xg * L + y) * L;
-      const int r = y / S, yl = y % S;
+      const int base = ((c * S + xl) * L + y) * L;
+      const cplx<R>* row = sm + off(y / S, xl, y % S, 0);
 #pragma unroll
-      for (int j = 0; j < L; ++j) x[j] = sm[off(r, xl, yl, j)];
+      for (int j = 0; j < L; ++j) x[j] = row[j];
       fft::Dft<L, +1, R>::run(x);
 #pragma unroll
-      for (int j = 0; j < L; ++j) {
-        R k = kin_at<R>(f, base + j);
-        x[j].re *= k;
-        x[j].im *= k;
-      }
+      for (int j = 0; j < L; ++j) x[j] = apply_kin<R>(f, base + j, x[j]);
       if constexpr (sizeof(R) == 4) {
-        float4* dst = reinterpret_cast<float4*>(gpsi) + base / 2;
+        float4* dst = reinterpret_cast<float4*>(gpsi + base);
 #pragma unroll
-        for (int j = 0; j < L / 2; ++j) __stcs(dst + j, make_float4(x[2 * j].re, x[2 * j].im, x[2 * j + 1].re, x[2 * j + 1].im));
+        for (int j = 0; j < L / 2; ++j)
+          __stcs(dst + j, make_float4(x[2 * j].re, x[2 * j].im, x[2 * j + 1].re, x[2 * j + 1].im));
       } else {
-        double2* dst = reinterpret_cast<double2*>(gpsi) + base;
+        double2* dst = reinterpret_cast<double2*>(gpsi + base);
 #pragma unroll
         for (int j = 0; j < L; ++j) __stcs(dst + j, make_double2(x[j].re, x[j].im));
       }
@@ -333,7 +354,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   void* kin = nullptr;
   uint32_t* bits = nullptr;
   cudaError_t e = cudaMalloc(&psi, esz * V * norb);
-  if (e == cudaSuccess) e = cudaMalloc(&kin, esz / 2 * V);
+  if (e == cudaSuccess) e = cudaMalloc(&kin, esz * V);
   if (e == cudaSuccess) e = cudaMalloc((void**)&bits, (size_t)(V / 32 + 1) * 4);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -342,13 +363,13 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
     return NRCPS_OK;  // keep the default choice
   }
   cudaMemsetAsync(psi, 0, esz * V * norb, ctx->stream);
-  cudaMemsetAsync(kin, 0, esz / 2 * V, ctx->stream);
+  cudaMemsetAsync(kin, 0, esz * V, ctx->stream);
   cudaMemsetAsync(bits, 0, (size_t)(V / 32 + 1) * 4, ctx->stream);
   FusedArgs f{};
   f.psi = psi;
   f.n_orb_total = norb;
   f.batch = (int)norb;
-  f.kin_f = (const float*)kin;
+  f.kin_f = (const float2*)kin;
   f.kin_d = (const double*)kin;
   f.field_mode = 1;
   f.field = bits;
@@ -393,7 +414,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   return NRCPS_OK;
 }
 
-// One fused step; `kin_table` is FP32 for prec F32 and FP64 for F64.
+// One fused step; `kin_table` is (hi, lo) float pairs for prec F32 and FP64 for F64.
 // cluster = 0 selects the autotuned (or default) cluster size.
 nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const void* kin_table,
                         nrcps_precision prec, const nrcps_position_factor* w, int cluster) {
@@ -402,7 +423,7 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   f.psi = psi;
   f.n_orb_total = (long)batch * nconf;
   f.batch = batch;
-  f.kin_f = prec == NRCPS_F32 ? (const float*)kin_table : nullptr;
+  f.kin_f = prec == NRCPS_F32 ? (const float2*)kin_table : nullptr;
   f.kin_d = prec == NRCPS_F64 ? (const double*)kin_table : nullptr;
   f.pos = w->dev_pos;
   f.field_mode = w->field_mode;

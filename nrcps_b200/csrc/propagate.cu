@@ -73,9 +73,9 @@ __global__ void __launch_bounds__(128) pencil_kernel(void* data, long total, Pen
     if constexpr (OP == OP_PRE_MUL) {
 #pragma unroll
       for (int j = 0; j < N; ++j) {
-        R k = (R)table[site0 + j * g.stride];
-        x[j].re *= k;
-        x[j].im *= k;
+        R hi, lo;
+        split<R>(table[site0 + j * g.stride], hi, lo);
+        x[j] = scale2<R>(x[j], hi, lo);
       }
     }
     fft::Dft<N, SIGN, R>::run(x);
@@ -88,9 +88,9 @@ __global__ void __launch_bounds__(128) pencil_kernel(void* data, long total, Pen
     if constexpr (OP == OP_POST_MUL) {
 #pragma unroll
       for (int j = 0; j < N; ++j) {
-        R k = (R)table[site0 + j * g.stride];
-        x[j].re *= k;
-        x[j].im *= k;
+        R hi, lo;
+        split<R>(table[site0 + j * g.stride], hi, lo);
+        x[j] = scale2<R>(x[j], hi, lo);
       }
     }
 #pragma unroll
@@ -306,9 +306,12 @@ bool fused_supported(nrcps_precision prec, const int d[3]);
 nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const void* kin_table,
                         nrcps_precision prec, const nrcps_position_factor* w, int cluster);
 
-__global__ void to_f32_kernel(float* dst, const double* src, long n) {
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    dst[i] = (float)src[i];
+// k -> (hi, lo) float pairs with hi + lo = k to ~1e-15.
+__global__ void split_f32_kernel(float2* dst, const double* src, long n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    float hi = (float)src[i];
+    dst[i] = make_float2(hi, (float)(src[i] - (double)hi));
+  }
 }
 
 template <typename R>
@@ -329,7 +332,7 @@ namespace nrcps {
 // Propagator step for the ensemble and the C ABI.  kin_f32 may be NULL (then
 // an FP32 copy of kin is made in the context when the FP32 fused kernel runs).
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
-                            const float* kin_f32, const nrcps_position_factor* w, nrcps_precision prec) {
+                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec) {
   if (ctx->fused_enabled && fused_supported(prec, d)) {
     const void* table = kin;
     if (prec == NRCPS_F32) {
@@ -339,12 +342,12 @@ nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf,
           if (ctx->kin_f32) cudaFree(ctx->kin_f32);
           ctx->kin_f32 = nullptr;
           ctx->kin_f32_len = 0;
-          NRCPS_TRY(check_cuda(ctx, cudaMalloc((void**)&ctx->kin_f32, sizeof(float) * V), "cudaMalloc(kin f32)"));
+          NRCPS_TRY(check_cuda(ctx, cudaMalloc((void**)&ctx->kin_f32, sizeof(float2) * V), "cudaMalloc(kin f32)"));
           ctx->kin_f32_len = V;
         }
-        to_f32_kernel<<<grid_for(V, 256), 256, 0, ctx->stream>>>(ctx->kin_f32, kin, V);
+        split_f32_kernel<<<grid_for(V, 256), 256, 0, ctx->stream>>>(ctx->kin_f32, kin, V);
         ctx->launches++;
-        NRCPS_TRY(check_launch(ctx, "to_f32_kernel"));
+        NRCPS_TRY(check_launch(ctx, "split_f32_kernel"));
         kin_f32 = ctx->kin_f32;
       }
       table = kin_f32;

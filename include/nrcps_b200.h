@@ -231,6 +231,18 @@ nrcps_status nrcps_pair_matrix(nrcps_context *ctx, const void *dev_psi1, const v
  * log_det != 0 returns log det instead (DET_TYPE_LOG). */
 nrcps_status nrcps_slater_dets(nrcps_context *ctx, const double *dev_S, const double *dev_psi1,
                                int N, int nconf, int mode, int log_det, double *dev_out);
+/* nrcps_slater_dets without any device allocation (no counterpart in the
+ * reference).  For callers that cannot let a library allocate device memory
+ * -- a host whose caching pool already owns the device memory, or code
+ * measuring between kernels already queued, where an allocation could stall
+ * the device -- the working memory comes from one fixed 16 MiB array in the
+ * library, which every GPU that loads the library keeps until exit.  Batches
+ * needing more (nconf * nmeas * (2N^2 + N) doubles) are rejected with
+ * NRCPS_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
+ * array's address; make it before any stream capture.  Calls that may run
+ * concurrently on the GPU share the array and race: serialise them. */
+nrcps_status nrcps_slater_dets_noalloc(nrcps_context *ctx, const double *dev_S, const double *dev_psi1,
+                                       int N, int nconf, int mode, int log_det, double *dev_out);
 
 /* ------------------------------------------------------------ ensemble
  * The production loop (production/slater_det/main.C:185-220, mode 0;

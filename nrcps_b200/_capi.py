@@ -86,6 +86,7 @@ SIGNATURES = {
     "nrcps_overlap_planewave": ([_P, _P, _I, _P, _I, _I, _L, _I, _P], _I),
     "nrcps_pair_matrix": ([_P, _P, _P, _I, _I, _L, _P, _P, _I, _P], _I),
     "nrcps_slater_dets": ([_P, _P, _P, _I, _I, _I, _I, _P], _I),
+    "nrcps_slater_dets_noalloc": ([_P, _P, _P, _I, _I, _I, _I, _P], _I),
     "nrcps_ensemble_create": ([_P, ctypes.POINTER(Job), _DP, _DP, _DP, _DP, _IP, _DP, _IP, ctypes.POINTER(_P)], _I),
     "nrcps_ensemble_run": ([_P, _U64, _P], _I),
     "nrcps_ensemble_destroy": ([_P], _I),

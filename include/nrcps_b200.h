@@ -77,6 +77,8 @@ nrcps_status nrcps_destroy(nrcps_context *ctx);
 const char *nrcps_last_error(const nrcps_context *ctx);
 /* cudaStream_t passed as void*; NULL selects the legacy default stream. */
 nrcps_status nrcps_set_stream(nrcps_context *ctx, void *stream);
+/* Waits for the context's stream; returns NRCPS_ERR_TIMEOUT if a kernel's
+ * bounded wait (on an asynchronous bulk copy) gave up since the last call. */
 nrcps_status nrcps_synchronize(nrcps_context *ctx);
 /* Library version string, e.g. "nrcps_b200 0.1 sm_100a". */
 const char *nrcps_version(void);

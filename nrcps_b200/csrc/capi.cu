@@ -64,6 +64,11 @@ extern "C" nrcps_status nrcps_create(int device, nrcps_context** out) {
   nrcps_context* ctx = new nrcps_context();
   ctx->device = device;
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (cudaMalloc((void**)&ctx->dev_err, sizeof(int)) != cudaSuccess ||
+      cudaMemset(ctx->dev_err, 0, sizeof(int)) != cudaSuccess) {
+    delete ctx;
+    return NRCPS_ERR_CUDA;
+  }
   *out = ctx;
   return NRCPS_OK;
 }
@@ -74,6 +79,7 @@ extern "C" nrcps_status nrcps_destroy(nrcps_context* ctx) {
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->gen_args) cudaFree(ctx->gen_args);
   if (ctx->kin_f32) cudaFree(ctx->kin_f32);
+  if (ctx->dev_err) cudaFree(ctx->dev_err);
   delete ctx;
   return NRCPS_OK;
 }
@@ -112,7 +118,16 @@ extern "C" nrcps_status nrcps_autotune(nrcps_context* ctx, nrcps_precision prec,
   return fused_autotune(ctx, prec, L, cluster);
 }
 
+// Waits for the context's stream, then reports a timed-out bounded wait in
+// any kernel since the last check (NRCPS_ERR_TIMEOUT; the flag is cleared).
 extern "C" nrcps_status nrcps_synchronize(nrcps_context* ctx) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  NRCPS_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"));
+  int flag = 0;
+  NRCPS_TRY(check_cuda(ctx, cudaMemcpy(&flag, ctx->dev_err, sizeof(int), cudaMemcpyDeviceToHost), "read flag"));
+  if (flag) {
+    cudaMemset(ctx->dev_err, 0, sizeof(int));
+    return set_error(ctx, NRCPS_ERR_TIMEOUT, "a device wait timed out (bulk copy did not complete)");
+  }
+  return NRCPS_OK;
 }

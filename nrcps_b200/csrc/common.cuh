@@ -85,6 +85,7 @@ struct Context {
   int fused_enabled = 1;  // single-pass cluster kernel where a variant exists
   int fused_cluster = 0;  // 0: autotuned / default cluster size
   // FP32 copy of a kinetic table for nrcps_propagate(F32).
+  int* dev_err = nullptr;  // device flag set by kernels whose bounded waits time out
   float2* kin_f32 = nullptr;  // (hi, lo) split of the last table
   long kin_f32_len = 0;
 };

@@ -47,6 +47,7 @@ struct FusedArgs {
   double a;
   double vol;
   double w_plus, w_minus;  // (1 + a)/V and (1 - a)/V for Z2 fields
+  int* err;                // device flag: 1 = a bounded wait timed out
 };
 
 // x * w for the position-space factor of site `site` (general modes).
@@ -99,24 +100,67 @@ struct FusedShape {
   static constexpr int S = L / C;             // x (or y) planes per CTA
   static constexpr int LP = L + 1;            // padded z row
   // complex elements per region; the extra S elements shift consecutive
-  // regions by half a bank row so the z-pass stores (lanes spanning two
-  // regions) do not alias
+  // regions so that a warp's rows spread over all banks
   static constexpr int REGION = S * S * LP + S;
+  static constexpr int WORK = C * REGION;     // padded working copy of the slab
+  static constexpr int STAGE = S * L * L;     // unpadded slab, landing zone of the bulk copy
   static constexpr int THREADS = S * L;       // one pencil per thread per pass
-  static constexpr size_t SMEM = sizeof(cplx<R>) * (size_t)C * REGION;
-  // FP32: ask for <= 128 registers per thread so two 256-thread CTAs share an SM
-  static constexpr int MIN_BLOCKS = (sizeof(R) == 4 && THREADS * 128 <= 32768) ? 32768 / (THREADS * 128) * 2 : 1;
+  static constexpr size_t SMEM = sizeof(cplx<R>) * (size_t)(STAGE + WORK) + 16;  // + mbarrier
+  static constexpr int CTAS_PER_SM = (int)(228 * 1024 / (SMEM + 1024)) > 4 ? 4 : (int)(228 * 1024 / (SMEM + 1024));
+  static constexpr int MIN_BLOCKS = CTAS_PER_SM < 1 ? 1 : CTAS_PER_SM;
   static_assert(L % C == 0, "cluster size must divide L");
+  static_assert((STAGE * sizeof(cplx<R>)) % 16 == 0, "bulk copy size must be a multiple of 16 bytes");
 };
+
+// ------------------------------------------------ bulk copy + mbarrier PTX
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One 1-D bulk copy global -> this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: gives up after ~2^24 polls (seconds), records the timeout
+// in *err and returns false; the kernel then finishes without hanging.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
+  for (int i = 0; i < (1 << 24); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (err) atomicExch(err, 1);
+  return false;
+}
 
 template <typename R, int L, int C>
 __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L, C>::MIN_BLOCKS)
     fused_step_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
-  constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION, NT = Sh::THREADS;
+  constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION;
   constexpr int V = L * L * L;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<R>* sm = reinterpret_cast<cplx<R>*>(smem_raw);
+  constexpr uint32_t STAGE_BYTES = (uint32_t)(Sh::STAGE * sizeof(cplx<R>));
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  cplx<R>* stage = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* sm = stage + Sh::STAGE;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Sh::WORK);
 
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
@@ -126,59 +170,57 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
 
   // local offset of (region r, xl, yl, z); regions are REGION apart
   auto off = [](int r, int xl, int yl, int z) { return r * REGION + (xl * S + yl) * LP + z; };
+  auto slab = [&](long orb) {  // this CTA's x-slab of orbital `orb` in HBM
+    return reinterpret_cast<const cplx<R>*>(f.psi) + (size_t)orb * V + (size_t)c * S * L * L;
+  };
 
-  // Z2 fields without a static factor take the fast path: one 32-bit word
-  // per pencil element, the bit position fixed per thread (L*L % 32 == 0).
   const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
 
-  for (long orb = cluster_id; orb < f.n_orb_total; orb += n_clusters) {
+  if (tid == 0) mbar_init(bar);
+  __syncthreads();
+  uint32_t parity = 0;
+  long orb = cluster_id;
+  if (tid == 0 && orb < f.n_orb_total) bulk_load(stage, slab(orb), STAGE_BYTES, bar);
+
+  for (; orb < f.n_orb_total; orb += n_clusters) {
     const long conf = orb / f.batch;
     const uint64_t kb = f.off0 + (uint64_t)conf * f.conf_stride;  // field offset of this configuration
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> x[L];
-    // ---- 1. z-pencils from HBM: thread -> (xl, y), y fastest
-    {
-      const int y = tid % L, xl = tid / L;
-      const int base = ((c * S + xl) * L + y) * L;
-      if constexpr (sizeof(R) == 4) {
-        const float4* src = reinterpret_cast<const float4*>(gpsi + base);
-#pragma unroll
-        for (int j = 0; j < L / 2; ++j) {
-          float4 v = __ldcs(src + j);
-          x[2 * j] = cplx<R>{v.x, v.y};
-          x[2 * j + 1] = cplx<R>{v.z, v.w};
-        }
-      } else {
-        const double2* src = reinterpret_cast<const double2*>(gpsi + base);
-#pragma unroll
-        for (int j = 0; j < L; ++j) {
-          double2 v = __ldcs(src + j);
-          x[j] = cplx<R>{v.x, v.y};
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < L; ++j) x[j] = apply_kin<R>(f, base + j, x[j]);
-      fft::Dft<L, -1, R>::run(x);
-      cplx<R>* row = sm + off(y / S, xl, y % S, 0);
-#pragma unroll
-      for (int j = 0; j < L; ++j) row[j] = x[j];
-    }
-    __syncthreads();
-    // ---- 2. forward DFT along y: thread -> (xl, z), z fastest
+    mbar_wait_bounded(bar, parity, f.err);
+    parity ^= 1u;
+    // ---- 1. k(p), forward DFT along y from the staged slab: thread -> (xl, z)
     {
       const int z = tid % L, xl = tid / L;
+      const int site0 = (c * S + xl) * L * L + z;
 #pragma unroll
-      for (int y = 0; y < L; ++y) x[y] = sm[off(y / S, xl, y % S, z)];
+      for (int y = 0; y < L; ++y) x[y] = apply_kin<R>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
       fft::Dft<L, -1, R>::run(x);
 #pragma unroll
       for (int y = 0; y < L; ++y) sm[off(y / S, xl, y % S, z)] = x[y];
     }
+    __syncthreads();
+    // the staging buffer is free: prefetch this cluster's next orbital
+    if (tid == 0 && orb + n_clusters < f.n_orb_total) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      bulk_load(stage, slab(orb + n_clusters), STAGE_BYTES, bar);
+    }
+    // ---- 2. forward DFT along z in place: thread -> (xl, y)
+    {
+      const int y = tid % L, xl = tid / L;
+      cplx<R>* row = sm + off(y / S, xl, y % S, 0);
+#pragma unroll
+      for (int j = 0; j < L; ++j) x[j] = row[j];
+      fft::Dft<L, -1, R>::run(x);
+#pragma unroll
+      for (int j = 0; j < L; ++j) row[j] = x[j];
+    }
     // ---- 3. x: forward DFT, times w, backward DFT on the pencils of
-    // y-slab c.  The pencil's element x lives in region c of CTA x/S; it is
-    // read and written in place through distributed shared memory (CTA c
+    // y-slab c.  Element x of such a pencil lives in region c of CTA x/S and
+    // is read and written in place through distributed shared memory (CTA c
     // touches only region c of its peers, so the accesses are disjoint).
     if constexpr (C > 1) cluster.sync();
     else __syncthreads();
@@ -210,41 +252,36 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
     }
     if constexpr (C > 1) cluster.sync();
     else __syncthreads();
-    // ---- 4. backward DFT along y
-    {
-      const int z = tid % L, xl = tid / L;
-#pragma unroll
-      for (int y = 0; y < L; ++y) x[y] = sm[off(y / S, xl, y % S, z)];
-      fft::Dft<L, +1, R>::run(x);
-#pragma unroll
-      for (int y = 0; y < L; ++y) sm[off(y / S, xl, y % S, z)] = x[y];
-    }
-    __syncthreads();
-    // ---- 5. backward DFT along z, times k, store
+    // ---- 4. backward DFT along z in place
     {
       const int y = tid % L, xl = tid / L;
-      const int base = ((c * S + xl) * L + y) * L;
-      const cplx<R>* row = sm + off(y / S, xl, y % S, 0);
+      cplx<R>* row = sm + off(y / S, xl, y % S, 0);
 #pragma unroll
       for (int j = 0; j < L; ++j) x[j] = row[j];
       fft::Dft<L, +1, R>::run(x);
 #pragma unroll
-      for (int j = 0; j < L; ++j) x[j] = apply_kin<R>(f, base + j, x[j]);
-      if constexpr (sizeof(R) == 4) {
-        float4* dst = reinterpret_cast<float4*>(gpsi + base);
+      for (int j = 0; j < L; ++j) row[j] = x[j];
+    }
+    __syncthreads();
+    // ---- 5. backward DFT along y, times k(p), coalesced streaming stores
+    {
+      const int z = tid % L, xl = tid / L;
+      const int site0 = (c * S + xl) * L * L + z;
 #pragma unroll
-        for (int j = 0; j < L / 2; ++j)
-          __stcs(dst + j, make_float4(x[2 * j].re, x[2 * j].im, x[2 * j + 1].re, x[2 * j + 1].im));
-      } else {
-        double2* dst = reinterpret_cast<double2*>(gpsi + base);
+      for (int y = 0; y < L; ++y) x[y] = sm[off(y / S, xl, y % S, z)];
+      fft::Dft<L, +1, R>::run(x);
 #pragma unroll
-        for (int j = 0; j < L; ++j) __stcs(dst + j, make_double2(x[j].re, x[j].im));
+      for (int y = 0; y < L; ++y) {
+        cplx<R> v = apply_kin<R>(f, site0 + y * L, x[y]);
+        if constexpr (sizeof(R) == 4)
+          __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(v.re, v.im));
+        else
+          __stcs(reinterpret_cast<double2*>(gpsi) + site0 + y * L, make_double2(v.re, v.im));
       }
     }
-    // Peers touch this CTA's shared memory only between the two cluster
-    // barriers of step 3, which every CTA has passed; a CTA-local barrier
-    // protects the next orbital's z-pass stores.
-    __syncthreads();
+    // Thread (xl, z) of step 1 of the next orbital writes exactly the
+    // working-copy elements it read in step 5, and peers touch this CTA's
+    // shared memory only between the barriers of step 3: no barrier needed.
   }
   // keep shared memory alive until every CTA of the cluster is done with it
   if constexpr (C > 1) cluster.sync();
@@ -278,6 +315,7 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   if (e != cudaSuccess || max_clusters <= 0) {
     cudaGetLastError();
     max_clusters = ctx->sm_count / C;
+    if (max_clusters < 1) return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "fused_step: cluster of %d does not fit", C);
   }
   (void)ctas_per_sm_hint;
   long clusters = max_clusters;
@@ -300,17 +338,17 @@ struct FusedVariant {
 };
 
 // Instantiated (precision, L, cluster size) variants.  Shared memory per CTA
-// is C regions of (L/C)^2 (L+1) + L/C complex values; all fit in 227 KB and
-// one pencil per thread keeps L/C * L <= 1024 threads.
+// is the staged slab (L/C) L^2 plus C padded regions of (L/C)^2 (L+1) + L/C
+// complex values; cluster sizes are chosen so that 2-4 CTAs share an SM.
+// Sizes above 8 are non-portable cluster shapes (allowed on B200).
 static const FusedVariant kVariants[] = {
     {NRCPS_F32, 8, 1, launch_fused<float, 8, 1>},     {NRCPS_F32, 16, 1, launch_fused<float, 16, 1>},
-    {NRCPS_F32, 16, 2, launch_fused<float, 16, 2>},   {NRCPS_F32, 24, 2, launch_fused<float, 24, 2>},
-    {NRCPS_F32, 24, 3, launch_fused<float, 24, 3>},   {NRCPS_F32, 32, 2, launch_fused<float, 32, 2>},
-    {NRCPS_F32, 32, 4, launch_fused<float, 32, 4>},   {NRCPS_F32, 32, 8, launch_fused<float, 32, 8>},
-    {NRCPS_F32, 48, 8, launch_fused<float, 48, 8>},   {NRCPS_F64, 8, 1, launch_fused<double, 8, 1>},
-    {NRCPS_F64, 16, 1, launch_fused<double, 16, 1>},  {NRCPS_F64, 16, 2, launch_fused<double, 16, 2>},
-    {NRCPS_F64, 24, 4, launch_fused<double, 24, 4>},  {NRCPS_F64, 32, 4, launch_fused<double, 32, 4>},
-    {NRCPS_F64, 32, 8, launch_fused<double, 32, 8>},
+    {NRCPS_F32, 16, 2, launch_fused<float, 16, 2>},   {NRCPS_F32, 24, 3, launch_fused<float, 24, 3>},
+    {NRCPS_F32, 24, 4, launch_fused<float, 24, 4>},   {NRCPS_F32, 32, 8, launch_fused<float, 32, 8>},
+    {NRCPS_F32, 32, 16, launch_fused<float, 32, 16>}, {NRCPS_F32, 48, 16, launch_fused<float, 48, 16>},
+    {NRCPS_F64, 8, 1, launch_fused<double, 8, 1>},    {NRCPS_F64, 16, 2, launch_fused<double, 16, 2>},
+    {NRCPS_F64, 24, 4, launch_fused<double, 24, 4>},  {NRCPS_F64, 32, 8, launch_fused<double, 32, 8>},
+    {NRCPS_F64, 32, 16, launch_fused<double, 32, 16>},
 };
 static const int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -377,6 +415,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   f.vol = (double)V;
   f.w_plus = 1.5 / V;
   f.w_minus = 0.5 / V;
+  f.err = ctx->dev_err;
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -434,6 +473,7 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   f.vol = (double)d[0] * d[1] * d[2];
   f.w_plus = (1.0 + f.a) / f.vol;
   f.w_minus = (1.0 - f.a) / f.vol;
+  f.err = ctx->dev_err;
   if (f.n_orb_total == 0) return NRCPS_OK;
   init_choices();
   const int L = d[0];

@@ -82,10 +82,10 @@ constexpr CS unit_root(long k, long n) {
 // with |e| up to ~1e-7.  Forward and backward transforms use conjugate
 // pairs, so their phase errors cancel while e does not: every F.B round trip
 // would scale each non-zero momentum by the same (1 + e) product, step after
-// step (a drift of ~1e-5 in the correlators over 32 steps).  The FP32
-// twiddle multiply therefore carries each factor as hi + lo floats.
-// unit_root_f32 below (the float pair closest to the unit circle) is kept
-// for reference tables only.
+// step.  unit_root_f32 picks, among the floats within two ulps of (c, s),
+// the pair whose squared norm is closest to 1.  (Round trips of plane
+// waves are then exact; the remaining rounding of general data is
+// unbiased.)
 constexpr double cabs_(double v) { return v < 0 ? -v : v; }
 constexpr double pow2_(int e) {
   double r = 1.0;
@@ -145,20 +145,10 @@ __device__ __forceinline__ cplx<R> twiddle(cplx<R> x) {
     else return cplx<R>{x.im, -x.re};
   } else {
     if constexpr (sizeof(R) == 4) {
-      // (hi + lo) pairs: the factor is exact to ~1e-15, so an F.B round trip
-      // carries no systematic norm error, only unbiased rounding
-      constexpr CS w = unit_root(k, N);
-      constexpr float c = (float)w.c;
-      constexpr float c_lo = (float)(w.c - (double)c);
-      constexpr float s0 = (float)w.s;
-      constexpr float s0_lo = (float)(w.s - (double)s0);
-      constexpr float s = SIGN > 0 ? s0 : -s0;
-      constexpr float s_lo = SIGN > 0 ? s0_lo : -s0_lo;
-      float re = x.re * c - x.im * s;
-      float im = x.re * s + x.im * c;
-      re = fmaf(x.re, c_lo, fmaf(-x.im, s_lo, re));
-      im = fmaf(x.re, s_lo, fmaf(x.im, c_lo, im));
-      return cplx<R>{re, im};
+      constexpr CSf w = unit_root_f32(k, N);
+      constexpr float c = w.c;
+      constexpr float s = SIGN > 0 ? w.s : -w.s;
+      return cplx<R>{x.re * c - x.im * s, x.re * s + x.im * c};
     } else {
       constexpr CS w = unit_root(k, N);
       constexpr R c = (R)w.c;
@@ -208,18 +198,12 @@ template <int SIGN, typename R>
 struct Butterfly<3, SIGN, R> {
   static __device__ __forceinline__ void run(cplx<R>* t) {
     constexpr R c = (R)-0.5;
-    constexpr double s_exact = 0.86602540378443864676372317075293618;  // sin(2 pi / 3)
-    constexpr R s = (R)s_exact;
-    constexpr R s_lo = (R)(s_exact - (double)s);  // FP32: hi + lo keeps the factor exact
+    // sin(2 pi / 3); in FP32 the float that keeps c^2 + s^2 closest to 1
+    constexpr R s = sizeof(R) == 4 ? (R)unit_root_f32(1, 3).s : (R)0.86602540378443864676372317075293618;
     cplx<R> u = add(t[1], t[2]);
     cplx<R> v = sub(t[1], t[2]);
     cplx<R> m{t[0].re + c * u.re, t[0].im + c * u.im};
-    cplx<R> sv{s * v.re, s * v.im};
-    if constexpr (sizeof(R) == 4) {
-      sv.re = fmaf(s_lo, v.re, sv.re);
-      sv.im = fmaf(s_lo, v.im, sv.im);
-    }
-    cplx<R> iv = mul_i<SIGN>(sv);
+    cplx<R> iv = mul_i<SIGN>(cplx<R>{s * v.re, s * v.im});
     t[0] = add(t[0], u);
     t[1] = add(m, iv);
     t[2] = sub(m, iv);

@@ -76,11 +76,10 @@ __device__ __forceinline__ cplx<R> apply_w_general(const FusedArgs& f, uint64_t 
   R rh, rl, ih, il;
   split<R>(wr, rh, rl);
   split<R>(wi, ih, il);
-  cplx<R> y = cmul(cplx<R>{rh, ih}, x);
-  if constexpr (sizeof(R) == 4) {
-    y.re = fmaf(x.re, rl, fmaf(-x.im, il, y.re));
-    y.im = fmaf(x.im, rl, fmaf(x.re, il, y.im));
-  }
+  // (x.re + i x.im)(wr + i wi) with each real product taken correctly rounded
+  cplx<R> y;
+  y.re = mul2<R>(x.re, rh, rl) - mul2<R>(x.im, ih, il);
+  y.im = mul2<R>(x.re, ih, il) + mul2<R>(x.im, rh, rl);
   return y;
 }
 

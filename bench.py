@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cluster", type=int, default=0, help="force the fused kernel's cluster size (0: autotuned)")
     ap.add_argument("--no-fused", action="store_true", help="pencil passes instead of the fused kernel")
+    ap.add_argument("--split", type=int, default=-1, help="fused kernel lane split: -1 autotuned, 0, 1")
     return ap.parse_args()
 
 
@@ -191,6 +192,8 @@ def run_b200(a):
         ctx.set_option("propagate.fused", 0)
     if a.cluster:
         ctx.set_option("fused.cluster", a.cluster)
+    if a.split >= 0:
+        ctx.set_option("fused.split", a.split)
 
     dims = (a.L,) * 3
     idx, _, _ = nb.momenta(dims, "PERFECT", 1.0, a.ef, 2.0)

@@ -86,10 +86,13 @@ const char *nrcps_version(void);
  * shape is the compile-time BLOCKS/THREADS of include/config.h:30-33):
  *   "propagate.fused"  1 (default): single-pass cluster kernel where one
  *                      exists for the shape; 0: five pencil passes;
- *   "fused.cluster"    0 (default): autotuned cluster size; else force it. */
+ *   "fused.cluster"    0 (default): autotuned cluster size; else force it;
+ *   "fused.split"      -1 (default): autotuned; 0: one thread per pencil;
+ *                      1: each pencil split over two lanes. */
 nrcps_status nrcps_set_option(nrcps_context *ctx, const char *name, long value);
-/* Times every fused-kernel cluster size for (prec, L) on this device and
- * keeps the fastest for later calls; *cluster receives it (may be NULL). */
+/* Times every fused-kernel variant (cluster size, lane split) for (prec, L)
+ * on this device and keeps the fastest for later calls; *cluster receives
+ * its cluster size, negated for the lane-split variants (may be NULL). */
 nrcps_status nrcps_autotune(nrcps_context *ctx, nrcps_precision prec, int L, int *cluster);
 
 /* ----------------------------------------------------- host-side tables

@@ -106,6 +106,9 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
   } else if (n == "fused.cluster") {
     if (value < 0 || value > 16) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.cluster out of range");
     ctx->fused_cluster = (int)value;
+  } else if (n == "fused.split") {
+    if (value < -1 || value > 1) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.split out of range");
+    ctx->fused_split = (int)value;
   } else {
     return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "unknown option %s", name);
   }

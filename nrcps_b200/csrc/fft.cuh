@@ -250,5 +250,53 @@ struct Dft {
   }
 };
 
+// -------------------------------------------------- pencils split over lanes
+// A pencil of N values held by two lanes (lane and lane ^ 16), h = 0 / 1.
+//
+// dft_split_dit: on entry lane h holds x[2m + h] (m < N/2) in v[m]; on exit
+// it holds X[h N/2 + k] in v[k].  Decimation in time: a length-N/2 DFT per
+// lane, the odd half times W_N^k, then one radix-2 stage whose partner
+// values come through one warp shuffle per real.
+//
+// dft_split_dif: on entry lane h holds X[h N/2 + k]; on exit x[2m + h].
+// Decimation in frequency: the radix-2 stage first (a = X[k] + X[k+N/2] on
+// lane 0, b = (X[k] - X[k+N/2]) W_N^k on lane 1), then the half-length DFT.
+//
+// Both are branch-free: per-lane choices are selects, so the warp never
+// diverges.
+template <int N, int SIGN, typename R>
+__device__ __forceinline__ void dft_split_dit(cplx<R>* v, int h) {
+  constexpr int H = N / 2;
+  Dft<H, SIGN, R>::run(v);
+  static_for<H>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    cplx<R> t = twiddle<N, k, SIGN, R>(v[k]);
+    v[k] = h ? t : v[k];
+  });
+  const R sg = h ? (R)-1 : (R)1;
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    cplx<R> o{__shfl_xor_sync(0xffffffffu, v[k].re, 16), __shfl_xor_sync(0xffffffffu, v[k].im, 16)};
+    v[k] = cplx<R>{o.re + sg * v[k].re, o.im + sg * v[k].im};
+  }
+}
+
+template <int N, int SIGN, typename R>
+__device__ __forceinline__ void dft_split_dif(cplx<R>* v, int h) {
+  constexpr int H = N / 2;
+  const R sg = h ? (R)-1 : (R)1;
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    cplx<R> o{__shfl_xor_sync(0xffffffffu, v[k].re, 16), __shfl_xor_sync(0xffffffffu, v[k].im, 16)};
+    v[k] = cplx<R>{o.re + sg * v[k].re, o.im + sg * v[k].im};
+  }
+  static_for<H>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    cplx<R> t = twiddle<N, k, SIGN, R>(v[k]);
+    v[k] = h ? t : v[k];
+  });
+  Dft<H, SIGN, R>::run(v);
+}
+
 }  // namespace fft
 }  // namespace nrcps

@@ -286,10 +286,183 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
   if constexpr (C > 1) cluster.sync();
 }
 
+// ------------------------------------------------ lane-split variant
+// Same algorithm and shared-memory layout as fused_step_kernel, but every
+// pencil is held by two lanes (lane and lane ^ 16), each with L/2 values:
+// half the registers per thread and twice the resident warps.  Forward
+// transforms run decimation-in-time (input split by parity, output by
+// halves), inverse ones decimation-in-frequency (the reverse), so each pass
+// reads and writes shared memory in the split its transform wants.
 template <typename R, int L, int C>
+struct SplitShape {
+  using Base = FusedShape<R, L, C>;
+  static constexpr int THREADS = 2 * Base::S * L;
+  static constexpr int H = L / 2;
+  static constexpr int MIN_BLOCKS = Base::CTAS_PER_SM < 1 ? 1 : Base::CTAS_PER_SM;
+  static_assert(L % 2 == 0 && (Base::S * L) % 16 == 0, "lane-split pencils need L even and S*L % 16 == 0");
+};
+
+template <typename R, int L, int C>
+__global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L, C>::MIN_BLOCKS)
+    fused_step_split_kernel(FusedArgs f) {
+  using Sh = FusedShape<R, L, C>;
+  constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION;
+  constexpr int H = L / 2;
+  constexpr int V = L * L * L;
+  constexpr uint32_t STAGE_BYTES = (uint32_t)(Sh::STAGE * sizeof(cplx<R>));
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  cplx<R>* stage = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* sm = stage + Sh::STAGE;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Sh::WORK);
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int c = (int)cluster.block_rank();
+  const long cluster_id = blockIdx.x / C;
+  const long n_clusters = gridDim.x / C;
+  const int tid = threadIdx.x;
+  const int h = (tid >> 4) & 1;                   // which half of the pencil
+  const int p = (tid >> 5) * 16 + (tid & 15);     // pencil index within the pass
+
+  auto off = [](int r, int xl, int yl, int z) { return r * REGION + (xl * S + yl) * LP + z; };
+  auto slab = [&](long orb) {
+    return reinterpret_cast<const cplx<R>*>(f.psi) + (size_t)orb * V + (size_t)c * S * L * L;
+  };
+
+  const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  R wp_hi, wp_lo, wm_hi, wm_lo;
+  split<R>(f.w_plus, wp_hi, wp_lo);
+  split<R>(f.w_minus, wm_hi, wm_lo);
+
+  if (tid == 0) mbar_init(bar);
+  __syncthreads();
+  uint32_t parity = 0;
+  long orb = cluster_id;
+  if (tid == 0 && orb < f.n_orb_total) bulk_load(stage, slab(orb), STAGE_BYTES, bar);
+
+  for (; orb < f.n_orb_total; orb += n_clusters) {
+    const long conf = orb / f.batch;
+    const uint64_t kb = f.off0 + (uint64_t)conf * f.conf_stride;
+    cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
+    cplx<R> v[H];
+    mbar_wait_bounded(bar, parity, f.err);
+    parity ^= 1u;
+    // ---- 1. k(p), forward DFT along y from the staged slab: pencil (xl, z)
+    {
+      const int z = p % L, xl = p / L;
+      const int site0 = (c * S + xl) * L * L + z;
+#pragma unroll
+      for (int m = 0; m < H; ++m) {
+        const int y = 2 * m + h;
+        v[m] = apply_kin<R>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
+      }
+      fft::dft_split_dit<L, -1, R>(v, h);
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        const int y = h * H + k;
+        sm[off(y / S, xl, y % S, z)] = v[k];
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && orb + n_clusters < f.n_orb_total) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      bulk_load(stage, slab(orb + n_clusters), STAGE_BYTES, bar);
+    }
+    // ---- 2. forward DFT along z in place: pencil (xl, y)
+    {
+      const int y = p % L, xl = p / L;
+      cplx<R>* row = sm + off(y / S, xl, y % S, 0);
+#pragma unroll
+      for (int m = 0; m < H; ++m) v[m] = row[2 * m + h];
+      __syncwarp();
+      fft::dft_split_dit<L, -1, R>(v, h);
+#pragma unroll
+      for (int k = 0; k < H; ++k) row[h * H + k] = v[k];
+    }
+    if constexpr (C > 1) cluster.sync();
+    else __syncthreads();
+    // ---- 3. x: forward DFT, times w, backward DFT through DSMEM: pencil (yl, z)
+    {
+      cplx<R>* base[C];
+#pragma unroll
+      for (int r = 0; r < C; ++r) base[r] = (C > 1 ? cluster.map_shared_rank(sm, r) : sm) + c * REGION;
+      const int z = p % L, yl = p / L;
+      const int site0 = (c * S + yl) * L + z;
+#pragma unroll
+      for (int m = 0; m < H; ++m) {
+        const int xx = 2 * m + h;
+        v[m] = base[xx / S][((xx % S) * S + yl) * LP + z];
+      }
+      fft::dft_split_dit<L, -1, R>(v, h);
+      if (z2_fast) {
+        const uint64_t k0 = kb + (uint64_t)site0;
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
+        const int bit = (int)(k0 & 31);
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+          const int xx = h * H + k;
+          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+          v[k] = scale2<R>(v[k], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < H; ++k) v[k] = apply_w_general<R>(f, kb, site0 + (h * H + k) * L * L, v[k]);
+      }
+      fft::dft_split_dif<L, +1, R>(v, h);
+#pragma unroll
+      for (int m = 0; m < H; ++m) {
+        const int xx = 2 * m + h;
+        base[xx / S][((xx % S) * S + yl) * LP + z] = v[m];
+      }
+    }
+    if constexpr (C > 1) cluster.sync();
+    else __syncthreads();
+    // ---- 4. backward DFT along z in place
+    {
+      const int y = p % L, xl = p / L;
+      cplx<R>* row = sm + off(y / S, xl, y % S, 0);
+#pragma unroll
+      for (int k = 0; k < H; ++k) v[k] = row[h * H + k];
+      __syncwarp();
+      fft::dft_split_dif<L, +1, R>(v, h);
+#pragma unroll
+      for (int m = 0; m < H; ++m) row[2 * m + h] = v[m];
+    }
+    __syncthreads();
+    // ---- 5. backward DFT along y, times k(p), streaming stores
+    {
+      const int z = p % L, xl = p / L;
+      const int site0 = (c * S + xl) * L * L + z;
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        const int y = h * H + k;
+        v[k] = sm[off(y / S, xl, y % S, z)];
+      }
+      fft::dft_split_dif<L, +1, R>(v, h);
+#pragma unroll
+      for (int m = 0; m < H; ++m) {
+        const int y = 2 * m + h;
+        cplx<R> w = apply_kin<R>(f, site0 + y * L, v[m]);
+        if constexpr (sizeof(R) == 4)
+          __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(w.re, w.im));
+        else
+          __stcs(reinterpret_cast<double2*>(gpsi) + site0 + y * L, make_double2(w.re, w.im));
+      }
+    }
+    // the next orbital's step 1 writes, per pencil, the elements this pencil
+    // read in step 5 -- but split differently between the two lanes, so the
+    // pair must be done reading first
+    __syncwarp();
+  }
+  if constexpr (C > 1) cluster.sync();
+}
+
+template <typename R, int L, int C, bool SPLIT = false>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
-  auto kern = fused_step_kernel<R, L, C>;
+  constexpr int THREADS = SPLIT ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
+  void (*kern)(FusedArgs);
+  if constexpr (SPLIT) kern = fused_step_split_kernel<R, L, C>;
+  else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");
   if (C > 8) {
@@ -304,7 +477,7 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   attr[0].val.clusterDim.x = C;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
-  cfg.blockDim = dim3(Sh::THREADS);
+  cfg.blockDim = dim3(THREADS);
   cfg.dynamicSmemBytes = Sh::SMEM;
   cfg.stream = ctx->stream;
   cfg.attrs = attr;
@@ -333,6 +506,7 @@ struct FusedVariant {
   int prec;  // nrcps_precision
   int L;
   int C;
+  int split;  // 1: two lanes per pencil
   FusedLauncher fn;
 };
 
@@ -341,13 +515,28 @@ struct FusedVariant {
 // complex values; cluster sizes are chosen so that 2-4 CTAs share an SM.
 // Sizes above 8 are non-portable cluster shapes (allowed on B200).
 static const FusedVariant kVariants[] = {
-    {NRCPS_F32, 8, 1, launch_fused<float, 8, 1>},     {NRCPS_F32, 16, 1, launch_fused<float, 16, 1>},
-    {NRCPS_F32, 16, 2, launch_fused<float, 16, 2>},   {NRCPS_F32, 24, 3, launch_fused<float, 24, 3>},
-    {NRCPS_F32, 24, 4, launch_fused<float, 24, 4>},   {NRCPS_F32, 32, 8, launch_fused<float, 32, 8>},
-    {NRCPS_F32, 32, 16, launch_fused<float, 32, 16>}, {NRCPS_F32, 48, 16, launch_fused<float, 48, 16>},
-    {NRCPS_F64, 8, 1, launch_fused<double, 8, 1>},    {NRCPS_F64, 16, 2, launch_fused<double, 16, 2>},
-    {NRCPS_F64, 24, 4, launch_fused<double, 24, 4>},  {NRCPS_F64, 32, 8, launch_fused<double, 32, 8>},
-    {NRCPS_F64, 32, 16, launch_fused<double, 32, 16>},
+    {NRCPS_F32, 8, 1, 0, launch_fused<float, 8, 1>},
+    {NRCPS_F32, 16, 1, 0, launch_fused<float, 16, 1>},
+    {NRCPS_F32, 16, 2, 0, launch_fused<float, 16, 2>},
+    {NRCPS_F32, 16, 1, 1, launch_fused<float, 16, 1, true>},
+    {NRCPS_F32, 16, 2, 1, launch_fused<float, 16, 2, true>},
+    {NRCPS_F32, 24, 3, 0, launch_fused<float, 24, 3>},
+    {NRCPS_F32, 24, 4, 0, launch_fused<float, 24, 4>},
+    {NRCPS_F32, 24, 3, 1, launch_fused<float, 24, 3, true>},
+    {NRCPS_F32, 32, 8, 0, launch_fused<float, 32, 8>},
+    {NRCPS_F32, 32, 16, 0, launch_fused<float, 32, 16>},
+    {NRCPS_F32, 32, 8, 1, launch_fused<float, 32, 8, true>},
+    {NRCPS_F32, 32, 16, 1, launch_fused<float, 32, 16, true>},
+    {NRCPS_F32, 48, 16, 0, launch_fused<float, 48, 16>},
+    {NRCPS_F32, 48, 16, 1, launch_fused<float, 48, 16, true>},
+    {NRCPS_F64, 8, 1, 0, launch_fused<double, 8, 1>},
+    {NRCPS_F64, 16, 2, 0, launch_fused<double, 16, 2>},
+    {NRCPS_F64, 16, 2, 1, launch_fused<double, 16, 2, true>},
+    {NRCPS_F64, 24, 4, 0, launch_fused<double, 24, 4>},
+    {NRCPS_F64, 32, 8, 0, launch_fused<double, 32, 8>},
+    {NRCPS_F64, 32, 16, 0, launch_fused<double, 32, 16>},
+    {NRCPS_F64, 32, 8, 1, launch_fused<double, 32, 8, true>},
+    {NRCPS_F64, 32, 16, 1, launch_fused<double, 32, 16, true>},
 };
 static const int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -376,7 +565,8 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   init_choices();
   int dev = ctx->device & 15;
   if (L < 64 && g_choice[dev][prec][L] >= 0) {
-    if (chosen_cluster) *chosen_cluster = kVariants[g_choice[dev][prec][L]].C;
+    if (chosen_cluster)
+      *chosen_cluster = kVariants[g_choice[dev][prec][L]].C * (kVariants[g_choice[dev][prec][L]].split ? -1 : 1);
     return NRCPS_OK;
   }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -448,7 +638,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   cudaFree(kin);
   cudaFree(bits);
   if (best_i >= 0 && L < 64) g_choice[dev][prec][L] = best_i;
-  if (chosen_cluster && best_i >= 0) *chosen_cluster = kVariants[best_i].C;
+  if (chosen_cluster && best_i >= 0) *chosen_cluster = kVariants[best_i].C * (kVariants[best_i].split ? -1 : 1);
   return NRCPS_OK;
 }
 
@@ -477,13 +667,22 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   init_choices();
   const int L = d[0];
   int pick = -1;
-  if (cluster > 0) {
-    for (int i = 0; i < kNumVariants; ++i)
-      if (kVariants[i].prec == prec && kVariants[i].L == L && kVariants[i].C == cluster) pick = i;
-    if (pick < 0) return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "no fused variant with cluster size %d", cluster);
+  const int want_split = ctx->fused_split;  // -1: any
+  if (cluster > 0 || want_split >= 0) {
+    const int tuned = g_choice[ctx->device & 15][prec][L];
+    if (tuned >= 0 && (cluster <= 0 || kVariants[tuned].C == cluster) &&
+        (want_split < 0 || kVariants[tuned].split == want_split))
+      pick = tuned;
+    for (int i = 0; i < kNumVariants && pick < 0; ++i)
+      if (kVariants[i].prec == prec && kVariants[i].L == L && (cluster <= 0 || kVariants[i].C == cluster) &&
+          (want_split < 0 || kVariants[i].split == want_split))
+        pick = i;
+    if (pick < 0)
+      return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "no fused variant with cluster size %d, split %d", cluster,
+                       want_split);
   } else {
     pick = g_choice[ctx->device & 15][prec][L];
-    if (pick < 0)  // default: the largest instantiated cluster for this shape
+    if (pick < 0)  // default: the last instantiated variant for this shape
       for (int i = 0; i < kNumVariants; ++i)
         if (kVariants[i].prec == prec && kVariants[i].L == L) pick = i;
   }

@@ -361,7 +361,22 @@ def test_fused_step_vs_oracle_fp64(ctx):
 
 
 def test_autotune_returns_a_variant(ctx):
-    assert ctx.autotune("f32", 32) in (8, 16)
+    assert abs(ctx.autotune("f32", 32)) in (8, 16)
+
+
+@pytest.mark.parametrize("L,precision", [(16, "f32"), (24, "f32"), (32, "f32"), (48, "f32"), (16, "f64"),
+                                         (32, "f64")])
+def test_lane_split_variant_agrees(ctx, L, precision):
+    psi, kinv, bits = _random_step_inputs(ctx, L, 2, 3, precision, seed=2)
+    outs = []
+    for sp in (0, 1):
+        ctx.set_option("fused.split", sp)
+        q = psi.clone()
+        nb.propagate(q, 3, kinv, bits, 0.5, ctx=ctx)
+        outs.append(q.cpu().numpy())
+    ctx.set_option("fused.split", -1)
+    tol = 1e-14 if precision == "f64" else 2e-6
+    assert max_norm_err(outs[1], outs[0]) < tol
 
 
 def test_synchronize_reports_no_timeout(ctx):

@@ -514,6 +514,8 @@ struct FusedVariant {
 // is the staged slab (L/C) L^2 plus C padded regions of (L/C)^2 (L+1) + L/C
 // complex values; cluster sizes are chosen so that 2-4 CTAs share an SM.
 // Sizes above 8 are non-portable cluster shapes (allowed on B200).
+// Listed best-first per (precision, L) as measured on B200 (the first entry
+// is the default before autotuning).
 static const FusedVariant kVariants[] = {
     {NRCPS_F32, 8, 1, 0, launch_fused<float, 8, 1>},
     {NRCPS_F32, 16, 1, 0, launch_fused<float, 16, 1>},
@@ -524,9 +526,9 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 24, 4, 0, launch_fused<float, 24, 4>},
     {NRCPS_F32, 24, 3, 1, launch_fused<float, 24, 3, true>},
     {NRCPS_F32, 32, 8, 0, launch_fused<float, 32, 8>},
-    {NRCPS_F32, 32, 16, 0, launch_fused<float, 32, 16>},
     {NRCPS_F32, 32, 8, 1, launch_fused<float, 32, 8, true>},
     {NRCPS_F32, 32, 16, 1, launch_fused<float, 32, 16, true>},
+    {NRCPS_F32, 32, 16, 0, launch_fused<float, 32, 16>},
     {NRCPS_F32, 48, 16, 0, launch_fused<float, 48, 16>},
     {NRCPS_F32, 48, 16, 1, launch_fused<float, 48, 16, true>},
     {NRCPS_F64, 8, 1, 0, launch_fused<double, 8, 1>},
@@ -682,9 +684,8 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
                        want_split);
   } else {
     pick = g_choice[ctx->device & 15][prec][L];
-    if (pick < 0)  // default: the last instantiated variant for this shape
-      for (int i = 0; i < kNumVariants; ++i)
-        if (kVariants[i].prec == prec && kVariants[i].L == L) pick = i;
+    for (int i = 0; i < kNumVariants && pick < 0; ++i)  // default: the first listed variant
+      if (kVariants[i].prec == prec && kVariants[i].L == L) pick = i;
   }
   return kVariants[pick].fn(ctx, f, 0);
 }

@@ -266,7 +266,9 @@ typedef struct {
   int precision;         /* nrcps_precision of the orbital propagation */
   int plane_wave;        /* 1: sources are plane waves given by index */
   int use_potential;
-  int qr_period;         /* 0: never re-orthonormalise */
+  int qr_period;         /* k > 0: CholeskyQR of every configuration's orbitals after each
+                            k-th step, determinants rescaled by prod R_ii (mode 0 only);
+                            0: never (the reference's unstabilised propagation) */
   double a;              /* (1 + a*phi) coupling when the interaction is local */
   int local_interaction; /* 1: c(p) constant, use a; 0: full Interaction::Initialize */
 } nrcps_job;

@@ -530,6 +530,7 @@ class EnsembleJob:
     wf_mass: float = 1.0
     wf_lambda: float = 0.176776695
     fermi_energy: float = 0.1
+    qr_period: int = 0  # re-orthonormalise every k steps (0: never)
 
     @property
     def dims(self):
@@ -571,7 +572,7 @@ class Ensemble:
         j.precision = _prec(job.precision)
         j.plane_wave = int(idx is not None)
         j.use_potential = int(pot is not None)
-        j.qr_period = 0
+        j.qr_period = job.qr_period
         j.a = float(itab[0] * vol)  # c(p) * V: the local (1 + a phi) coupling
         j.local_interaction = int(local)
         self._keep = (xi, itab, pot, src, idx, w, opp)

@@ -29,6 +29,10 @@ nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, i
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
                             const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec);
 nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster);
+nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
+                                 double* G, double* logR);
+nrcps_status rescale_dets(nrcps_context* ctx, double* dets, const double* logR, int N, int nconf, long conf_stride,
+                          long offset);
 }  // namespace nrcps
 
 struct nrcps_ensemble {
@@ -52,6 +56,8 @@ struct nrcps_ensemble {
   double* S = nullptr;
   double* P1 = nullptr;
   double* lu_scr = nullptr;
+  double* qr_G = nullptr;     // Gram matrices / R^-1 of a re-orthonormalisation
+  double* qr_logR = nullptr;  // running sum of log R_ii per configuration and orbital
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t gauss_offset = 0;    // stream position of the next configuration (Gaussian fields)
@@ -138,6 +144,8 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       e->psi, prec == NRCPS_F64, N, nc, vol, e->pw_index, e->src);
   ctx->launches++;
   NRCPS_TRY(check_launch(ctx, "scatter_sources_kernel"));
+  if (e->qr_logR)
+    NRCPS_TRY(check_cuda(ctx, cudaMemsetAsync(e->qr_logR, 0, sizeof(double) * nc * N, ctx->stream), "memset logR"));
   for (int t = 0; t < T; ++t) {
     // -------- measurement at slice t (before the step, main.C:204-211)
     if (j.mode == 0) {
@@ -145,6 +153,8 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       else NRCPS_TRY(overlap_impl(ctx, e->src, N, e->psi, N, nc, vol, prec, e->S));
       NRCPS_TRY(slater_dets_impl(ctx, e->S, nullptr, N, nc, 0, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
                                  e->lu_scr));
+      if (e->qr_logR && t >= j.qr_period)
+        NRCPS_TRY(rescale_dets(ctx, dets, e->qr_logR, N, nc, 2L * T * e->nmeas, 2L * t * e->nmeas));
     } else {
       NRCPS_TRY(pair_impl(ctx, e->psi, e->psi, N, nc, vol, e->w, e->opp, prec, e->S));
       if (e->pw_index) NRCPS_TRY(gather_impl(ctx, e->pw_index, N, e->psi, N, nc, vol, prec, e->P1));
@@ -184,6 +194,8 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       pf.conf_stride = (uint64_t)T * vol;
     }
     NRCPS_TRY(propagate_impl(ctx, e->psi, N, nc, d3, e->kinv, e->kinv_f, &pf, prec));
+    if (e->qr_logR && (t + 1) % j.qr_period == 0 && t + 1 < T)
+      NRCPS_TRY(qr_reorthonormalise(ctx, e->psi, N, vol, nc, prec, e->qr_G, e->qr_logR));
   }
   e->launches_per_run = ctx->launches - n0;
   return NRCPS_OK;
@@ -206,8 +218,12 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   NRCPS_REQUIRE(ctx, job->mode == 0 || (job->mode == 1 && w && opposite), "nrcps_ensemble_create: pair tables missing");
   NRCPS_REQUIRE(ctx, job->local_interaction || itab, "nrcps_ensemble_create: interaction table missing");
   NRCPS_REQUIRE(ctx, !job->use_potential || pot, "nrcps_ensemble_create: potential table missing");
-  if (job->qr_period != 0)
-    return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "nrcps_ensemble_create: QR re-orthonormalisation not built");
+  NRCPS_REQUIRE(ctx, job->qr_period >= 0, "nrcps_ensemble_create: qr_period < 0");
+  if (job->qr_period > 0 && job->mode != 0)
+    return set_error(ctx, NRCPS_ERR_UNSUPPORTED,
+                     "nrcps_ensemble_create: re-orthonormalisation is built for the one-body measurement (mode 0)");
+  if (job->qr_period > 0 && job->n_orb > 64)
+    return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "nrcps_ensemble_create: re-orthonormalisation needs N <= 64");
   const int fk = job->field_kind;
   NRCPS_REQUIRE(ctx, fk >= 0 && fk <= 3, "nrcps_ensemble_create: bad field kind");
   nrcps_ensemble* e = new nrcps_ensemble();
@@ -267,6 +283,10 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   }
   if ((st = dalloc(ctx, &e->S, 16 * (size_t)nc * N * N))) return fail(st);
   if ((st = dalloc(ctx, &e->lu_scr, slater_dets_scratch_bytes(N, nc, job->mode)))) return fail(st);
+  if (job->qr_period > 0) {
+    if ((st = dalloc(ctx, &e->qr_G, 16 * (size_t)nc * N * N))) return fail(st);
+    if ((st = dalloc(ctx, &e->qr_logR, 8 * (size_t)nc * N))) return fail(st);
+  }
   *out = e;
   return NRCPS_OK;
 }
@@ -344,7 +364,7 @@ extern "C" nrcps_status nrcps_ensemble_destroy(nrcps_ensemble* e) {
   if (e->exec) cudaGraphExecDestroy(e->exec);
   if (e->graph) cudaGraphDestroy(e->graph);
   void* bufs[] = {e->psi, e->src, e->pw_index, e->kinv, e->kinv_f, e->pos, e->itab, e->w, e->opp,
-                  e->bits, e->phi, e->fld, e->S, e->P1, e->lu_scr};
+                  e->bits, e->phi, e->fld, e->S, e->P1, e->lu_scr, e->qr_G, e->qr_logR};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete e;

@@ -1,0 +1,225 @@
+// qr.cu -- periodic re-orthonormalisation of the orbitals (CholeskyQR in FP64).
+//
+// The reference propagates unstabilised (its only option is a host-side
+// norm rescale, Propagator::Normalize, src/alg/propagator.C:78-135).  At
+// long Euclidean times the orbitals of a configuration align and the Slater
+// matrices lose precision.  Here, every qr_period slices, each
+// configuration's orbital block Psi (V x N) is replaced by Q with Psi = Q R:
+//   G = Psi^H Psi (FP64 accumulation), G = R^H R (Cholesky), Psi <- Psi R^-1.
+// R is upper triangular in orbital order, so the first n columns of Psi are
+// the first n columns of Q times the leading n x n block of R, and every
+// leading-minor determinant the measurement needs is recovered as
+//   det S_n(Psi) = det S_n(Q) * prod_{i <= n} R_ii.
+// The running sum of log R_ii per orbital is kept per configuration and the
+// measured determinants are rescaled by exp(sum_{i<=n} log R_ii).
+#include "common.cuh"
+
+namespace nrcps {
+
+// G[c][i][j] = sum_p conj(psi_{c,i}(p)) psi_{c,j}(p); one block per (c, j).
+template <typename R>
+__global__ void __launch_bounds__(256) gram_kernel(const void* __restrict__ psi, int N, long vol,
+                                                   double* __restrict__ G) {
+  const long cj = blockIdx.x;
+  const long c = cj / N;
+  const int j = (int)(cj % N);
+  const cplx<R>* base = reinterpret_cast<const cplx<R>*>(psi) + (size_t)c * N * vol;
+  __shared__ double red[8][2][8];
+  for (int i0 = 0; i0 < N; i0 += 8) {
+    double ar[8], ai[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ar[k] = ai[k] = 0.0;
+    for (long p = threadIdx.x; p < vol; p += blockDim.x) {
+      cplx<R> q = base[(size_t)j * vol + p];
+      const double qr = q.re, qi = q.im;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (i0 + k < N) {
+          cplx<R> a = base[(size_t)(i0 + k) * vol + p];
+          ar[k] += (double)a.re * qr + (double)a.im * qi;
+          ai[k] += (double)a.re * qi - (double)a.im * qr;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      for (int o = 16; o > 0; o >>= 1) {
+        ar[k] += __shfl_down_sync(0xffffffffu, ar[k], o);
+        ai[k] += __shfl_down_sync(0xffffffffu, ai[k], o);
+      }
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        red[threadIdx.x >> 5][0][k] = ar[k];
+        red[threadIdx.x >> 5][1][k] = ai[k];
+      }
+    __syncthreads();
+    if (threadIdx.x < 8 && i0 + (int)threadIdx.x < N) {
+      const int k = threadIdx.x;
+      double sr = 0, si = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        sr += red[w][0][k];
+        si += red[w][1][k];
+      }
+      double* g = G + 2 * ((c * N + (i0 + k)) * (long)N + j);
+      g[0] = sr;
+      g[1] = si;
+    }
+    __syncthreads();
+  }
+}
+
+// Per configuration: Cholesky G = R^H R (R upper), Rinv = R^{-1}, and
+// logR[c][i] += log R_ii.  One thread per configuration; G is overwritten
+// with Rinv.  A non-positive pivot marks the configuration with NaN in logR.
+__global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double* __restrict__ logR) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nconf; c += gridDim.x * blockDim.x) {
+    double* g = G + 2L * c * N * N;
+    auto re = [&](int i, int j) -> double& { return g[2 * (i * N + j)]; };
+    auto im = [&](int i, int j) -> double& { return g[2 * (i * N + j) + 1]; };
+    // Cholesky in place, upper triangle: G = R^H R
+    bool ok = true;
+    for (int i = 0; i < N && ok; ++i) {
+      double d = re(i, i);
+      for (int k = 0; k < i; ++k) d -= re(k, i) * re(k, i) + im(k, i) * im(k, i);
+      if (!(d > 0.0)) {
+        ok = false;
+        break;
+      }
+      const double rii = sqrt(d);
+      re(i, i) = rii;
+      im(i, i) = 0.0;
+      for (int j = i + 1; j < N; ++j) {
+        // R_ij = (G_ij - sum_k conj(R_ki) R_kj) / R_ii
+        double sr = re(i, j), si = im(i, j);
+        for (int k = 0; k < i; ++k) {
+          const double ar = re(k, i), ai = -im(k, i), br = re(k, j), bi = im(k, j);
+          sr -= ar * br - ai * bi;
+          si -= ar * bi + ai * br;
+        }
+        re(i, j) = sr / rii;
+        im(i, j) = si / rii;
+      }
+    }
+    if (!ok) {
+      for (int i = 0; i < N; ++i) logR[(long)c * N + i] = nan("");
+      continue;
+    }
+    for (int i = 0; i < N; ++i) logR[(long)c * N + i] += log(re(i, i));
+    // Rinv (upper triangular) by back substitution, column by column, into
+    // the lower-left (unused) storage is not possible for complex R; invert
+    // in place row by row from the bottom: Rinv_ii = 1/R_ii,
+    // Rinv_ij = -(sum_{k=i+1..j} R_ik Rinv_kj) / R_ii for j > i.
+    for (int i = N - 1; i >= 0; --i) {
+      const double rii = re(i, i);
+      for (int j = N - 1; j > i; --j) {
+        double sr = 0, si = 0;
+        for (int k = i + 1; k <= j; ++k) {
+          const double ar = re(i, k), ai = im(i, k), br = re(k, j), bi = im(k, j);
+          sr += ar * br - ai * bi;
+          si += ar * bi + ai * br;
+        }
+        re(i, j) = -sr / rii;
+        im(i, j) = -si / rii;
+      }
+      re(i, i) = 1.0 / rii;
+    }
+  }
+}
+
+// psi_{c,t}(p) <- sum_{i <= t} psi_{c,i}(p) Rinv[i][t]; one thread per site,
+// all N orbitals of a configuration in registers (N <= 64).
+template <typename R, int NMAX>
+__global__ void __launch_bounds__(128) apply_rinv_kernel(void* __restrict__ psi, int N, long vol, int nconf,
+                                                          const double* __restrict__ Rinv) {
+  extern __shared__ double rs[];  // 2 N^2 doubles of this block's configuration
+  const long sites_per_block = blockDim.x;
+  const long blocks_per_conf = (vol + sites_per_block - 1) / sites_per_block;
+  const long c = blockIdx.x / blocks_per_conf;
+  if (c >= nconf) return;
+  const long p = (blockIdx.x % blocks_per_conf) * sites_per_block + threadIdx.x;
+  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) rs[e] = Rinv[2L * c * N * N + e];
+  __syncthreads();
+  if (p >= vol) return;
+  cplx<R>* base = reinterpret_cast<cplx<R>*>(psi) + (size_t)c * N * vol + p;
+  double xr[NMAX], xi[NMAX];
+#pragma unroll
+  for (int i = 0; i < NMAX; ++i)
+    if (i < N) {
+      cplx<R> v = base[(size_t)i * vol];
+      xr[i] = v.re;
+      xi[i] = v.im;
+    }
+#pragma unroll
+  for (int t = NMAX - 1; t >= 0; --t) {
+    if (t >= N) continue;
+    double sr = 0, si = 0;
+#pragma unroll
+    for (int i = 0; i <= t; ++i) {
+      const double ar = rs[2 * (i * N + t)], ai = rs[2 * (i * N + t) + 1];
+      sr += xr[i] * ar - xi[i] * ai;
+      si += xr[i] * ai + xi[i] * ar;
+    }
+    base[(size_t)t * vol] = cplx<R>{(R)sr, (R)si};
+  }
+}
+
+// dets[c][t][n-1] *= exp(sum_{i<n} logR[c][i]) for the minors measured at slice t.
+__global__ void rescale_dets_kernel(double* dets, const double* logR, int N, int nconf, long conf_stride,
+                                    long offset) {
+  const long total = (long)nconf * N;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long c = e / N;
+    const int n = (int)(e % N);
+    double s = 0;
+    for (int i = 0; i <= n; ++i) s += logR[c * N + i];
+    const double f = exp(s);
+    double* d = dets + c * conf_stride + offset + 2L * n;
+    d[0] *= f;
+    d[1] *= f;
+  }
+}
+
+template <int NMAX>
+static nrcps_status launch_apply(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
+                                 const double* Rinv) {
+  const long bpc = (vol + 127) / 128;
+  const size_t sh = sizeof(double) * 2 * N * N;
+  if (prec == NRCPS_F64)
+    apply_rinv_kernel<double, NMAX><<<(unsigned)(bpc * nconf), 128, sh, ctx->stream>>>(psi, N, vol, nconf, Rinv);
+  else
+    apply_rinv_kernel<float, NMAX><<<(unsigned)(bpc * nconf), 128, sh, ctx->stream>>>(psi, N, vol, nconf, Rinv);
+  ctx->launches++;
+  return check_launch(ctx, "apply_rinv_kernel");
+}
+
+// One re-orthonormalisation of nconf configurations of N orbitals.
+// G: scratch of nconf * N * N complex doubles; logR accumulates.
+nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
+                                 double* G, double* logR) {
+  if (N > 64) return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "QR re-orthonormalisation supports N <= 64");
+  if (prec == NRCPS_F64)
+    gram_kernel<double><<<(unsigned)((long)nconf * N), 256, 0, ctx->stream>>>(psi, N, vol, G);
+  else
+    gram_kernel<float><<<(unsigned)((long)nconf * N), 256, 0, ctx->stream>>>(psi, N, vol, G);
+  ctx->launches++;
+  NRCPS_TRY(check_launch(ctx, "gram_kernel"));
+  chol_inv_kernel<<<grid_for(nconf, 64), 64, 0, ctx->stream>>>(G, N, nconf, logR);
+  ctx->launches++;
+  NRCPS_TRY(check_launch(ctx, "chol_inv_kernel"));
+  if (N <= 8) return launch_apply<8>(ctx, psi, N, vol, nconf, prec, G);
+  if (N <= 16) return launch_apply<16>(ctx, psi, N, vol, nconf, prec, G);
+  if (N <= 24) return launch_apply<24>(ctx, psi, N, vol, nconf, prec, G);
+  if (N <= 40) return launch_apply<40>(ctx, psi, N, vol, nconf, prec, G);
+  return launch_apply<64>(ctx, psi, N, vol, nconf, prec, G);
+}
+
+nrcps_status rescale_dets(nrcps_context* ctx, double* dets, const double* logR, int N, int nconf, long conf_stride,
+                          long offset) {
+  rescale_dets_kernel<<<grid_for((long)nconf * N, 256), 256, 0, ctx->stream>>>(dets, logR, N, nconf, conf_stride,
+                                                                               offset);
+  ctx->launches++;
+  return check_launch(ctx, "rescale_dets_kernel");
+}
+
+}  // namespace nrcps

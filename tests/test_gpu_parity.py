@@ -383,3 +383,36 @@ def test_synchronize_reports_no_timeout(ctx):
     psi, kinv, bits = _random_step_inputs(ctx, 32, 2, 2, "f32")
     nb.propagate(psi, 2, kinv, bits, 0.5, ctx=ctx)
     ctx.synchronize()  # raises NrcpsError(TIMEOUT) if a bounded wait gave up
+
+
+# ------------------------------------------------ re-orthonormalisation
+@pytest.mark.parametrize("period", [1, 2, 5])
+def test_qr_reorthonormalisation_preserves_determinants_fp64(ctx, period):
+    """det S_n(Psi) = det S_n(Q) prod R_ii: re-orthonormalised runs reproduce
+    the unstabilised determinants (the reference's semantics)."""
+    base = dict(L=8, T=12, n_conf=6, fermi_energy=0.35, precision="f64", seed=4321)
+    idx, _, _ = nb.momenta((8, 8, 8), "PERFECT", 1.0, 0.35, 2.0)
+    plain = nb.Ensemble(nb.EnsembleJob(**base), plane_wave_index=idx, ctx=ctx).run(0).cpu().numpy()
+    qr = nb.Ensemble(nb.EnsembleJob(qr_period=period, **base), plane_wave_index=idx, ctx=ctx).run(0).cpu().numpy()
+    assert rel_err(qr, plain) < 1e-11
+
+
+def test_qr_dense_sources_fp64(golden, ctx):
+    g = golden("ensemble_trapped.npz")
+    src = g["sources"]
+    job = dict(L=8, T=6, n_conf=2, seed=31, precision="f64", cutoff=0.99999, potential=True, kappa=0.005)
+    plain = nb.Ensemble(nb.EnsembleJob(**job), sources=src, ctx=ctx).run(0).cpu().numpy()
+    qr = nb.Ensemble(nb.EnsembleJob(qr_period=2, **job), sources=src, ctx=ctx).run(0).cpu().numpy()
+    assert rel_err(qr, plain) < 1e-11
+
+
+def test_qr_fp32_against_fp64(golden, ctx):
+    g = golden("ensemble_config1.npz")
+    idx, _, _ = nb.momenta((16, 16, 16), "PERFECT", 1.0, 0.1, 2.0)
+    base = dict(L=16, T=32, n_conf=64, seed=1234)
+    d64 = nb.Ensemble(nb.EnsembleJob(precision="f64", **base), plane_wave_index=idx, ctx=ctx).run(0).cpu().numpy()
+    d32 = nb.Ensemble(nb.EnsembleJob(precision="f32", qr_period=8, **base), plane_wave_index=idx,
+                      ctx=ctx).run(0).cpu().numpy()
+    assert rel_err(d32, d64) < 5e-5
+    assert rel_err((np.abs(d32) ** 2).mean(0), (np.abs(d64) ** 2).mean(0)) < FP32_REL
+    assert rel_err(d64[:2], g["dets"]) < FP64_REL

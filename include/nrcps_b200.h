@@ -227,6 +227,21 @@ nrcps_status nrcps_overlap_planewave(nrcps_context *ctx, const int *dev_index, i
 nrcps_status nrcps_pair_matrix(nrcps_context *ctx, const void *dev_psi1, const void *dev_psi2, int n,
                                int nconf, long vol, const double *dev_w, const int *dev_opposite,
                                nrcps_precision prec, double *dev_phi);
+/* Cuda::InnerProduct (src/utils/cuda/cuda_utils.cu:88-127) as the
+ * reference's GPU build calls it: kets and bras are device arrays of nf
+ * device pointers to V complex FP64 vectors; dev_mat[t + nf*s] =
+ * <kets[s] | bras[t]> (nf*nf complex FP64, device). */
+nrcps_status nrcps_inner_product_ptrs(nrcps_context *ctx, const double *const *dev_kets,
+                                      const double *const *dev_bras, int nf, long vol,
+                                      double *dev_mat);
+/* TwoBody::Run(Float**, Float**, complex<Float>*, int)
+ * (src/two_body/cuda/two_body_run.cu:41-83) with the same pointer arrays:
+ * dev_phi[t + nf*s] = sum_i w_i props1[s](i) props2[t](opposite(i)).  Every
+ * element is computed (the reference's batched kernel drops rows and
+ * columns when nf is not a multiple of 3, two_body_run.cu:56). */
+nrcps_status nrcps_pair_matrix_ptrs(nrcps_context *ctx, const double *const *dev_props1,
+                                    const double *const *dev_props2, int nf, long vol,
+                                    const double *dev_w, const int *dev_opposite, double *dev_phi);
 /* SlaterDet::Run / SlaterDet2::Run (src/slater_det/slater_det.C:59-115,
  * slater_det2.C:78-148) with ludcmp (src/utils/ludcmp.C:9-65) in FP64 for
  * every leading minor n = 1..N of nconf matrices S (N x N complex):

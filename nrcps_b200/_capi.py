@@ -85,6 +85,8 @@ SIGNATURES = {
     "nrcps_overlap": ([_P, _P, _I, _P, _I, _I, _L, _I, _P], _I),
     "nrcps_overlap_planewave": ([_P, _P, _I, _P, _I, _I, _L, _I, _P], _I),
     "nrcps_pair_matrix": ([_P, _P, _P, _I, _I, _L, _P, _P, _I, _P], _I),
+    "nrcps_inner_product_ptrs": ([_P, _P, _P, _I, _L, _P], _I),
+    "nrcps_pair_matrix_ptrs": ([_P, _P, _P, _I, _L, _P, _P, _P], _I),
     "nrcps_slater_dets": ([_P, _P, _P, _I, _I, _I, _I, _P], _I),
     "nrcps_slater_dets_noalloc": ([_P, _P, _P, _I, _I, _I, _I, _P], _I),
     "nrcps_ensemble_create": ([_P, ctypes.POINTER(Job), _DP, _DP, _DP, _DP, _IP, _DP, _IP, ctypes.POINTER(_P)], _I),

@@ -118,6 +118,78 @@ __global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1
   }
 }
 
+// ------------------------------------------------- pointer-array variants
+// mat[t + nf*s] = <kets[s] | bras[t]> (the layout of Cuda::InnerProduct,
+// src/utils/cuda/cuda_utils_kernels.cu:4-48), FP64, one block per (s, t).
+__global__ void __launch_bounds__(256) inner_ptrs_kernel(const double* const* __restrict__ kets,
+                                                         const double* const* __restrict__ bras, int nf, long vol,
+                                                         double* __restrict__ mat) {
+  const int s = blockIdx.x / nf, t = blockIdx.x % nf;
+  const double2* a = reinterpret_cast<const double2*>(kets[s]);
+  const double2* b = reinterpret_cast<const double2*>(bras[t]);
+  double re = 0.0, im = 0.0;
+  for (long i = threadIdx.x; i < vol; i += blockDim.x) {
+    double2 x = a[i], y = b[i];
+    re += x.x * y.x + x.y * y.y;
+    im += x.x * y.y - x.y * y.x;
+  }
+  __shared__ double red[2][8];
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_down_sync(0xffffffffu, re, o);
+    im += __shfl_down_sync(0xffffffffu, im, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = re;
+    red[1][threadIdx.x >> 5] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sr = 0, si = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      sr += red[0][k];
+      si += red[1][k];
+    }
+    mat[2L * (t + (long)nf * s)] = sr;
+    mat[2L * (t + (long)nf * s) + 1] = si;
+  }
+}
+
+// phi[t + nf*s] = sum_i w_i props1[s](i) props2[t](opp(i)), FP64.
+__global__ void __launch_bounds__(256) pair_ptrs_kernel(const double* const* __restrict__ p1,
+                                                        const double* const* __restrict__ p2, int nf, long vol,
+                                                        const double* __restrict__ w, const int* __restrict__ opp,
+                                                        double* __restrict__ phi) {
+  const int s = blockIdx.x / nf, t = blockIdx.x % nf;
+  const double2* a = reinterpret_cast<const double2*>(p1[s]);
+  const double2* b = reinterpret_cast<const double2*>(p2[t]);
+  double re = 0.0, im = 0.0;
+  for (long i = threadIdx.x; i < vol; i += blockDim.x) {
+    double2 x = a[i], y = b[opp[i]];
+    const double wi = w[i];
+    re += (x.x * y.x - x.y * y.y) * wi;
+    im += (x.x * y.y + x.y * y.x) * wi;
+  }
+  __shared__ double red[2][8];
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_down_sync(0xffffffffu, re, o);
+    im += __shfl_down_sync(0xffffffffu, im, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = re;
+    red[1][threadIdx.x >> 5] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sr = 0, si = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      sr += red[0][k];
+      si += red[1][k];
+    }
+    phi[2L * (t + (long)nf * s)] = sr;
+    phi[2L * (t + (long)nf * s) + 1] = si;
+  }
+}
+
 // ------------------------------------------------------------------- LU
 struct dc {
   double re, im;
@@ -313,6 +385,29 @@ extern "C" nrcps_status nrcps_pair_matrix(nrcps_context* ctx, const void* dev_ps
   NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_w && dev_opposite && dev_phi && n >= 0 && nconf >= 0 && vol > 0,
                 "nrcps_pair_matrix: bad arguments");
   return pair_impl(ctx, dev_psi1, dev_psi2, n, nconf, vol, dev_w, dev_opposite, prec, dev_phi);
+}
+
+extern "C" nrcps_status nrcps_inner_product_ptrs(nrcps_context* ctx, const double* const* dev_kets,
+                                                 const double* const* dev_bras, int nf, long vol, double* dev_mat) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  NRCPS_REQUIRE(ctx, dev_kets && dev_bras && dev_mat && nf >= 0 && vol > 0, "nrcps_inner_product_ptrs: bad arguments");
+  if (nf == 0) return NRCPS_OK;
+  inner_ptrs_kernel<<<(unsigned)(nf * nf), 256, 0, ctx->stream>>>(dev_kets, dev_bras, nf, vol, dev_mat);
+  ctx->launches++;
+  return check_launch(ctx, "inner_ptrs_kernel");
+}
+
+extern "C" nrcps_status nrcps_pair_matrix_ptrs(nrcps_context* ctx, const double* const* dev_props1,
+                                               const double* const* dev_props2, int nf, long vol, const double* dev_w,
+                                               const int* dev_opposite, double* dev_phi) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  NRCPS_REQUIRE(ctx, dev_props1 && dev_props2 && dev_w && dev_opposite && dev_phi && nf >= 0 && vol > 0,
+                "nrcps_pair_matrix_ptrs: bad arguments");
+  if (nf == 0) return NRCPS_OK;
+  pair_ptrs_kernel<<<(unsigned)(nf * nf), 256, 0, ctx->stream>>>(dev_props1, dev_props2, nf, vol, dev_w,
+                                                                 dev_opposite, dev_phi);
+  ctx->launches++;
+  return check_launch(ctx, "pair_ptrs_kernel");
 }
 
 extern "C" nrcps_status nrcps_slater_dets(nrcps_context* ctx, const double* dev_S, const double* dev_psi1, int N,

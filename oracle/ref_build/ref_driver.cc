@@ -17,6 +17,10 @@
 //   lu        -- ludcmp + det on matrices read from a file (src/utils/ludcmp.C).
 //   bench     -- the ensemble loop timed with clock_gettime, for the CPU baseline.
 //
+// Built twice: against the reference's CPU units (nrcps_ref) and, as
+// nrcps_dropin, against its GPU configuration with the shims of
+// nrcps_b200/shim in place of its CUDA units (the drop-in check).
+//
 // Arguments are key=value pairs; see parse_job() for the keys.
 
 #include <complex>
@@ -49,7 +53,28 @@ using namespace std;
 #include "uniform_deviates.h"
 #include "verbose.h"
 
+#ifdef USE_GPU
+#include <cuda_runtime.h>
+#endif
+
 namespace {
+
+// Vectors handed out by the reference's classes are device pointers in its
+// GPU build (Propagator::Get, OneBody::Get, Lattice::Get); copy to the host
+// before writing them.
+void to_host(double* dst, const double* src, size_t n) {
+#ifdef USE_GPU
+  cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost);
+#else
+  memcpy(dst, src, n * sizeof(double));
+#endif
+}
+
+void write_vec(FILE* f, const double* src, size_t n) {
+  vector<double> h(n);
+  to_host(&h[0], src, n);
+  fwrite(&h[0], sizeof(double), n, f);
+}
 
 typedef map<string, string> KV;
 
@@ -317,7 +342,7 @@ int run_ensemble(const KV& kv, bool timed_only) {
   const string out = get(kv, "out", ".");
   if (!timed_only && kv.count("out")) {
     FILE* f = open_out(out + "/sources.bin");
-    for (int n = 0; n < N; ++n) fwrite(one_bodies[n]->Get(), sizeof(double), 2 * vol, f);
+    for (int n = 0; n < N; ++n) write_vec(f, one_bodies[n]->Get(), 2 * vol);
     fclose(f);
   }
 
@@ -347,7 +372,7 @@ int run_ensemble(const KV& kv, bool timed_only) {
     for (int n = 0; n < N; ++n) propagator.Set(one_bodies[n]->Get(), n);
     for (int t = 0; t < T; ++t) {
       if (fp && j == 0 && t < dump_props) {
-        for (int n = 0; n < N; ++n) fwrite(props[n], sizeof(double), 2 * vol, fp);
+        for (int n = 0; n < N; ++n) write_vec(fp, props[n], 2 * vol);
       }
       if (mode == "slater2") {
         // production/slater_det2_trapped/main-no_cum.C:201-208: pair matrix from
@@ -371,8 +396,7 @@ int run_ensemble(const KV& kv, bool timed_only) {
       }
       if (fd) fwrite(&row[0], sizeof(complex<double>), nmeas, fd);
       if (ff && slices_done < dump_fields) {
-        Float* fl = lattice.Get();
-        fwrite(fl, sizeof(double), 2 * vol, ff);
+        write_vec(ff, lattice.Get(), 2 * vol);
       }
       for (size_t p = 0; p < hamiltonians.size(); ++p) hamiltonians[p]->Initialize();
       propagator.Run(hamiltonians);

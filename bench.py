@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--cluster", type=int, default=0, help="force the fused kernel's cluster size (0: autotuned)")
     ap.add_argument("--no-fused", action="store_true", help="pencil passes instead of the fused kernel")
     ap.add_argument("--split", type=int, default=-1, help="fused kernel lane split: -1 autotuned, 0, 1")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU path measurement")
     return ap.parse_args()
 
 
@@ -168,6 +169,52 @@ def run_reference(a):
     return 0
 
 
+# ------------------------------------------------------- plain FP64 GPU path
+def plain_fp64_gpu(a, ctx, idx, configs: int = 2, slices: int = 8):
+    """The reference's GPU call structure through the class API, in FP64:
+    one configuration at a time, Propagator::Run over [K, I, K] as separate
+    Kinetic / Interaction (FFT, multiply, FFT) launches, fields drawn per
+    slice by Lattice::Refresh, the Slater matrix by one overlap per slice and
+    the determinants of all leading minors -- the 'plain FP64 GPU path' the
+    batched FP32 path is compared with."""
+    import torch
+    import nrcps_b200 as nb
+
+    dims = (a.L,) * 3
+    vol = a.L ** 3
+    n = len(idx)
+    rng = nb.Random("RANLXS2", a.seed)
+    lat = nb.Lattice(dims, rng, "ZTWO", ctx)
+    inter = nb.Interaction(lat, 1.0, [0.019894367886486918], 1.0, 2.0)
+    kin = nb.Kinetic(dims, "PERFECT", 1.0, 0.5, 2.0, ctx)
+    prop = nb.Propagator(n, dims, "f64", ctx)
+    src = torch.zeros((n, vol), dtype=torch.complex128, device=ctx.device)
+    src[torch.arange(n), torch.as_tensor(idx, dtype=torch.long)] = 1
+    ham = [kin, inter, kin]
+
+    def one_config():
+        prop.get().b.copy_(src.reshape(prop.get().b.shape))
+        for _ in range(slices):
+            S = nb.overlap(src, prop.get().b.reshape(1, n, vol), ctx)
+            nb.slater_dets(S, ctx=ctx)
+            for h in ham:
+                h.initialize()
+            prop.run(ham)
+            lat.refresh()
+
+    one_config()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(configs):
+        one_config()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": configs * slices / (ms / 1000.0), "unit": UNIT,
+            "sample": f"{configs} configurations x {slices} slices, L={a.L}^3 N={n}, FP64, class-API call structure"}
+
+
 # -------------------------------------------------------------------- b200
 def run_b200(a):
     import ctypes
@@ -178,6 +225,7 @@ def run_b200(a):
 
     import nrcps_b200 as nb
     from nrcps_b200 import _capi as C
+    from nrcps_b200 import parallel
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -198,6 +246,7 @@ def run_b200(a):
     dims = (a.L,) * 3
     idx, _, _ = nb.momenta(dims, "PERFECT", 1.0, a.ef, 2.0)
     n_orb = len(idx)
+    # each rank runs its own stream, seeded seed + 491 * rank (src/random/random.C:88)
     job = nb.EnsembleJob(L=a.L, T=a.T, n_conf=a.configs, seed=a.seed, rank=rank, precision=a.precision,
                          fermi_energy=a.ef)
     ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
@@ -206,9 +255,9 @@ def run_b200(a):
     def step(i):
         dets = ens.run(i * a.configs)
         # production/slater_det/main.C:208-211 and :226: corr[n][t] += |det|^2, summed over ranks
-        corr.copy_((dets.real ** 2 + dets.imag ** 2).sum(0))
-        if world > 1:
-            dist.all_reduce(corr)
+        c = parallel.accumulate(dets, "slater")
+        parallel.global_sum(c)
+        corr.copy_(c.real.T)
         return dets
 
     def barrier():
@@ -306,13 +355,17 @@ def run_b200(a):
     e2e = {"value": world * a.configs * a.T * a.steps / (float(t.item()) / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": idx_host.numel() * 4, "d2h_bytes_per_step": dets_host.numel() * 16}
 
+    plain = plain_fp64_gpu(a, ctx, idx) if rank == 0 and not a.no_plain else None
+
     if rank == 0:
         cb = None if a.no_cpu_baseline else cpu_baseline(a, a.cpu_sample_slices, n_orb)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": a.precision, "data": "synthetic (device-drawn fields, plane-wave sources)",
                 "config": workload(a, n_orb), "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
-                "gpu_launches": launches_per_step * a.steps, "clocks": clocks.summary()}
+                "gpu_launches": launches_per_step * a.steps, "clocks": clocks.summary(),
+                "plain_fp64_gpu": plain,
+                "speedup_vs_plain_fp64_gpu": (value / world / plain["value"]) if plain else None}
         print(json.dumps(line))
     ens.close()
     if world > 1:

@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--cluster", type=int, default=0, help="force the fused kernel's cluster size (0: autotuned)")
     ap.add_argument("--no-fused", action="store_true", help="pencil passes instead of the fused kernel")
     ap.add_argument("--split", type=int, default=-1, help="fused kernel lane split: -1 autotuned, 0, 1")
+    ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 pull, 1 split, 2 push, 3 read-only")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU path measurement")
     return ap.parse_args()
 
@@ -242,6 +243,8 @@ def run_b200(a):
         ctx.set_option("fused.cluster", a.cluster)
     if a.split >= 0:
         ctx.set_option("fused.split", a.split)
+    if a.kind >= 0:
+        ctx.set_option("fused.kind", a.kind)
 
     dims = (a.L,) * 3
     idx, _, _ = nb.momenta(dims, "PERFECT", 1.0, a.ef, 2.0)

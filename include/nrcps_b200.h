@@ -88,7 +88,12 @@ const char *nrcps_version(void);
  *                      exists for the shape; 0: five pencil passes;
  *   "fused.cluster"    0 (default): autotuned cluster size; else force it;
  *   "fused.split"      -1 (default): autotuned; 0: one thread per pencil;
- *                      1: each pencil split over two lanes. */
+ *                      1: each pencil split over two lanes;
+ *   "fused.kind"       -1 (default): autotuned; 0: one thread per pencil,
+ *                      the x-pass reads and writes peers' shared memory;
+ *                      1: lane split; 2: whole regions move between CTAs
+ *                      by bulk copy; 3: as 2, with the slab prefetched into
+ *                      L2 instead of staged in shared memory. */
 nrcps_status nrcps_set_option(nrcps_context *ctx, const char *name, long value);
 /* Times every fused-kernel variant (cluster size, lane split) for (prec, L)
  * on this device and keeps the fastest for later calls; *cluster receives

@@ -109,6 +109,9 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
   } else if (n == "fused.split") {
     if (value < -1 || value > 1) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.split out of range");
     ctx->fused_split = (int)value;
+  } else if (n == "fused.kind") {
+    if (value < -1 || value > 3) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
+    ctx->fused_kind = (int)value;
   } else {
     return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "unknown option %s", name);
   }

@@ -97,6 +97,7 @@ struct Context {
   int fused_enabled = 1;  // single-pass cluster kernel where a variant exists
   int fused_cluster = 0;  // 0: autotuned / default cluster size
   int fused_split = -1;   // -1: autotuned; 0: one lane per pencil; 1: two lanes per pencil
+  int fused_kind = -1;    // -1: autotuned; else the fused kernel's kind (0..3)
   // FP32 copy of a kinetic table for nrcps_propagate(F32).
   int* dev_err = nullptr;  // device flag set by kernels whose bounded waits time out
   float2* kin_f32 = nullptr;  // (hi, lo) split of the last table

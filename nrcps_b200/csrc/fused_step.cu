@@ -456,14 +456,279 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
   if constexpr (C > 1) cluster.sync();
 }
 
-template <typename R, int L, int C, bool SPLIT = false>
+// ------------------------------------------------ cluster helpers
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Bounded wait with cluster-scope acquire: the awaited bytes were written
+// by other CTAs of the cluster.
+__device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_t parity, int* err) {
+  for (int i = 0; i < (1 << 24); ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  if (err) atomicExch(err, 1);
+  return false;
+}
+
+// Prefetch of a global range into L2 by the bulk copy engine (no completion).
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// ------------------------------------------------ bulk-copy exchange variant
+// Same passes, but both exchanges move whole padded regions with the bulk
+// copy engine (cp.async.bulk shared::cta -> shared::cluster), completing on
+// the receiver's mbarrier: no per-element remote access and no cluster
+// barrier in the loop.
+//
+// Shared memory per CTA: stage (HBM landing zone of the next slab), work
+// (x-slab c, region r = y-slab r) and recv (y-slab c, slot s = x-slab s).
+//   1. wait for the slab; k(p), DFT along y: stage -> work; prefetch the
+//      next slab into stage;
+//   2. DFT along z of the rows of work, in place; region r is copied to
+//      slot c of the recv of CTA r;
+//   3. wait for recv (C regions); DFT along x, times w, inverse DFT, in
+//      place; slot s is copied back to region c of the work of CTA s;
+//   4. wait for work; inverse DFT along z in place;
+//   5. inverse DFT along y, times k(p), streaming stores to HBM.
+// Buffer reuse needs no extra signal: slot s of recv is written only by
+// CTA s and copied back only to CTA s, so when s has received its results
+// (its work mbarrier) it knows that slot s of this CTA has been read out;
+// the same holds for region r of work with CTA r.  Every mbarrier wait is
+// bounded.
+template <typename R, int L, int C, bool STAGED = true>
+struct BulkShape {
+  using Base = FusedShape<R, L, C>;
+  static constexpr int THREADS = Base::THREADS;
+  static constexpr uint32_t REGION_BYTES = (uint32_t)(Base::REGION * sizeof(cplx<R>));
+  static constexpr uint32_t XBYTES = (uint32_t)(C * REGION_BYTES);       // one exchange, received
+  static constexpr uint32_t STAGE_BYTES = (uint32_t)(Base::STAGE * sizeof(cplx<R>));
+  static constexpr size_t SMEM = 128 + (STAGED ? STAGE_BYTES : 0) + 2 * (size_t)XBYTES;
+  static constexpr int CTAS = (int)(228 * 1024 / (SMEM + 1024));
+  static constexpr int WANT = (384 / THREADS) < 1 ? 1 : 384 / THREADS;
+  static constexpr int MIN_BLOCKS = CTAS < 1 ? 1 : (CTAS > WANT ? WANT : CTAS);
+  static_assert(REGION_BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
+  static_assert(XBYTES < (1u << 20), "mbarrier transaction count range");
+};
+
+// One bulk copy from this CTA's shared memory to a cluster peer's (dst and
+// bar are shared::cluster addresses), completing on the peer's mbarrier.
+__device__ __forceinline__ void bulk_to_peer(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst),
+               "r"(smem_u32(src)), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// STAGED = false: no stage buffer; the next slab is prefetched into L2 and
+// pass 1 reads it from there (two buffers instead of three per CTA).
+template <typename R, int L, int C, bool STAGED>
+__global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape<R, L, C, STAGED>::MIN_BLOCKS)
+    fused_step_bulk_kernel(FusedArgs f) {
+  using Sh = FusedShape<R, L, C>;
+  using Bs = BulkShape<R, L, C, STAGED>;
+  static_assert(C > 1, "the exchange is between CTAs of a cluster");
+  constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION;
+  constexpr int V = L * L * L;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar_hbm = reinterpret_cast<uint64_t*>(smem_raw);
+  uint64_t* bar_recv = bar_hbm + 1;
+  uint64_t* bar_work = bar_hbm + 2;
+  cplx<R>* stage = reinterpret_cast<cplx<R>*>(smem_raw + 128);
+  cplx<R>* work = stage + (STAGED ? Sh::STAGE : 0);
+  cplx<R>* recv = work + Sh::WORK;
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int c = (int)cluster.block_rank();
+  const long cluster_id = blockIdx.x / C;
+  const long n_clusters = gridDim.x / C;
+  const int tid = threadIdx.x;
+
+  auto off = [](int r, int xl, int yl, int z) { return r * REGION + (xl * S + yl) * LP + z; };
+  auto slab = [&](long orb) {
+    return reinterpret_cast<const cplx<R>*>(f.psi) + (size_t)orb * V + (size_t)c * S * L * L;
+  };
+
+  const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  R wp_hi, wp_lo, wm_hi, wm_lo;
+  split<R>(f.w_plus, wp_hi, wp_lo);
+  split<R>(f.w_minus, wm_hi, wm_lo);
+
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar_hbm)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar_recv)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar_work)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  cluster.sync();  // every CTA's mbarriers are initialised before any copy targets them
+  uint32_t parity = 0;
+  long orb = cluster_id;
+  if (tid == 0 && orb < f.n_orb_total) {
+    if constexpr (STAGED) bulk_load(stage, slab(orb), Bs::STAGE_BYTES, bar_hbm);
+    else prefetch_l2(slab(orb), Bs::STAGE_BYTES);
+  }
+
+  for (; orb < f.n_orb_total; orb += n_clusters) {
+    const long conf = orb / f.batch;
+    const uint64_t kb = f.off0 + (uint64_t)conf * f.conf_stride;
+    cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
+    cplx<R> x[L];
+    if constexpr (STAGED) {
+      mbar_wait_bounded(bar_hbm, parity, f.err);
+    } else if (tid == 0 && orb + n_clusters < f.n_orb_total) {
+      prefetch_l2(slab(orb + n_clusters), Bs::STAGE_BYTES);
+    }
+    // ---- 1. k(p), forward DFT along y from the slab: thread -> (xl, z)
+    {
+      const int z = tid % L, xl = tid / L;
+      const int site0 = (c * S + xl) * L * L + z;
+      if constexpr (STAGED) {
+#pragma unroll
+        for (int y = 0; y < L; ++y) x[y] = apply_kin<R>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
+      } else {
+        const cplx<R>* src = slab(orb);
+#pragma unroll
+        for (int y = 0; y < L; ++y) {
+          cplx<R> v;
+          if constexpr (sizeof(R) == 4) {
+            float2 t = __ldcg(reinterpret_cast<const float2*>(src) + (xl * L + y) * L + z);
+            v = cplx<R>{t.x, t.y};
+          } else {
+            double2 t = __ldcg(reinterpret_cast<const double2*>(src) + (xl * L + y) * L + z);
+            v = cplx<R>{t.x, t.y};
+          }
+          x[y] = apply_kin<R>(f, site0 + y * L, v);
+        }
+      }
+      fft::Dft<L, -1, R>::run(x);
+#pragma unroll
+      for (int y = 0; y < L; ++y) work[off(y / S, xl, y % S, z)] = x[y];
+    }
+    __syncthreads();
+    if constexpr (STAGED) {
+      if (tid == 0 && orb + n_clusters < f.n_orb_total) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        bulk_load(stage, slab(orb + n_clusters), Bs::STAGE_BYTES, bar_hbm);
+      }
+    }
+    // ---- 2. forward DFT along z in place: thread -> (xl, y); then region r -> CTA r
+    {
+      const int y = tid % L, xl = tid / L;
+      cplx<R>* row = work + off(y / S, xl, y % S, 0);
+#pragma unroll
+      for (int j = 0; j < L; ++j) x[j] = row[j];
+      fft::Dft<L, -1, R>::run(x);
+#pragma unroll
+      for (int j = 0; j < L; ++j) row[j] = x[j];
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> bulk copy reads
+    __syncthreads();
+    if (tid < C) {
+      const uint32_t dst = mapa_u32(smem_u32(recv + c * REGION), (uint32_t)tid);
+      const uint32_t bar = mapa_u32(smem_u32(bar_recv), (uint32_t)tid);
+      bulk_to_peer(dst, work + tid * REGION, Bs::REGION_BYTES, bar);
+    }
+    if (tid == 0) expect_tx(bar_recv, Bs::XBYTES);
+    mbar_wait_cluster_bounded(bar_recv, parity, f.err);
+    // ---- 3. x: forward DFT, times w, backward DFT on the pencils of y-slab c, in recv
+    {
+      const int z = tid % L, yl = tid / L;
+      const int site0 = (c * S + yl) * L + z;
+#pragma unroll
+      for (int xx = 0; xx < L; ++xx) x[xx] = recv[off(xx / S, xx % S, yl, z)];
+      fft::Dft<L, -1, R>::run(x);
+      if (z2_fast) {
+        const uint64_t k0 = kb + (uint64_t)site0;
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
+        const int bit = (int)(k0 & 31);
+#pragma unroll
+        for (int xx = 0; xx < L; ++xx) {
+          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+          x[xx] = scale2<R>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+        }
+      } else {
+#pragma unroll
+        for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
+      }
+      fft::Dft<L, +1, R>::run(x);
+#pragma unroll
+      for (int xx = 0; xx < L; ++xx) recv[off(xx / S, xx % S, yl, z)] = x[xx];
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid < C) {
+      const uint32_t dst = mapa_u32(smem_u32(work + c * REGION), (uint32_t)tid);
+      const uint32_t bar = mapa_u32(smem_u32(bar_work), (uint32_t)tid);
+      bulk_to_peer(dst, recv + tid * REGION, Bs::REGION_BYTES, bar);
+    }
+    if (tid == 0) expect_tx(bar_work, Bs::XBYTES);
+    mbar_wait_cluster_bounded(bar_work, parity, f.err);
+    parity ^= 1u;
+    // ---- 4. backward DFT along z in place
+    {
+      const int y = tid % L, xl = tid / L;
+      cplx<R>* row = work + off(y / S, xl, y % S, 0);
+#pragma unroll
+      for (int j = 0; j < L; ++j) x[j] = row[j];
+      fft::Dft<L, +1, R>::run(x);
+#pragma unroll
+      for (int j = 0; j < L; ++j) row[j] = x[j];
+    }
+    __syncthreads();
+    // ---- 5. backward DFT along y, times k(p), streaming stores
+    {
+      const int z = tid % L, xl = tid / L;
+      const int site0 = (c * S + xl) * L * L + z;
+#pragma unroll
+      for (int y = 0; y < L; ++y) x[y] = work[off(y / S, xl, y % S, z)];
+      fft::Dft<L, +1, R>::run(x);
+#pragma unroll
+      for (int y = 0; y < L; ++y) {
+        cplx<R> v = apply_kin<R>(f, site0 + y * L, x[y]);
+        if constexpr (sizeof(R) == 4)
+          __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(v.re, v.im));
+        else
+          __stcs(reinterpret_cast<double2*>(gpsi) + site0 + y * L, make_double2(v.re, v.im));
+      }
+    }
+    // Pass 1 of the next orbital writes, per thread, the work elements this
+    // thread read in pass 5; no copy reads work between pass 4 and the next
+    // pass 2 (all copies out of work completed before this CTA's recv filled).
+  }
+  cluster.sync();  // no CTA leaves while a copy may still target it
+}
+
+// KIND 0: one lane per pencil, exchange through peers' shared memory;
+// 1: two lanes per pencil; 2: bulk-copy exchange, staged slab; 3: bulk-copy
+// exchange, slab prefetched into L2.
+template <typename R, int L, int C, int KIND = 0>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
-  constexpr int THREADS = SPLIT ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
+  constexpr int THREADS = KIND == 1 ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
+  constexpr size_t SMEM = KIND == 2   ? BulkShape<R, L, C, true>::SMEM
+                          : KIND == 3 ? BulkShape<R, L, C, false>::SMEM
+                                      : Sh::SMEM;
   void (*kern)(FusedArgs);
-  if constexpr (SPLIT) kern = fused_step_split_kernel<R, L, C>;
+  if constexpr (KIND == 1) kern = fused_step_split_kernel<R, L, C>;
+  else if constexpr (KIND == 2) kern = fused_step_bulk_kernel<R, L, C, true>;
+  else if constexpr (KIND == 3) kern = fused_step_bulk_kernel<R, L, C, false>;
   else kern = fused_step_kernel<R, L, C>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::SMEM);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");
   if (C > 8) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -478,7 +743,7 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.blockDim = dim3(THREADS);
-  cfg.dynamicSmemBytes = Sh::SMEM;
+  cfg.dynamicSmemBytes = SMEM;
   cfg.stream = ctx->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
@@ -506,39 +771,46 @@ struct FusedVariant {
   int prec;  // nrcps_precision
   int L;
   int C;
-  int split;  // 1: two lanes per pencil
+  int kind;  // 0: exchange through peers' shared memory; 1: lane split; 2/3: bulk-copy exchange
   FusedLauncher fn;
 };
 
-// Instantiated (precision, L, cluster size) variants.  Shared memory per CTA
-// is the staged slab (L/C) L^2 plus C padded regions of (L/C)^2 (L+1) + L/C
-// complex values; cluster sizes are chosen so that 2-4 CTAs share an SM.
-// Sizes above 8 are non-portable cluster shapes (allowed on B200).
+// Instantiated (precision, L, cluster size, kind) variants.  Shared memory
+// per CTA is one or two buffers of C padded regions of (L/C)^2 (L+1) + L/C
+// complex values, plus the staged slab (L/C) L^2 for kinds 0-2; cluster
+// sizes are chosen so that 2-4 CTAs share an SM.  Sizes above 8 are
+// non-portable cluster shapes (allowed on B200).
 // Listed best-first per (precision, L) as measured on B200 (the first entry
 // is the default before autotuning).
 static const FusedVariant kVariants[] = {
     {NRCPS_F32, 8, 1, 0, launch_fused<float, 8, 1>},
     {NRCPS_F32, 16, 1, 0, launch_fused<float, 16, 1>},
+    {NRCPS_F32, 16, 2, 2, launch_fused<float, 16, 2, 2>},
     {NRCPS_F32, 16, 2, 0, launch_fused<float, 16, 2>},
-    {NRCPS_F32, 16, 1, 1, launch_fused<float, 16, 1, true>},
-    {NRCPS_F32, 16, 2, 1, launch_fused<float, 16, 2, true>},
+    {NRCPS_F32, 16, 1, 1, launch_fused<float, 16, 1, 1>},
+    {NRCPS_F32, 24, 3, 2, launch_fused<float, 24, 3, 2>},
+    {NRCPS_F32, 24, 4, 2, launch_fused<float, 24, 4, 2>},
     {NRCPS_F32, 24, 3, 0, launch_fused<float, 24, 3>},
     {NRCPS_F32, 24, 4, 0, launch_fused<float, 24, 4>},
-    {NRCPS_F32, 24, 3, 1, launch_fused<float, 24, 3, true>},
+    {NRCPS_F32, 32, 8, 3, launch_fused<float, 32, 8, 3>},
+    {NRCPS_F32, 32, 16, 3, launch_fused<float, 32, 16, 3>},
     {NRCPS_F32, 32, 8, 0, launch_fused<float, 32, 8>},
-    {NRCPS_F32, 32, 8, 1, launch_fused<float, 32, 8, true>},
-    {NRCPS_F32, 32, 16, 1, launch_fused<float, 32, 16, true>},
-    {NRCPS_F32, 32, 16, 0, launch_fused<float, 32, 16>},
+    {NRCPS_F32, 32, 8, 2, launch_fused<float, 32, 8, 2>},
+    {NRCPS_F32, 32, 8, 1, launch_fused<float, 32, 8, 1>},
     {NRCPS_F32, 48, 16, 0, launch_fused<float, 48, 16>},
-    {NRCPS_F32, 48, 16, 1, launch_fused<float, 48, 16, true>},
+    {NRCPS_F32, 48, 16, 3, launch_fused<float, 48, 16, 3>},
+    {NRCPS_F32, 48, 16, 1, launch_fused<float, 48, 16, 1>},
     {NRCPS_F64, 8, 1, 0, launch_fused<double, 8, 1>},
+    {NRCPS_F64, 16, 2, 2, launch_fused<double, 16, 2, 2>},
     {NRCPS_F64, 16, 2, 0, launch_fused<double, 16, 2>},
-    {NRCPS_F64, 16, 2, 1, launch_fused<double, 16, 2, true>},
+    {NRCPS_F64, 16, 2, 1, launch_fused<double, 16, 2, 1>},
+    {NRCPS_F64, 24, 4, 2, launch_fused<double, 24, 4, 2>},
     {NRCPS_F64, 24, 4, 0, launch_fused<double, 24, 4>},
-    {NRCPS_F64, 32, 8, 0, launch_fused<double, 32, 8>},
+    {NRCPS_F64, 32, 16, 3, launch_fused<double, 32, 16, 3>},
     {NRCPS_F64, 32, 16, 0, launch_fused<double, 32, 16>},
-    {NRCPS_F64, 32, 8, 1, launch_fused<double, 32, 8, true>},
-    {NRCPS_F64, 32, 16, 1, launch_fused<double, 32, 16, true>},
+    {NRCPS_F64, 32, 8, 0, launch_fused<double, 32, 8>},
+    {NRCPS_F64, 32, 16, 2, launch_fused<double, 32, 16, 2>},
+    {NRCPS_F64, 32, 8, 1, launch_fused<double, 32, 8, 1>},
 };
 static const int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -568,7 +840,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   int dev = ctx->device & 15;
   if (L < 64 && g_choice[dev][prec][L] >= 0) {
     if (chosen_cluster)
-      *chosen_cluster = kVariants[g_choice[dev][prec][L]].C * (kVariants[g_choice[dev][prec][L]].split ? -1 : 1);
+      *chosen_cluster = kVariants[g_choice[dev][prec][L]].C * (kVariants[g_choice[dev][prec][L]].kind == 1 ? -1 : 1);
     return NRCPS_OK;
   }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -640,7 +912,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   cudaFree(kin);
   cudaFree(bits);
   if (best_i >= 0 && L < 64) g_choice[dev][prec][L] = best_i;
-  if (chosen_cluster && best_i >= 0) *chosen_cluster = kVariants[best_i].C * (kVariants[best_i].split ? -1 : 1);
+  if (chosen_cluster && best_i >= 0) *chosen_cluster = kVariants[best_i].C * (kVariants[best_i].kind == 1 ? -1 : 1);
   return NRCPS_OK;
 }
 
@@ -670,18 +942,19 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   const int L = d[0];
   int pick = -1;
   const int want_split = ctx->fused_split;  // -1: any
-  if (cluster > 0 || want_split >= 0) {
+  const int want_kind = ctx->fused_kind;    // -1: any
+  auto admissible = [&](const FusedVariant& v) {
+    return (cluster <= 0 || v.C == cluster) && (want_split < 0 || (v.kind == 1) == (want_split == 1)) &&
+           (want_kind < 0 || v.kind == want_kind);
+  };
+  if (cluster > 0 || want_split >= 0 || want_kind >= 0) {
     const int tuned = g_choice[ctx->device & 15][prec][L];
-    if (tuned >= 0 && (cluster <= 0 || kVariants[tuned].C == cluster) &&
-        (want_split < 0 || kVariants[tuned].split == want_split))
-      pick = tuned;
+    if (tuned >= 0 && admissible(kVariants[tuned])) pick = tuned;
     for (int i = 0; i < kNumVariants && pick < 0; ++i)
-      if (kVariants[i].prec == prec && kVariants[i].L == L && (cluster <= 0 || kVariants[i].C == cluster) &&
-          (want_split < 0 || kVariants[i].split == want_split))
-        pick = i;
+      if (kVariants[i].prec == prec && kVariants[i].L == L && admissible(kVariants[i])) pick = i;
     if (pick < 0)
-      return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "no fused variant with cluster size %d, split %d", cluster,
-                       want_split);
+      return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "no fused variant with cluster size %d, split %d, kind %d",
+                       cluster, want_split, want_kind);
   } else {
     pick = g_choice[ctx->device & 15][prec][L];
     for (int i = 0; i < kNumVariants && pick < 0; ++i)  // default: the first listed variant

@@ -379,6 +379,32 @@ def test_lane_split_variant_agrees(ctx, L, precision):
     assert max_norm_err(outs[1], outs[0]) < tol
 
 
+_EXCHANGE_VARIANTS = [(2, "f32", 16, 2), (2, "f32", 24, 3), (2, "f32", 24, 4), (2, "f32", 32, 8), (2, "f64", 16, 2),
+                      (2, "f64", 24, 4), (2, "f64", 32, 16), (3, "f32", 32, 8), (3, "f32", 32, 16),
+                      (3, "f32", 48, 16), (3, "f64", 32, 16)]
+
+
+@pytest.mark.parametrize("kind,precision,L,cluster", _EXCHANGE_VARIANTS)
+def test_exchange_variants_are_bit_identical(ctx, kind, precision, L, cluster):
+    """The bulk-copy exchanges (kinds 2 and 3) move the same values through
+    the same arithmetic as the peer-access kernel (kind 0): results agree
+    bit for bit."""
+    psi, kinv, bits = _random_step_inputs(ctx, L, 3, 5, precision, seed=3)
+    try:
+        ctx.set_option("fused.kind", 0)
+        ref = psi.clone()
+        nb.propagate(ref, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.set_option("fused.kind", kind)
+        ctx.set_option("fused.cluster", cluster)
+        q = psi.clone()
+        nb.propagate(q, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.synchronize()
+        assert torch.equal(q, ref)
+    finally:
+        ctx.set_option("fused.cluster", 0)
+        ctx.set_option("fused.kind", -1)
+
+
 def test_synchronize_reports_no_timeout(ctx):
     psi, kinv, bits = _random_step_inputs(ctx, 32, 2, 2, "f32")
     nb.propagate(psi, 2, kinv, bits, 0.5, ctx=ctx)

@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--cluster", type=int, default=0, help="force the fused kernel's cluster size (0: autotuned)")
     ap.add_argument("--no-fused", action="store_true", help="pencil passes instead of the fused kernel")
     ap.add_argument("--split", type=int, default=-1, help="fused kernel lane split: -1 autotuned, 0, 1")
-    ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 pull, 1 split, 2 push, 3 read-only")
+    ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 peer access, 1 split, 2 bulk staged, 3 bulk L2, 4-6 packed 0/2/3")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU path measurement")
     return ap.parse_args()
 

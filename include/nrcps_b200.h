@@ -93,7 +93,13 @@ const char *nrcps_version(void);
  *                      the x-pass reads and writes peers' shared memory;
  *                      1: lane split; 2: whole regions move between CTAs
  *                      by bulk copy; 3: as 2, with the slab prefetched into
- *                      L2 instead of staged in shared memory. */
+ *                      L2 instead of staged in shared memory; 4, 5, 6: kinds
+ *                      0, 2, 3 with packed FP32x2 transforms (two
+ *                      half-length DFTs per instruction; FP32 only);
+ *   "overlap.tc"       1 (default): dense-source overlaps of FP32 orbitals
+ *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
+ *                      accumulation) where V is a multiple of 16; 0: the
+ *                      CUDA-core kernel with FP64 accumulation. */
 nrcps_status nrcps_set_option(nrcps_context *ctx, const char *name, long value);
 /* Times every fused-kernel variant (cluster size, lane split) for (prec, L)
  * on this device and keeps the fastest for later calls; *cluster receives

@@ -79,6 +79,7 @@ extern "C" nrcps_status nrcps_destroy(nrcps_context* ctx) {
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->gen_args) cudaFree(ctx->gen_args);
   if (ctx->kin_f32) cudaFree(ctx->kin_f32);
+  if (ctx->tc_split) cudaFree(ctx->tc_split);
   if (ctx->dev_err) cudaFree(ctx->dev_err);
   delete ctx;
   return NRCPS_OK;
@@ -110,8 +111,10 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
     if (value < -1 || value > 1) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.split out of range");
     ctx->fused_split = (int)value;
   } else if (n == "fused.kind") {
-    if (value < -1 || value > 3) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
+    if (value < -1 || value > 6) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
     ctx->fused_kind = (int)value;
+  } else if (n == "overlap.tc") {
+    ctx->overlap_tc = value != 0;
   } else {
     return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "unknown option %s", name);
   }

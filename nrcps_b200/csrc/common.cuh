@@ -97,7 +97,11 @@ struct Context {
   int fused_enabled = 1;  // single-pass cluster kernel where a variant exists
   int fused_cluster = 0;  // 0: autotuned / default cluster size
   int fused_split = -1;   // -1: autotuned; 0: one lane per pencil; 1: two lanes per pencil
-  int fused_kind = -1;    // -1: autotuned; else the fused kernel's kind (0..3)
+  int fused_kind = -1;    // -1: autotuned; else the fused kernel's kind (0..6)
+  int overlap_tc = 1;     // 1: tensor-core overlap for FP32 orbitals where the shape allows; 0: CUDA cores
+  // TF32 hi / lo split of the sources for nrcps_overlap's tensor-core path (grown on demand)
+  void* tc_split = nullptr;
+  size_t tc_split_bytes = 0;
   // FP32 copy of a kinetic table for nrcps_propagate(F32).
   int* dev_err = nullptr;  // device flag set by kernels whose bounded waits time out
   float2* kin_f32 = nullptr;  // (hi, lo) split of the last table
@@ -116,6 +120,13 @@ nrcps_status check_launch(nrcps_context* ctx, const char* what);
 void* scratch(nrcps_context* ctx, size_t bytes, nrcps_status* st);
 
 inline long vol_of(const int dims[3]) { return (long)dims[0] * dims[1] * dims[2]; }
+
+// tensor-core overlap (overlap_tc.cu)
+bool overlap_tc_supported(long vol, int ns, int nt, int nconf);
+size_t overlap_tc_split_bytes(int ns, long vol);
+nrcps_status overlap_tc_prepare(nrcps_context* ctx, const double* src, int ns, long vol, float* split);
+nrcps_status overlap_tc(nrcps_context* ctx, const float* split, int ns, const void* psi, int nt, int nconf, long vol,
+                        double* S);
 
 inline unsigned grid_for(long n, int block, long cap = 148L * 64) {
   long g = (n + block - 1) / block;

@@ -43,6 +43,7 @@ struct nrcps_ensemble {
   size_t esize = 0;  // bytes per complex orbital entry
   void* psi = nullptr;
   double* src = nullptr;
+  float* src_split = nullptr;  // TF32 hi/lo sources of the tensor-core overlap (FP32 orbitals)
   int* pw_index = nullptr;
   double* kinv = nullptr;
   float2* kinv_f = nullptr;  // (hi, lo) split of kinv
@@ -150,6 +151,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
     // -------- measurement at slice t (before the step, main.C:204-211)
     if (j.mode == 0) {
       if (e->pw_index) NRCPS_TRY(gather_impl(ctx, e->pw_index, N, e->psi, N, nc, vol, prec, e->S));
+      else if (e->src_split) NRCPS_TRY(overlap_tc(ctx, e->src_split, N, e->psi, N, nc, vol, e->S));
       else NRCPS_TRY(overlap_impl(ctx, e->src, N, e->psi, N, nc, vol, prec, e->S));
       NRCPS_TRY(slater_dets_impl(ctx, e->S, nullptr, N, nc, 0, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
                                  e->lu_scr));
@@ -158,6 +160,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
     } else {
       NRCPS_TRY(pair_impl(ctx, e->psi, e->psi, N, nc, vol, e->w, e->opp, prec, e->S));
       if (e->pw_index) NRCPS_TRY(gather_impl(ctx, e->pw_index, N, e->psi, N, nc, vol, prec, e->P1));
+      else if (e->src_split) NRCPS_TRY(overlap_tc(ctx, e->src_split, N, e->psi, N, nc, vol, e->P1));
       else NRCPS_TRY(overlap_impl(ctx, e->src, N, e->psi, N, nc, vol, prec, e->P1));
       NRCPS_TRY(slater_dets_impl(ctx, e->S, e->P1, N, nc, 1, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
                                  e->lu_scr));
@@ -269,6 +272,11 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   } else {
     if ((st = dalloc(ctx, &e->src, 16 * (size_t)N * V)) || (st = upload(ctx, e->src, sources, 16 * (size_t)N * V)))
       return fail(st);
+    if (job->precision == NRCPS_F32 && ctx->overlap_tc && overlap_tc_supported(V, N, N, nc)) {
+      if ((st = dalloc(ctx, (char**)&e->src_split, overlap_tc_split_bytes(N, V))) ||
+          (st = overlap_tc_prepare(ctx, e->src, N, V, e->src_split)))
+        return fail(st);
+    }
   }
   if (job->mode == 1) {
     if ((st = dalloc(ctx, &e->w, 8 * V)) || (st = upload(ctx, e->w, w, 8 * V))) return fail(st);
@@ -363,7 +371,7 @@ extern "C" nrcps_status nrcps_ensemble_destroy(nrcps_ensemble* e) {
   if (e->ctx) cudaStreamSynchronize(e->ctx->stream);
   if (e->exec) cudaGraphExecDestroy(e->exec);
   if (e->graph) cudaGraphDestroy(e->graph);
-  void* bufs[] = {e->psi, e->src, e->pw_index, e->kinv, e->kinv_f, e->pos, e->itab, e->w, e->opp,
+  void* bufs[] = {e->psi, e->src, e->src_split, e->pw_index, e->kinv, e->kinv_f, e->pos, e->itab, e->w, e->opp,
                   e->bits, e->phi, e->fld, e->S, e->P1, e->lu_scr, e->qr_G, e->qr_logR};
   for (void* b : bufs)
     if (b) cudaFree(b);

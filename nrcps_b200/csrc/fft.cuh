@@ -250,6 +250,170 @@ struct Dft {
   }
 };
 
+// ------------------------------------------- packed FP32x2 transforms
+// Two independent complex sequences carried in the two lanes of float2
+// registers (re = (re_0, re_1), im = (im_0, im_1)), so that every butterfly
+// add and every twiddle product is one sm_100 packed instruction
+// (FADD2 / FMUL2 / FFMA2) for both sequences.  The structure and the
+// constants are those of Dft above; only the issue count changes.
+struct cpk {
+  float2 re, im;
+};
+
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b with one rounding: b * (-1) is exact inside the fused multiply-add
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ cpk padd(cpk a, cpk b) { return cpk{padd(a.re, b.re), padd(a.im, b.im)}; }
+__device__ __forceinline__ cpk psub(cpk a, cpk b) { return cpk{psub(a.re, b.re), psub(a.im, b.im)}; }
+
+// x * W_N^K (lane-uniform twiddle)
+template <int N, int K, int SIGN>
+__device__ __forceinline__ cpk ptwiddle(cpk x) {
+  constexpr int k = ((K % N) + N) % N;
+  if constexpr (k == 0) {
+    return x;
+  } else if constexpr ((4 * k) % N == 0) {
+    constexpr int q = (4 * k) / N;
+    constexpr int qs = SIGN > 0 ? q : (4 - q) % 4;
+    const float2 z = make_float2(0.f, 0.f);
+    if constexpr (qs == 1) return cpk{psub(z, x.im), x.re};
+    else if constexpr (qs == 2) return cpk{psub(z, x.re), psub(z, x.im)};
+    else return cpk{x.im, psub(z, x.re)};
+  } else {
+    constexpr CSf w = unit_root_f32(k, N);
+    constexpr float c = w.c;
+    constexpr float s = SIGN > 0 ? w.s : -w.s;
+    const float2 u = __fmul2_rn(x.im, make_float2(-s, -s));
+    const float2 v = __fmul2_rn(x.re, make_float2(s, s));
+    return cpk{__ffma2_rn(x.re, make_float2(c, c), u), __ffma2_rn(x.im, make_float2(c, c), v)};
+  }
+}
+
+template <int P, int SIGN>
+struct PButterfly;
+
+template <int SIGN>
+struct PButterfly<2, SIGN> {
+  static __device__ __forceinline__ void run(cpk* t) {
+    cpk a = t[0], b = t[1];
+    t[0] = padd(a, b);
+    t[1] = psub(a, b);
+  }
+};
+
+template <int SIGN>
+struct PButterfly<4, SIGN> {
+  static __device__ __forceinline__ void run(cpk* t) {
+    cpk s02 = padd(t[0], t[2]), d02 = psub(t[0], t[2]);
+    cpk s13 = padd(t[1], t[3]), d = psub(t[1], t[3]);
+    t[0] = padd(s02, s13);
+    t[2] = psub(s02, s13);
+    // d02 +- SIGN i d, with the multiplication by i folded into the adds
+    if constexpr (SIGN > 0) {
+      t[1] = cpk{psub(d02.re, d.im), padd(d02.im, d.re)};
+      t[3] = cpk{padd(d02.re, d.im), psub(d02.im, d.re)};
+    } else {
+      t[1] = cpk{padd(d02.re, d.im), psub(d02.im, d.re)};
+      t[3] = cpk{psub(d02.re, d.im), padd(d02.im, d.re)};
+    }
+  }
+};
+
+template <int SIGN>
+struct PButterfly<3, SIGN> {
+  static __device__ __forceinline__ void run(cpk* t) {
+    constexpr float c = -0.5f;
+    constexpr float s = unit_root_f32(1, 3).s;
+    cpk u = padd(t[1], t[2]);
+    cpk v = psub(t[1], t[2]);
+    cpk m{__ffma2_rn(u.re, make_float2(c, c), t[0].re), __ffma2_rn(u.im, make_float2(c, c), t[0].im)};
+    cpk sv{__fmul2_rn(v.re, make_float2(s, s)), __fmul2_rn(v.im, make_float2(s, s))};
+    t[0] = padd(t[0], u);
+    if constexpr (SIGN > 0) {  // m +- i sv
+      t[1] = cpk{psub(m.re, sv.im), padd(m.im, sv.re)};
+      t[2] = cpk{padd(m.re, sv.im), psub(m.im, sv.re)};
+    } else {
+      t[1] = cpk{padd(m.re, sv.im), psub(m.im, sv.re)};
+      t[2] = cpk{psub(m.re, sv.im), padd(m.im, sv.re)};
+    }
+  }
+};
+
+// In-place DFT of two sequences at once (natural order in and out).
+template <int N, int SIGN>
+struct PDft {
+  static __device__ __forceinline__ void run(cpk* x) {
+    constexpr int P = Radix<N>::value;
+    constexpr int M = N / P;
+    if constexpr (N == 1) {
+      return;
+    } else if constexpr (M == 1) {
+      PButterfly<P, SIGN>::run(x);
+    } else {
+      cpk s[P][M];
+#pragma unroll
+      for (int q = 0; q < P; ++q)
+#pragma unroll
+        for (int j = 0; j < M; ++j) s[q][j] = x[j * P + q];
+#pragma unroll
+      for (int q = 0; q < P; ++q) PDft<M, SIGN>::run(s[q]);
+      static_for<M>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        cpk t[P];
+        static_for<P>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          t[q] = ptwiddle<N, q * k, SIGN>(s[q][k]);
+        });
+        PButterfly<P, SIGN>::run(t);
+#pragma unroll
+        for (int ss = 0; ss < P; ++ss) x[k + ss * M] = t[ss];
+      });
+    }
+  }
+};
+
+// Length-N DFT of one FP32 pencil (N even) through the packed half-length
+// transform.  Decimation in time: the even and odd subsequences ride in the
+// two lanes of one length-N/2 packed DFT, then one scalar radix-2 stage
+// X[k] = E[k] + W^k O[k], X[k + N/2] = E[k] - W^k O[k].
+template <int N, int SIGN>
+__device__ __forceinline__ void dft_packed(cplx<float>* x) {
+  constexpr int H = N / 2;
+  cpk e[H];
+#pragma unroll
+  for (int m = 0; m < H; ++m) {
+    e[m].re = make_float2(x[2 * m].re, x[2 * m + 1].re);
+    e[m].im = make_float2(x[2 * m].im, x[2 * m + 1].im);
+  }
+  PDft<H, SIGN>::run(e);
+  static_for<H>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    const cplx<float> E{e[k].re.x, e[k].im.x};
+    const cplx<float> t = twiddle<N, k, SIGN, float>(cplx<float>{e[k].re.y, e[k].im.y});
+    x[k] = cplx<float>{E.re + t.re, E.im + t.im};
+    x[k + H] = cplx<float>{E.re - t.re, E.im - t.im};
+  });
+}
+
+// Dispatch: the packed transform for FP32 pencils of even length when PK.
+template <int N, int SIGN, typename R, bool PK>
+__device__ __forceinline__ void dft(cplx<R>* x) {
+  if constexpr (PK && sizeof(R) == 4 && N % 2 == 0 && N >= 4) dft_packed<N, SIGN>(reinterpret_cast<cplx<float>*>(x));
+  else Dft<N, SIGN, R>::run(x);
+}
+
+// x * (hi + lo) on both components at once, correctly rounded as mul2:
+// q = -x hi (exact negation of the rounded product), e = x hi + q exactly,
+// result = (x lo + e) - q with one rounding each.
+__device__ __forceinline__ cplx<float> scale2_packed(cplx<float> x, float hi, float lo) {
+  const float2 v = make_float2(x.re, x.im);
+  const float2 q = __fmul2_rn(v, make_float2(-hi, -hi));
+  const float2 e = __ffma2_rn(v, make_float2(hi, hi), q);
+  const float2 g = __ffma2_rn(v, make_float2(lo, lo), e);
+  const float2 r = __ffma2_rn(q, make_float2(-1.f, -1.f), g);
+  return cplx<float>{r.x, r.y};
+}
+
 // -------------------------------------------------- pencils split over lanes
 // A pencil of N values held by two lanes (lane and lane ^ 16), h = 0 / 1.
 //

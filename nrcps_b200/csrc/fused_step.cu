@@ -83,15 +83,23 @@ __device__ __forceinline__ cplx<R> apply_w_general(const FusedArgs& f, uint64_t 
   return y;
 }
 
-template <typename R>
+template <typename R, bool PK = false>
 __device__ __forceinline__ cplx<R> apply_kin(const FusedArgs& f, int site, cplx<R> x) {
   if constexpr (sizeof(R) == 4) {
     float2 k = __ldg(f.kin_f + site);
-    return scale2<R>(x, k.x, k.y);
+    if constexpr (PK) return fft::scale2_packed(x, k.x, k.y);
+    else return scale2<R>(x, k.x, k.y);
   } else {
     R k = __ldg(f.kin_d + site);
     return cplx<R>{x.re * k, x.im * k};
   }
+}
+
+// x * (hi + lo), packed when PK (FP32 only)
+template <typename R, bool PK>
+__device__ __forceinline__ cplx<R> scale_w(cplx<R> x, R hi, R lo) {
+  if constexpr (PK && sizeof(R) == 4) return fft::scale2_packed(x, hi, lo);
+  else return scale2<R>(x, hi, lo);
 }
 
 template <typename R, int L, int C>
@@ -149,7 +157,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
-template <typename R, int L, int C>
+template <typename R, int L, int C, bool PK = false>
 __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L, C>::MIN_BLOCKS)
     fused_step_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
@@ -196,8 +204,8 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
       const int z = tid % L, xl = tid / L;
       const int site0 = (c * S + xl) * L * L + z;
 #pragma unroll
-      for (int y = 0; y < L; ++y) x[y] = apply_kin<R>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
-      fft::Dft<L, -1, R>::run(x);
+      for (int y = 0; y < L; ++y) x[y] = apply_kin<R, PK>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
+      fft::dft<L, -1, R, PK>(x);
 #pragma unroll
       for (int y = 0; y < L; ++y) sm[off(y / S, xl, y % S, z)] = x[y];
     }
@@ -213,7 +221,7 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
       cplx<R>* row = sm + off(y / S, xl, y % S, 0);
 #pragma unroll
       for (int j = 0; j < L; ++j) x[j] = row[j];
-      fft::Dft<L, -1, R>::run(x);
+      fft::dft<L, -1, R, PK>(x);
 #pragma unroll
       for (int j = 0; j < L; ++j) row[j] = x[j];
     }
@@ -231,7 +239,7 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
       const int site0 = (c * S + yl) * L + z;  // site of x = 0
 #pragma unroll
       for (int xx = 0; xx < L; ++xx) x[xx] = base[xx / S][((xx % S) * S + yl) * LP + z];
-      fft::Dft<L, -1, R>::run(x);
+      fft::dft<L, -1, R, PK>(x);
       if (z2_fast) {
         const uint64_t k0 = kb + (uint64_t)site0;
         const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
@@ -239,13 +247,13 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
 #pragma unroll
         for (int xx = 0; xx < L; ++xx) {
           const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
-          x[xx] = scale2<R>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
         }
       } else {
 #pragma unroll
         for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
       }
-      fft::Dft<L, +1, R>::run(x);
+      fft::dft<L, +1, R, PK>(x);
 #pragma unroll
       for (int xx = 0; xx < L; ++xx) base[xx / S][((xx % S) * S + yl) * LP + z] = x[xx];
     }
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
       cplx<R>* row = sm + off(y / S, xl, y % S, 0);
 #pragma unroll
       for (int j = 0; j < L; ++j) x[j] = row[j];
-      fft::Dft<L, +1, R>::run(x);
+      fft::dft<L, +1, R, PK>(x);
 #pragma unroll
       for (int j = 0; j < L; ++j) row[j] = x[j];
     }
@@ -268,10 +276,10 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
       const int site0 = (c * S + xl) * L * L + z;
 #pragma unroll
       for (int y = 0; y < L; ++y) x[y] = sm[off(y / S, xl, y % S, z)];
-      fft::Dft<L, +1, R>::run(x);
+      fft::dft<L, +1, R, PK>(x);
 #pragma unroll
       for (int y = 0; y < L; ++y) {
-        cplx<R> v = apply_kin<R>(f, site0 + y * L, x[y]);
+        cplx<R> v = apply_kin<R, PK>(f, site0 + y * L, x[y]);
         if constexpr (sizeof(R) == 4)
           __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(v.re, v.im));
         else
@@ -536,7 +544,7 @@ __device__ __forceinline__ void bulk_to_peer(uint32_t dst, const void* src, uint
 
 // STAGED = false: no stage buffer; the next slab is prefetched into L2 and
 // pass 1 reads it from there (two buffers instead of three per CTA).
-template <typename R, int L, int C, bool STAGED>
+template <typename R, int L, int C, bool STAGED, bool PK = false>
 __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape<R, L, C, STAGED>::MIN_BLOCKS)
     fused_step_bulk_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
@@ -599,7 +607,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
       const int site0 = (c * S + xl) * L * L + z;
       if constexpr (STAGED) {
 #pragma unroll
-        for (int y = 0; y < L; ++y) x[y] = apply_kin<R>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
+        for (int y = 0; y < L; ++y) x[y] = apply_kin<R, PK>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
       } else {
         const cplx<R>* src = slab(orb);
 #pragma unroll
@@ -612,10 +620,10 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
             double2 t = __ldcg(reinterpret_cast<const double2*>(src) + (xl * L + y) * L + z);
             v = cplx<R>{t.x, t.y};
           }
-          x[y] = apply_kin<R>(f, site0 + y * L, v);
+          x[y] = apply_kin<R, PK>(f, site0 + y * L, v);
         }
       }
-      fft::Dft<L, -1, R>::run(x);
+      fft::dft<L, -1, R, PK>(x);
 #pragma unroll
       for (int y = 0; y < L; ++y) work[off(y / S, xl, y % S, z)] = x[y];
     }
@@ -632,7 +640,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
       cplx<R>* row = work + off(y / S, xl, y % S, 0);
 #pragma unroll
       for (int j = 0; j < L; ++j) x[j] = row[j];
-      fft::Dft<L, -1, R>::run(x);
+      fft::dft<L, -1, R, PK>(x);
 #pragma unroll
       for (int j = 0; j < L; ++j) row[j] = x[j];
     }
@@ -651,7 +659,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
       const int site0 = (c * S + yl) * L + z;
 #pragma unroll
       for (int xx = 0; xx < L; ++xx) x[xx] = recv[off(xx / S, xx % S, yl, z)];
-      fft::Dft<L, -1, R>::run(x);
+      fft::dft<L, -1, R, PK>(x);
       if (z2_fast) {
         const uint64_t k0 = kb + (uint64_t)site0;
         const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
@@ -659,13 +667,13 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
 #pragma unroll
         for (int xx = 0; xx < L; ++xx) {
           const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
-          x[xx] = scale2<R>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
         }
       } else {
 #pragma unroll
         for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
       }
-      fft::Dft<L, +1, R>::run(x);
+      fft::dft<L, +1, R, PK>(x);
 #pragma unroll
       for (int xx = 0; xx < L; ++xx) recv[off(xx / S, xx % S, yl, z)] = x[xx];
     }
@@ -685,7 +693,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
       cplx<R>* row = work + off(y / S, xl, y % S, 0);
 #pragma unroll
       for (int j = 0; j < L; ++j) x[j] = row[j];
-      fft::Dft<L, +1, R>::run(x);
+      fft::dft<L, +1, R, PK>(x);
 #pragma unroll
       for (int j = 0; j < L; ++j) row[j] = x[j];
     }
@@ -696,10 +704,10 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
       const int site0 = (c * S + xl) * L * L + z;
 #pragma unroll
       for (int y = 0; y < L; ++y) x[y] = work[off(y / S, xl, y % S, z)];
-      fft::Dft<L, +1, R>::run(x);
+      fft::dft<L, +1, R, PK>(x);
 #pragma unroll
       for (int y = 0; y < L; ++y) {
-        cplx<R> v = apply_kin<R>(f, site0 + y * L, x[y]);
+        cplx<R> v = apply_kin<R, PK>(f, site0 + y * L, x[y]);
         if constexpr (sizeof(R) == 4)
           __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(v.re, v.im));
         else
@@ -715,18 +723,23 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
 
 // KIND 0: one lane per pencil, exchange through peers' shared memory;
 // 1: two lanes per pencil; 2: bulk-copy exchange, staged slab; 3: bulk-copy
-// exchange, slab prefetched into L2.
+// exchange, slab prefetched into L2; 4, 5, 6: kinds 0, 2, 3 with the packed
+// FP32x2 transforms (FP32 only).
 template <typename R, int L, int C, int KIND = 0>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
+  static_assert(KIND < 4 || sizeof(R) == 4, "packed transforms are FP32");
   constexpr int THREADS = KIND == 1 ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
-  constexpr size_t SMEM = KIND == 2   ? BulkShape<R, L, C, true>::SMEM
-                          : KIND == 3 ? BulkShape<R, L, C, false>::SMEM
-                                      : Sh::SMEM;
+  constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
+                          : (KIND == 3 || KIND == 6) ? BulkShape<R, L, C, false>::SMEM
+                                                     : Sh::SMEM;
   void (*kern)(FusedArgs);
   if constexpr (KIND == 1) kern = fused_step_split_kernel<R, L, C>;
   else if constexpr (KIND == 2) kern = fused_step_bulk_kernel<R, L, C, true>;
   else if constexpr (KIND == 3) kern = fused_step_bulk_kernel<R, L, C, false>;
+  else if constexpr (KIND == 4) kern = fused_step_kernel<R, L, C, true>;
+  else if constexpr (KIND == 5) kern = fused_step_bulk_kernel<R, L, C, true, true>;
+  else if constexpr (KIND == 6) kern = fused_step_bulk_kernel<R, L, C, false, true>;
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");
@@ -771,7 +784,7 @@ struct FusedVariant {
   int prec;  // nrcps_precision
   int L;
   int C;
-  int kind;  // 0: exchange through peers' shared memory; 1: lane split; 2/3: bulk-copy exchange
+  int kind;  // 0: exchange through peers' shared memory; 1: lane split; 2/3: bulk-copy exchange; 4-6: packed
   FusedLauncher fn;
 };
 
@@ -783,20 +796,28 @@ struct FusedVariant {
 // Listed best-first per (precision, L) as measured on B200 (the first entry
 // is the default before autotuning).
 static const FusedVariant kVariants[] = {
+    {NRCPS_F32, 8, 1, 4, launch_fused<float, 8, 1, 4>},
     {NRCPS_F32, 8, 1, 0, launch_fused<float, 8, 1>},
+    {NRCPS_F32, 16, 1, 4, launch_fused<float, 16, 1, 4>},
     {NRCPS_F32, 16, 1, 0, launch_fused<float, 16, 1>},
     {NRCPS_F32, 16, 2, 2, launch_fused<float, 16, 2, 2>},
     {NRCPS_F32, 16, 2, 0, launch_fused<float, 16, 2>},
     {NRCPS_F32, 16, 1, 1, launch_fused<float, 16, 1, 1>},
+    {NRCPS_F32, 24, 3, 5, launch_fused<float, 24, 3, 5>},
+    {NRCPS_F32, 24, 4, 4, launch_fused<float, 24, 4, 4>},
     {NRCPS_F32, 24, 3, 2, launch_fused<float, 24, 3, 2>},
     {NRCPS_F32, 24, 4, 2, launch_fused<float, 24, 4, 2>},
     {NRCPS_F32, 24, 3, 0, launch_fused<float, 24, 3>},
     {NRCPS_F32, 24, 4, 0, launch_fused<float, 24, 4>},
+    {NRCPS_F32, 32, 8, 4, launch_fused<float, 32, 8, 4>},
+    {NRCPS_F32, 32, 8, 6, launch_fused<float, 32, 8, 6>},
+    {NRCPS_F32, 32, 8, 5, launch_fused<float, 32, 8, 5>},
     {NRCPS_F32, 32, 8, 3, launch_fused<float, 32, 8, 3>},
     {NRCPS_F32, 32, 16, 3, launch_fused<float, 32, 16, 3>},
     {NRCPS_F32, 32, 8, 0, launch_fused<float, 32, 8>},
     {NRCPS_F32, 32, 8, 2, launch_fused<float, 32, 8, 2>},
     {NRCPS_F32, 32, 8, 1, launch_fused<float, 32, 8, 1>},
+    {NRCPS_F32, 48, 16, 4, launch_fused<float, 48, 16, 4>},
     {NRCPS_F32, 48, 16, 0, launch_fused<float, 48, 16>},
     {NRCPS_F32, 48, 16, 3, launch_fused<float, 48, 16, 3>},
     {NRCPS_F32, 48, 16, 1, launch_fused<float, 48, 16, 1>},
@@ -882,29 +903,44 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
+  // Two rounds over the variants, each timed on 3 launches after one
+  // untimed launch; a variant's time is its faster round (single rounds
+  // varied by ~15 % between neighbouring variants on B200).
   float best = 1e30f;
   int best_i = -1;
   long saved = ctx->launches;
+  float round_ms[kNumVariants];
+  bool ok[kNumVariants];
   for (int i = 0; i < kNumVariants; ++i) {
-    if (kVariants[i].prec != prec || kVariants[i].L != L) continue;
-    if (kVariants[i].fn(ctx, f, 0) != NRCPS_OK) {
-      cudaGetLastError();
-      continue;
-    }
-    cudaEventRecord(t0, ctx->stream);
-    for (int r = 0; r < 3; ++r) kVariants[i].fn(ctx, f, 0);
-    cudaEventRecord(t1, ctx->stream);
-    if (cudaEventSynchronize(t1) != cudaSuccess) {
-      cudaGetLastError();
-      continue;
-    }
-    float ms = 0;
-    cudaEventElapsedTime(&ms, t0, t1);
-    if (ms < best) {
-      best = ms;
-      best_i = i;
+    round_ms[i] = 1e30f;
+    ok[i] = kVariants[i].prec == prec && kVariants[i].L == L;
+  }
+  for (int round = 0; round < 2; ++round) {
+    for (int i = 0; i < kNumVariants; ++i) {
+      if (!ok[i]) continue;
+      if (kVariants[i].fn(ctx, f, 0) != NRCPS_OK) {
+        cudaGetLastError();
+        ok[i] = false;
+        continue;
+      }
+      cudaEventRecord(t0, ctx->stream);
+      for (int r = 0; r < 3; ++r) kVariants[i].fn(ctx, f, 0);
+      cudaEventRecord(t1, ctx->stream);
+      if (cudaEventSynchronize(t1) != cudaSuccess) {
+        cudaGetLastError();
+        ok[i] = false;
+        continue;
+      }
+      float ms = 0;
+      cudaEventElapsedTime(&ms, t0, t1);
+      if (ms < round_ms[i]) round_ms[i] = ms;
     }
   }
+  for (int i = 0; i < kNumVariants; ++i)
+    if (ok[i] && round_ms[i] < best) {
+      best = round_ms[i];
+      best_i = i;
+    }
   ctx->launches = saved;
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);

@@ -367,6 +367,22 @@ extern "C" nrcps_status nrcps_overlap(nrcps_context* ctx, const double* dev_src,
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
   NRCPS_REQUIRE(ctx, dev_src && dev_psi && dev_S && ns >= 0 && nt >= 0 && nconf >= 0 && vol > 0,
                 "nrcps_overlap: bad arguments");
+  if (prec == NRCPS_F32 && ctx->overlap_tc && ns > 0 && nt > 0 && nconf > 0 && ((uintptr_t)dev_psi & 15) == 0 &&
+      overlap_tc_supported(vol, ns, nt, nconf)) {
+    const size_t need = overlap_tc_split_bytes(ns, vol);
+    if (need > ctx->tc_split_bytes) {
+      if (ctx->tc_split) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->tc_split);
+        ctx->tc_split = nullptr;
+        ctx->tc_split_bytes = 0;
+      }
+      NRCPS_TRY(check_cuda(ctx, cudaMalloc(&ctx->tc_split, need), "cudaMalloc(overlap split)"));
+      ctx->tc_split_bytes = need;
+    }
+    NRCPS_TRY(overlap_tc_prepare(ctx, dev_src, ns, vol, (float*)ctx->tc_split));
+    return overlap_tc(ctx, (const float*)ctx->tc_split, ns, dev_psi, nt, nconf, vol, dev_S);
+  }
   return overlap_impl(ctx, dev_src, ns, dev_psi, nt, nconf, vol, prec, dev_S);
 }
 

@@ -405,6 +405,46 @@ def test_exchange_variants_are_bit_identical(ctx, kind, precision, L, cluster):
         ctx.set_option("fused.kind", -1)
 
 
+_PACKED_VARIANTS = [(4, 8, 1), (4, 16, 1), (4, 24, 4), (5, 24, 3), (4, 32, 8), (5, 32, 8), (6, 32, 8), (4, 48, 16)]
+
+
+@pytest.mark.parametrize("kind,L,cluster", _PACKED_VARIANTS)
+def test_packed_variants_agree(ctx, kind, L, cluster):
+    """Kinds 4-6 compute the transforms two half-length DFTs per packed
+    FP32x2 instruction: a different (equally accurate) operation order, so
+    they agree with the scalar kernel to FP32 rounding, not bit for bit."""
+    psi, kinv, bits = _random_step_inputs(ctx, L, 3, 5, "f32", seed=5)
+    try:
+        ctx.set_option("fused.kind", 0)
+        ctx.set_option("fused.cluster", cluster)
+        ref = psi.clone()
+        nb.propagate(ref, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.set_option("fused.kind", kind)
+        q = psi.clone()
+        nb.propagate(q, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.synchronize()
+        assert max_norm_err(q.cpu().numpy(), ref.cpu().numpy()) < 2e-6
+    finally:
+        ctx.set_option("fused.cluster", 0)
+        ctx.set_option("fused.kind", -1)
+
+
+@pytest.mark.parametrize("kind", [5, 6])
+def test_packed_exchange_variants_are_bit_identical(ctx, kind):
+    psi, kinv, bits = _random_step_inputs(ctx, 32, 3, 5, "f32", seed=6)
+    try:
+        ctx.set_option("fused.kind", 4)
+        ref = psi.clone()
+        nb.propagate(ref, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.set_option("fused.kind", kind)
+        q = psi.clone()
+        nb.propagate(q, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.synchronize()
+        assert torch.equal(q, ref)
+    finally:
+        ctx.set_option("fused.kind", -1)
+
+
 def test_synchronize_reports_no_timeout(ctx):
     psi, kinv, bits = _random_step_inputs(ctx, 32, 2, 2, "f32")
     nb.propagate(psi, 2, kinv, bits, 0.5, ctx=ctx)

@@ -19,13 +19,15 @@
 // buffer, so the result carries FP64 accumulation across K.
 //
 // One CTA per (64 orbitals, K range); 6 warps:
-//   warp 0      TMA producer: the raw FP32 psi tile (64 x 32 floats) and the
-//               A hi / lo tiles (64 x 32 each), 128-byte swizzle;
+//   warp 0      TMA producer: the raw FP32 psi tile (64 x 32 floats, into the
+//               B_hi half of the operand tile) and the A hi / lo tiles
+//               (64 x 32 each), 128-byte swizzle, 6 stages;
 //   warp 1      TMEM owner (2 x 128 columns) and MMA issuer (one thread);
-//   warps 2-5   split the raw psi tile into its hi / lo halves in the
-//               operand tile (the swizzle is position-preserving, so the
-//               split is elementwise), drain every chunk (tcgen05.ld of the
-//               accumulator, quadrant sums in FP64) and write the results
+//   warps 2-5   split the raw psi tile in place into its hi / lo halves
+//               (the swizzle is position-preserving, so the split is
+//               elementwise);
+//   warps 6-9   drain every chunk (tcgen05.ld of the accumulator, quadrant
+//               sums in FP64 shared memory) and write the results
 //               (atomically added when K is split over CTAs).
 // Every mbarrier wait is bounded; a timeout sets the context's error flag
 // and all roles leave their loops, wait for their own copies and MMAs in
@@ -40,16 +42,17 @@ namespace tc {
 constexpr int BN = 64;                         // orbitals (n) per tile
 constexpr int BN2 = 2 * BN;                    // MMA N: [B_hi; B_lo] rows = accumulator columns per buffer
 constexpr int BK = 32;                         // floats of K per stage: one 128-byte swizzle row
-constexpr int STAGES = 4;
+constexpr int STAGES = 6;
 constexpr int CHUNK = 8;                       // k-blocks (256 floats of K) per FP32 accumulation in TMEM
 constexpr uint32_t RAW_BYTES = BN * BK * 4;    // 8 KB: raw psi tile
 constexpr uint32_t BP_BYTES = 2 * RAW_BYTES;   // 16 KB: [B_hi; B_lo], 128 rows
 constexpr uint32_t AH_BYTES = 64 * BK * 4;     // 8 KB: one A half (64 rows)
 constexpr uint32_t A_BYTES = 2 * AH_BYTES;     // 16 KB: [A_hi; A_lo], 128 rows
-constexpr uint32_t STAGE_BYTES = A_BYTES + BP_BYTES + RAW_BYTES;  // 40 KB, 1024-aligned pieces
+constexpr uint32_t STAGE_BYTES = A_BYTES + BP_BYTES;  // 32 KB, 1024-aligned pieces
 constexpr uint32_t TX_BYTES = RAW_BYTES + A_BYTES;
-constexpr uint32_t ACC_BYTES = 64 * BN * 8;    // 32 KB: FP64 running sums of the 64 result rows
-constexpr int THREADS = 192;
+constexpr int ACC_LD = BN + 1;                 // padded row: lane i's row starts 2 banks after lane i-1's
+constexpr uint32_t ACC_BYTES = ((64 * ACC_LD * 8 + 1023) / 1024) * 1024;  // FP64 running sums of the 64 result rows
+constexpr int THREADS = 320;
 constexpr uint32_t TMEM_COLS = 2 * BN2;        // two accumulator buffers
 constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + ACC_BYTES + 1024 /* alignment */ + 256 /* barriers */;
 constexpr int MAX_NS_BLOCK = 32;               // 2 ns <= 64 accumulator rows per half
@@ -135,6 +138,10 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "memory");
 }
 
+// TF32 rounding of a finite float's bit pattern, to nearest with ties away
+// from zero (as cvt.rna.tf32.f32): two integer operations.
+__device__ __forceinline__ uint32_t tf32_round_bits(uint32_t b) { return (b + 0x1000u) & 0xFFFFE000u; }
+
 __device__ __forceinline__ uint32_t tf32_rna(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -164,7 +171,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   // 1024-byte aligned stage area (the swizzle atoms repeat every 1024 bytes)
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  double* acc = reinterpret_cast<double*>(base + (size_t)STAGES * STAGE_BYTES);  // [64][BN] FP64 sums
+  double* acc = reinterpret_cast<double*>(base + (size_t)STAGES * STAGE_BYTES);  // [64][ACC_LD] FP64 sums
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + (size_t)STAGES * STAGE_BYTES + ACC_BYTES);
   uint64_t* full = bars;                  // TMA landed (raw psi + A)
   uint64_t* conv = bars + STAGES;         // operand tile split (4 converter warps)
@@ -177,7 +184,6 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   auto stage_a = [&](int s) { return base + (size_t)s * STAGE_BYTES; };
   auto stage_b = [&](int s) { return base + (size_t)s * STAGE_BYTES + A_BYTES; };
-  auto stage_raw = [&](int s) { return base + (size_t)s * STAGE_BYTES + A_BYTES + BP_BYTES; };
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tile = blockIdx.x, split = blockIdx.y;
@@ -203,7 +209,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  for (int i = threadIdx.x; i < 64 * BN; i += THREADS) acc[i] = 0.0;
+  for (int i = threadIdx.x; i < 64 * ACC_LD; i += THREADS) acc[i] = 0.0;
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
                  "r"(TMEM_COLS)
@@ -226,7 +232,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int kx = (kb0 + i) * BK;
         tma_load_2d(stage_a(s), &map_ahi, kx, 0, full + s);
         tma_load_2d(stage_a(s) + AH_BYTES, &map_alo, kx, 0, full + s);
-        tma_load_2d(stage_raw(s), &map_psi, kx, n0, full + s);
+        tma_load_2d(stage_b(s), &map_psi, kx, n0, full + s);  // raw psi lands in the B_hi half
         ++issued;
       }
       // copies still in flight land before the CTA may leave
@@ -261,19 +267,53 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (stop) break;
       }
     }
-  } else {
-    // ------------------------------------------------ converters + drains
+  } else if (warp < 6) {
+    // ------------------------------------------------------------ converters
+    // In place: the raw tile becomes B_hi = x rounded to TF32 (nearest, ties
+    // away: add half a TF32 ulp to the magnitude bits, clear the 13 low
+    // mantissa bits) and B_lo = x - B_hi (exact in FP32), itself rounded to
+    // TF32 the same way, so the tensor core reads exactly hi and lo and
+    // hi + lo carries x to ~2^-22.
     const int ct = threadIdx.x - 64;  // 0..127
-    const int q = warp & 3;           // TMEM lane quarter this warp may access
-    const int row = 32 * q + lane;    // accumulator row (M)
+    bool ok = true;
+    for (int i = 0; i < nk && ok; ++i) {
+      const int s = i % STAGES;
+      if (!bar_wait(full + s, (uint32_t)(i / STAGES) & 1u, abort_flag, g.err)) ok = false;
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      uint4* bp = reinterpret_cast<uint4*>(stage_b(s));
+#pragma unroll
+      for (int r = 0; r < (int)(RAW_BYTES / 16 / 128); ++r) {
+        const int e = ct + 128 * r;
+        const uint4 x = bp[e];
+        uint4 hi, lo;
+        hi.x = tf32_round_bits(x.x);
+        hi.y = tf32_round_bits(x.y);
+        hi.z = tf32_round_bits(x.z);
+        hi.w = tf32_round_bits(x.w);
+        lo.x = tf32_round_bits(__float_as_uint(__uint_as_float(x.x) - __uint_as_float(hi.x)));
+        lo.y = tf32_round_bits(__float_as_uint(__uint_as_float(x.y) - __uint_as_float(hi.y)));
+        lo.z = tf32_round_bits(__float_as_uint(__uint_as_float(x.z) - __uint_as_float(hi.z)));
+        lo.w = tf32_round_bits(__float_as_uint(__uint_as_float(x.w) - __uint_as_float(hi.w)));
+        bp[e] = hi;
+        bp[e + RAW_BYTES / 16] = lo;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
+      __syncwarp();
+      if (lane == 0) bar_arrive(conv + s);
+    }
+  } else {
+    // ------------------------------------------------------ drains + output
+    const int et = threadIdx.x - 192;  // 0..127
+    const int q = warp & 3;            // TMEM lane quarter this warp may access
+    const int row = 32 * q + lane;     // accumulator row (M)
     // tcgen05.ld is warp-collective: `live` is warp-uniform; rows >= 2 ns of
     // a live quarter load and discard
     const bool live = 32 * (q & 1) < 2 * g.ns;
     bool ok = true;
-    // Every warp runs the same sequence of drains and named barriers on
-    // every path; after a failed wait (ok false, warp-uniform) it only skips
-    // the work.
-    auto drain = [&](int j) {
+    // Every drain warp runs the same sequence of named barriers on every
+    // path; after a failed wait (ok false, warp-uniform) it only skips work.
+    for (int j = 0; j < nchunks; ++j) {
       const int b = j & 1;
       if (ok && !bar_wait(tfull + b, (uint32_t)(j >> 1) & 1u, abort_flag, g.err)) ok = false;
       ok = __all_sync(0xffffffffu, ok);
@@ -282,7 +322,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       for (int phase = 0; phase < 2; ++phase) {
         if (ok && live && (q >= 2) == (phase == 0)) {
           const uint32_t t0 = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * BN2);
-          double* arow = acc + (size_t)(row & 63) * BN;
+          double* arow = acc + (size_t)(row & 63) * ACC_LD;
 #pragma unroll 1
           for (int c0 = 0; c0 < BN; c0 += 32) {
             float u[32], v[32];
@@ -297,43 +337,10 @@ __global__ void __launch_bounds__(THREADS, 1)
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) bar_arrive(tempty + b);
-    };
-    for (int j = 0; j < nchunks; ++j) {
-      const int i1 = (j + 1) * CHUNK < nk ? (j + 1) * CHUNK : nk;
-      for (int i = j * CHUNK; i < i1; ++i) {
-        const int s = i % STAGES;
-        if (ok && !bar_wait(full + s, (uint32_t)(i / STAGES) & 1u, abort_flag, g.err)) ok = false;
-        ok = __all_sync(0xffffffffu, ok);
-        if (!ok) continue;
-        const float4* raw = reinterpret_cast<const float4*>(stage_raw(s));
-        uint4* bp = reinterpret_cast<uint4*>(stage_b(s));
-#pragma unroll
-        for (int r = 0; r < (int)(RAW_BYTES / 16 / 128); ++r) {
-          const int e = ct + 128 * r;
-          const float4 x = raw[e];
-          uint4 hi, lo;
-          hi.x = tf32_rna(x.x);
-          hi.y = tf32_rna(x.y);
-          hi.z = tf32_rna(x.z);
-          hi.w = tf32_rna(x.w);
-          lo.x = tf32_rna(x.x - __uint_as_float(hi.x));
-          lo.y = tf32_rna(x.y - __uint_as_float(hi.y));
-          lo.z = tf32_rna(x.z - __uint_as_float(hi.z));
-          lo.w = tf32_rna(x.w - __uint_as_float(hi.w));
-          bp[e] = hi;
-          bp[e + RAW_BYTES / 16] = lo;
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
-        __syncwarp();
-        if (lane == 0) bar_arrive(conv + s);
-      }
-      if (j >= 1) drain(j - 1);
     }
-    if (nchunks > 0) drain(nchunks - 1);
     // ------------------------------------------------------------ output
-    asm volatile("bar.sync 1, 128;" ::: "memory");
     if (ok) {
-      for (int e = ct; e < 2 * g.ns * BN; e += 128) {
+      for (int e = et; e < 2 * g.ns * BN; e += 128) {
         const int m = e / BN, col = e - m * BN;
         const int n = n0 + col;
         if (n >= g.n_rows) continue;
@@ -341,7 +348,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int s = g.s_base + (im ? m - g.ns : m);
         const int c = n / g.nt, t = n - c * g.nt;
         double* o = g.S + (((long)c * g.ns_total + s) * g.nt + t) * 2 + (im ? 1 : 0);
-        const double val = acc[(size_t)m * BN + col];
+        const double val = acc[(size_t)m * ACC_LD + col];
         if (g.atomic_out) atomicAdd(o, val);
         else *o = val;
       }
@@ -459,8 +466,28 @@ nrcps_status overlap_tc(nrcps_context* ctx, const float* split, int ns, const vo
   }
   const int tiles = (n_rows + tc::BN - 1) / tc::BN;
   const int kb_total = (int)(K / tc::BK);
-  // split K so that the grid covers the SMs about twice
-  int splits = (2 * ctx->sm_count + tiles - 1) / tiles;
+  // Split K over CTAs so that the grid fills its last wave (one CTA per SM):
+  // the smallest split count whose waves are at least 90 % full, else the
+  // fullest of 1..8; at least two waves when the tiles alone are fewer.
+  int splits = 1;
+  {
+    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    const int min_s = tiles < 2 * sms ? (2 * sms + tiles - 1) / tiles : 1;
+    double best = -1.0;
+    for (int sp = min_s; sp <= min_s + 7; ++sp) {
+      const long ctas = (long)tiles * sp;
+      const long waves = (ctas + sms - 1) / sms;
+      const double eff = (double)ctas / (double)(waves * sms);
+      if (eff >= 0.9) {
+        splits = sp;
+        break;
+      }
+      if (eff > best) {
+        best = eff;
+        splits = sp;
+      }
+    }
+  }
   if (splits > kb_total / 8) splits = kb_total / 8 > 0 ? kb_total / 8 : 1;
   if (splits < 1) splits = 1;
   const int per = (kb_total + splits - 1) / splits;

@@ -1,0 +1,126 @@
+"""Times the hot kernels of libnrcps_b200 in isolation (CUDA events on the
+context's stream, after warm-up), one JSON line per measurement.
+
+    python -m nrcps_b200.kernel_bench step    --L 32 --orbitals 19456 [--kind K --cluster C] [--precision f32]
+    python -m nrcps_b200.kernel_bench overlap --L 32 --ns 19 --nconf 1024 [--tc 1|0]
+    python -m nrcps_b200.kernel_bench dets    --N 19 --nconf 4096
+
+step:    one transfer-matrix step (nrcps_propagate, Z2 field, a = 0.5) over
+         `orbitals` orbitals in batches of 19; GB/s counts one read and one
+         write of every orbital.
+overlap: S = <src|psi> for FP32 orbitals with dense FP64 sources
+         (nrcps_overlap); GB/s counts one read of psi, TFLOP/s the useful
+         8 ns nt V complex multiply-adds per configuration.
+dets:    determinants of all N leading minors of nconf FP64 matrices.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+
+import numpy as np
+import torch
+
+from . import _capi as C
+from ._capi import lib
+from .api import Context, draw_z2_bits, kinetic_table, overlap, slater_dets
+
+
+def _time(fn, reps: int, warmup: int = 2) -> float:
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def bench_step(ctx: Context, L: int, orbitals: int, precision: str, kind: int, cluster: int, reps: int) -> dict:
+    dims = (L, L, L)
+    batch = 19
+    nconf = max(1, orbitals // batch)
+    psi = torch.randn((nconf * batch,) + dims, dtype=torch.complex64 if precision == "f32" else torch.complex128,
+                      device=ctx.device)
+    bits = draw_z2_bits("RANLXS2", 7, 0, nconf * L ** 3, ctx)
+    kinv = torch.from_numpy(1.0 / kinetic_table(dims, "PERFECT", 1.0, 0.5, 2.0)).to(ctx.device)
+    pf = C.PositionFactor()
+    pf.field_mode, pf.dev_field, pf.bit0, pf.conf_stride = 1, bits.data_ptr(), 0, L ** 3
+    pf.a, pf.dev_pos = 0.5, None
+    d3 = np.array(dims, dtype=np.int32)
+    ctx.set_option("fused.kind", kind)
+    ctx.set_option("fused.cluster", cluster)
+
+    def run():
+        ctx.check(lib().nrcps_propagate(ctx.handle, ctypes.c_void_p(psi.data_ptr()), batch, nconf,
+                                        d3.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                        ctypes.c_void_p(kinv.data_ptr()), ctypes.byref(pf),
+                                        C.F32 if precision == "f32" else C.F64), "propagate")
+
+    try:
+        ms = _time(run, reps)
+        ctx.synchronize()
+    finally:
+        ctx.set_option("fused.kind", -1)
+        ctx.set_option("fused.cluster", 0)
+    esize = 8 if precision == "f32" else 16
+    return {"kernel": "step", "L": L, "orbitals": nconf * batch, "precision": precision, "kind": kind,
+            "cluster": cluster, "ms": round(ms, 4), "GBps": round(2.0 * L ** 3 * esize * nconf * batch / ms / 1e6, 1)}
+
+
+def bench_overlap(ctx: Context, L: int, ns: int, nconf: int, tc: int, reps: int) -> dict:
+    V = L ** 3
+    g = torch.Generator(device=ctx.device).manual_seed(1)
+    src = torch.randn((ns, V), dtype=torch.complex128, device=ctx.device, generator=g) / V ** 0.5
+    psi = torch.randn((nconf, ns, V), dtype=torch.complex64, device=ctx.device, generator=g)
+    ctx.set_option("overlap.tc", tc)
+    try:
+        ms = _time(lambda: overlap(src, psi, ctx), reps)
+        ctx.synchronize()
+    finally:
+        ctx.set_option("overlap.tc", 1)
+    return {"kernel": "overlap", "L": L, "ns": ns, "nconf": nconf, "tc": tc, "ms": round(ms, 4),
+            "GBps": round(psi.numel() * 8 / ms / 1e6, 1),
+            "useful_TFLOPs": round(8.0 * ns * ns * V * nconf / ms / 1e9, 2)}
+
+
+def bench_dets(ctx: Context, N: int, nconf: int, reps: int) -> dict:
+    g = torch.Generator(device=ctx.device).manual_seed(2)
+    S = torch.randn((nconf, N, N), dtype=torch.complex128, device=ctx.device, generator=g)
+    ms = _time(lambda: slater_dets(S, ctx=ctx), reps)
+    ctx.synchronize()
+    return {"kernel": "dets", "N": N, "nconf": nconf, "ms": round(ms, 4),
+            "matrices_per_s": round(nconf / ms * 1e3, 1)}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["step", "overlap", "dets"])
+    ap.add_argument("--L", type=int, default=32)
+    ap.add_argument("--orbitals", type=int, default=19456)
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--kind", type=int, default=-1)
+    ap.add_argument("--cluster", type=int, default=0)
+    ap.add_argument("--ns", type=int, default=19)
+    ap.add_argument("--nconf", type=int, default=1024)
+    ap.add_argument("--tc", type=int, default=1)
+    ap.add_argument("--N", type=int, default=19)
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args(argv)
+    ctx = Context(0)
+    if a.what == "step":
+        r = bench_step(ctx, a.L, a.orbitals, a.precision, a.kind, a.cluster, a.reps)
+    elif a.what == "overlap":
+        r = bench_overlap(ctx, a.L, a.ns, a.nconf, a.tc, a.reps)
+    else:
+        r = bench_dets(ctx, a.N, a.nconf, a.reps)
+    print(json.dumps(r), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -10,19 +10,19 @@
 //   m < ns:       A[m][2p] = Re src_m, A[m][2p+1] = Im src_m     -> Re S,
 //   ns <= m < 2ns: A[m][2p] = -Im src_s, A[m][2p+1] = Re src_s   -> Im S.
 // Precision: every operand is split into TF32 hi + lo (x = hi + lo to ~2^-22)
-// and the four products are formed by ONE M=128, N=128, K=8 MMA per k-step:
+// and the four products are formed by ONE M=128, N=256, K=8 MMA per k-step:
 // the A tile stacks [A_hi; A_lo] (rows 0-63, 64-127) and the B tile stacks
-// [B_hi; B_lo] (rows 0-63, 64-127), so the FP32 accumulator holds A_x B_y^T
+// [B_hi; B_lo] (rows 0-127, 128-255), so the FP32 accumulator holds A_x B_y^T
 // in its four quadrants.  The tensor core accumulates in FP32 for 256 floats
 // of K only (a chunk); each chunk's accumulator is drained into FP64 sums
 // in shared memory while the next chunk accumulates in the second TMEM
 // buffer, so the result carries FP64 accumulation across K.
 //
-// One CTA per (64 orbitals, K range); 6 warps:
-//   warp 0      TMA producer: the raw FP32 psi tile (64 x 32 floats, into the
+// One CTA per (128 orbitals, K range); 10 warps:
+//   warp 0      TMA producer: the raw FP32 psi tile (128 x 32 floats, into the
 //               B_hi half of the operand tile) and the A hi / lo tiles
-//               (64 x 32 each), 128-byte swizzle, 6 stages;
-//   warp 1      TMEM owner (2 x 128 columns) and MMA issuer (one thread);
+//               (64 x 32 each), 128-byte swizzle, 3 stages;
+//   warp 1      TMEM owner (2 x 256 columns) and MMA issuer (one thread);
 //   warps 2-5   split the raw psi tile in place into its hi / lo halves
 //               (the swizzle is position-preserving, so the split is
 //               elementwise);
@@ -39,16 +39,16 @@
 namespace nrcps {
 namespace tc {
 
-constexpr int BN = 64;                         // orbitals (n) per tile
+constexpr int BN = 128;                        // orbitals (n) per tile
 constexpr int BN2 = 2 * BN;                    // MMA N: [B_hi; B_lo] rows = accumulator columns per buffer
 constexpr int BK = 32;                         // floats of K per stage: one 128-byte swizzle row
-constexpr int STAGES = 6;
+constexpr int STAGES = 3;
 constexpr int CHUNK = 8;                       // k-blocks (256 floats of K) per FP32 accumulation in TMEM
-constexpr uint32_t RAW_BYTES = BN * BK * 4;    // 8 KB: raw psi tile
-constexpr uint32_t BP_BYTES = 2 * RAW_BYTES;   // 16 KB: [B_hi; B_lo], 128 rows
+constexpr uint32_t RAW_BYTES = BN * BK * 4;    // 16 KB: raw psi tile
+constexpr uint32_t BP_BYTES = 2 * RAW_BYTES;   // 32 KB: [B_hi; B_lo], 256 rows
 constexpr uint32_t AH_BYTES = 64 * BK * 4;     // 8 KB: one A half (64 rows)
 constexpr uint32_t A_BYTES = 2 * AH_BYTES;     // 16 KB: [A_hi; A_lo], 128 rows
-constexpr uint32_t STAGE_BYTES = A_BYTES + BP_BYTES;  // 32 KB, 1024-aligned pieces
+constexpr uint32_t STAGE_BYTES = A_BYTES + BP_BYTES;  // 48 KB, 1024-aligned pieces
 constexpr uint32_t TX_BYTES = RAW_BYTES + A_BYTES;
 constexpr int ACC_LD = BN + 1;                 // padded row: lane i's row starts 2 banks after lane i-1's
 constexpr uint32_t ACC_BYTES = ((64 * ACC_LD * 8 + 1023) / 1024) * 1024;  // FP64 running sums of the 64 result rows
@@ -57,7 +57,7 @@ constexpr uint32_t TMEM_COLS = 2 * BN2;        // two accumulator buffers
 constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + ACC_BYTES + 1024 /* alignment */ + 256 /* barriers */;
 constexpr int MAX_NS_BLOCK = 32;               // 2 ns <= 64 accumulator rows per half
 
-// instruction descriptor: D F32, A/B TF32, both K-major, N = 128, M = 128
+// instruction descriptor: D F32, A/B TF32, both K-major, N = 256, M = 128
 constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (((uint32_t)BN2 >> 3) << 17) | ((128u >> 4) << 24);
 
 struct Args {

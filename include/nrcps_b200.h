@@ -99,7 +99,10 @@ const char *nrcps_version(void);
  *   "overlap.tc"       1 (default): dense-source overlaps of FP32 orbitals
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the
- *                      CUDA-core kernel with FP64 accumulation. */
+ *                      CUDA-core kernel with FP64 accumulation;
+ *   "lu.warp"          1 (default): leading-minor determinants with one warp
+ *                      per minor in shared memory (N <= 64); 0: one thread
+ *                      per minor with global scratch. */
 nrcps_status nrcps_set_option(nrcps_context *ctx, const char *name, long value);
 /* Times every fused-kernel variant (cluster size, lane split) for (prec, L)
  * on this device and keeps the fastest for later calls; *cluster receives

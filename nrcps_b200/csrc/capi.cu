@@ -113,6 +113,8 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
   } else if (n == "fused.kind") {
     if (value < -1 || value > 6) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
     ctx->fused_kind = (int)value;
+  } else if (n == "lu.warp") {
+    ctx->lu_warp = value != 0;
   } else if (n == "overlap.tc") {
     ctx->overlap_tc = value != 0;
   } else {

@@ -17,7 +17,7 @@
 namespace nrcps {
 nrcps_status ranlux_generate(nrcps_context* ctx, int kind, long seed, uint64_t u_lo, uint64_t u_hi, int out_kind,
                              double* d, uint32_t* bits);
-nrcps_status slater_dets_impl(nrcps_context* ctx, const double* S, const double* psi1, int N, int nconf, int mode,
+nrcps_status slater_dets_dispatch(nrcps_context* ctx, const double* S, const double* psi1, int N, int nconf, int mode,
                               int log_det, double* out, long out_conf_stride, long out_offset, double* scr);
 size_t slater_dets_scratch_bytes(int N, int nconf, int mode);
 nrcps_status overlap_impl(nrcps_context* ctx, const double* src, int ns, const void* psi, int nt, int nconf,
@@ -153,7 +153,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       if (e->pw_index) NRCPS_TRY(gather_impl(ctx, e->pw_index, N, e->psi, N, nc, vol, prec, e->S));
       else if (e->src_split) NRCPS_TRY(overlap_tc(ctx, e->src_split, N, e->psi, N, nc, vol, e->S));
       else NRCPS_TRY(overlap_impl(ctx, e->src, N, e->psi, N, nc, vol, prec, e->S));
-      NRCPS_TRY(slater_dets_impl(ctx, e->S, nullptr, N, nc, 0, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
+      NRCPS_TRY(slater_dets_dispatch(ctx, e->S, nullptr, N, nc, 0, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
                                  e->lu_scr));
       if (e->qr_logR && t >= j.qr_period)
         NRCPS_TRY(rescale_dets(ctx, dets, e->qr_logR, N, nc, 2L * T * e->nmeas, 2L * t * e->nmeas));
@@ -162,7 +162,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       if (e->pw_index) NRCPS_TRY(gather_impl(ctx, e->pw_index, N, e->psi, N, nc, vol, prec, e->P1));
       else if (e->src_split) NRCPS_TRY(overlap_tc(ctx, e->src_split, N, e->psi, N, nc, vol, e->P1));
       else NRCPS_TRY(overlap_impl(ctx, e->src, N, e->psi, N, nc, vol, prec, e->P1));
-      NRCPS_TRY(slater_dets_impl(ctx, e->S, e->P1, N, nc, 1, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
+      NRCPS_TRY(slater_dets_dispatch(ctx, e->S, e->P1, N, nc, 1, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
                                  e->lu_scr));
     }
     // -------- Hamiltonians on the field of slice t, then the step

@@ -304,6 +304,150 @@ __global__ void slater_dets_kernel(const double* __restrict__ S, const double* _
   }
 }
 
+// One warp per (matrix, measured minor), the minor in shared memory.  The
+// same Crout factorisation with implicit-scaled partial pivoting as
+// ludcmp_dev, organised right-looking: element (i, k) receives the products
+// l_ij u_jk in the same order j = 0, 1, ... as Crout's running sum, the
+// pivot search sees the same updated column, ties go to the last row as
+// in `if (dum >= big)`, and rows swap whole -- so the factors and the
+// determinant follow the same arithmetic.  Lanes split rows (pivot search,
+// multipliers) and columns (swaps, trailing update); no global scratch.
+constexpr int kWarpLuMaxWarps = 4;  // warps per block (fewer for large N: shared memory)
+
+__global__ void __launch_bounds__(32 * kWarpLuMaxWarps) slater_dets_warp_kernel(const double* __restrict__ S,
+                                                                            const double* __restrict__ psi1, int N,
+                                                                            int nconf, int mode, int log_det,
+                                                                            double* __restrict__ out,
+                                                                            long out_conf_stride, long out_offset) {
+  extern __shared__ __align__(16) unsigned char lu_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  dc* a = reinterpret_cast<dc*>(lu_smem) + (size_t)warp * N * N;
+  double* vv = reinterpret_cast<double*>(reinterpret_cast<dc*>(lu_smem) + (size_t)wpb * N * N) + warp * N;
+  const int nmeas = mode ? 2 * N : N;
+  const long total = (long)nconf * nmeas;
+  for (long e = (long)blockIdx.x * wpb + warp; e < total; e += (long)gridDim.x * wpb) {
+    const long c = e / nmeas;
+    const int m = (int)(e % nmeas);
+    const int n = mode ? m / 2 + 1 : m + 1;
+    const int t0 = (mode && (m % 2 == 0)) ? n - 1 : -1;
+    const dc* Sc = reinterpret_cast<const dc*>(S) + c * (long)N * N;
+    const dc* P = mode ? reinterpret_cast<const dc*>(psi1) + c * (long)N * N : nullptr;
+    for (int idx = lane; idx < n * n; idx += 32) {
+      const int i = idx / n, k = idx - i * n;
+      // SlaterDet2::Run column t0 from psi1[s + t0*N] (slater_det2.C:102-106)
+      a[idx] = (k == t0) ? P[i + (long)t0 * N] : Sc[(long)N * i + k];
+    }
+    __syncwarp();
+    bool zero_row = false;
+    for (int i = lane; i < n; i += 32) {
+      double big = 0.0;
+      for (int k = 0; k < n; ++k) big = fmax(big, dabs(a[n * i + k]));
+      if (big == 0.0) zero_row = true;
+      vv[i] = 1.0 / big;
+    }
+    const bool singular = __any_sync(0xffffffffu, zero_row);
+    __syncwarp();
+    double d = 1.0;
+    for (int j = 0; j < n && !singular; ++j) {
+      double best = -1.0;
+      int bi = -1;
+      for (int i = j + lane; i < n; i += 32) {
+        const double dum = vv[i] * dabs(a[n * i + j]);
+        if (dum >= best) {
+          best = dum;
+          bi = i;
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ob > best || (ob == best && oi > bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      const int imax = bi;
+      if (imax != j) {
+        for (int k = lane; k < n; k += 32) {
+          const dc t = a[n * imax + k];
+          a[n * imax + k] = a[n * j + k];
+          a[n * j + k] = t;
+        }
+        d = -d;
+        if (lane == 0) vv[imax] = vv[j];
+      }
+      __syncwarp();
+      if (lane == 0 && dabs(a[n * j + j]) == 0.0) a[n * j + j] = dc{1.0e-20, 0.0};
+      __syncwarp();
+      const dc r = drecip(a[n * j + j]);
+      for (int i = j + 1 + lane; i < n; i += 32) a[n * i + j] = dmul(a[n * i + j], r);
+      __syncwarp();
+      for (int k = j + 1 + lane; k < n; k += 32) {
+        const dc u = a[n * j + k];
+        for (int i = j + 1; i < n; ++i) {
+          const dc p = dmul(a[n * i + j], u);
+          a[n * i + k].re -= p.re;
+          a[n * i + k].im -= p.im;
+        }
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      dc r;
+      if (singular) {
+        r = dc{nan(""), nan("")};  // an all-zero row: flagged to the host
+      } else if (!log_det) {
+        r = dc{d, 0.0};
+        for (int i = 0; i < n; ++i) r = dmul(r, a[n * i + i]);
+      } else {
+        r = dc{log(fabs(d)), d < 0 ? 3.14159265358979323846 : 0.0};
+        for (int i = 0; i < n; ++i) {
+          r.re += log(dabs(a[n * i + i]));
+          r.im += atan2(a[n * i + i].im, a[n * i + i].re);
+        }
+      }
+      double* o = out + c * out_conf_stride + out_offset + 2L * m;
+      o[0] = r.re;
+      o[1] = r.im;
+    }
+    __syncwarp();
+  }
+}
+
+constexpr int kWarpLuMaxN = 64;
+constexpr size_t kWarpLuSmemCap = 200 * 1024;
+
+static size_t warp_lu_bytes(int N) { return (size_t)N * N * sizeof(dc) + N * sizeof(double); }
+static int warp_lu_warps(int N) {
+  int w = (int)(kWarpLuSmemCap / warp_lu_bytes(N));
+  return w < 1 ? 1 : (w > kWarpLuMaxWarps ? kWarpLuMaxWarps : w);
+}
+
+// Leading-minor determinants through the warp kernel (N <= 64, no scratch).
+nrcps_status slater_dets_warp(nrcps_context* ctx, const double* S, const double* psi1, int N, int nconf, int mode,
+                              int log_det, double* out, long out_conf_stride, long out_offset) {
+  const int nmeas = mode ? 2 * N : N;
+  const long total = (long)nconf * nmeas;
+  if (total == 0) return NRCPS_OK;
+  static bool attr_set[16] = {false};
+  if (!attr_set[ctx->device & 15]) {
+    NRCPS_TRY(check_cuda(ctx,
+                         cudaFuncSetAttribute(slater_dets_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kWarpLuSmemCap),
+                         "slater_dets_warp: smem attribute"));
+    attr_set[ctx->device & 15] = true;
+  }
+  const int wpb = warp_lu_warps(N);
+  const long blocks = (total + wpb - 1) / wpb;
+  const unsigned g = (unsigned)(blocks < (long)ctx->sm_count * 64 ? blocks : (long)ctx->sm_count * 64);
+  slater_dets_warp_kernel<<<g, 32 * wpb, (size_t)wpb * warp_lu_bytes(N), ctx->stream>>>(S, psi1, N, nconf, mode, log_det,
+                                                                                   out, out_conf_stride, out_offset);
+  ctx->launches++;
+  return check_launch(ctx, "slater_dets_warp_kernel");
+}
+
 size_t slater_dets_scratch_bytes(int N, int nconf, int mode) {
   const int nmeas = mode ? 2 * N : N;
   return sizeof(double) * (size_t)nconf * nmeas * (2L * N * N + N);
@@ -325,6 +469,15 @@ nrcps_status slater_dets_impl(nrcps_context* ctx, const double* S, const double*
                                                                              scr, out_conf_stride, out_offset);
   ctx->launches++;
   return check_launch(ctx, "slater_dets_kernel");
+}
+
+// The determinant path of the library: the warp kernel for N <= 64 (unless
+// the "lu.warp" option is 0), else the per-thread kernel with scratch.
+nrcps_status slater_dets_dispatch(nrcps_context* ctx, const double* S, const double* psi1, int N, int nconf, int mode,
+                                  int log_det, double* out, long out_conf_stride, long out_offset, double* scr) {
+  if (N <= kWarpLuMaxN && ctx->lu_warp)
+    return slater_dets_warp(ctx, S, psi1, N, nconf, mode, log_det, out, out_conf_stride, out_offset);
+  return slater_dets_impl(ctx, S, psi1, N, nconf, mode, log_det, out, out_conf_stride, out_offset, scr);
 }
 
 nrcps_status overlap_impl(nrcps_context* ctx, const double* src, int ns, const void* psi, int nt, int nconf,
@@ -432,5 +585,5 @@ extern "C" nrcps_status nrcps_slater_dets(nrcps_context* ctx, const double* dev_
   NRCPS_REQUIRE(ctx, dev_S && dev_out && N > 0 && nconf >= 0 && (mode == 0 || (mode == 1 && dev_psi1)),
                 "nrcps_slater_dets: bad arguments");
   const int nmeas = mode ? 2 * N : N;
-  return slater_dets_impl(ctx, dev_S, dev_psi1, N, nconf, mode, log_det, dev_out, 2L * nmeas, 0, nullptr);
+  return slater_dets_dispatch(ctx, dev_S, dev_psi1, N, nconf, mode, log_det, dev_out, 2L * nmeas, 0, nullptr);
 }

@@ -95,7 +95,9 @@ const char *nrcps_version(void);
  *                      by bulk copy; 3: as 2, with the slab prefetched into
  *                      L2 instead of staged in shared memory; 4, 5, 6: kinds
  *                      0, 2, 3 with packed FP32x2 transforms (two
- *                      half-length DFTs per instruction; FP32 only);
+ *                      half-length DFTs per instruction; FP32 only); 7, 8:
+ *                      kinds 0, 4 with the slab prefetched into L2 instead
+ *                      of staged in shared memory (four CTAs per SM);
  *   "overlap.tc"       1 (default): dense-source overlaps of FP32 orbitals
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the

@@ -157,8 +157,26 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
-template <typename R, int L, int C, bool PK = false>
-__global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L, C>::MIN_BLOCKS)
+// Prefetch of a global range into L2 by the bulk copy engine (no completion).
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Launch shape of the peer-access kernel: STAGED keeps the HBM landing zone
+// of the next slab in shared memory (bulk copy); unstaged, the next slab is
+// prefetched into L2 and pass 1 reads it from there, which halves the shared
+// memory and lets four CTAs share an SM (registers capped accordingly).
+template <typename R, int L, int C, bool STAGED>
+struct PullShape {
+  using Base = FusedShape<R, L, C>;
+  static constexpr int THREADS = Base::THREADS;
+  static constexpr size_t SMEM = STAGED ? Base::SMEM : sizeof(cplx<R>) * (size_t)Base::WORK + 16;
+  static constexpr int FIT = (int)(228 * 1024 / (SMEM + 1024));
+  static constexpr int MIN_BLOCKS = STAGED ? Base::MIN_BLOCKS : (FIT > 4 ? 4 : (FIT < 1 ? 1 : FIT));
+};
+
+template <typename R, int L, int C, bool PK = false, bool STAGED = true>
+__global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape<R, L, C, STAGED>::MIN_BLOCKS)
     fused_step_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
   constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION;
@@ -166,7 +184,7 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
   constexpr uint32_t STAGE_BYTES = (uint32_t)(Sh::STAGE * sizeof(cplx<R>));
   extern __shared__ __align__(128) unsigned char smem_raw[];
   cplx<R>* stage = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* sm = stage + Sh::STAGE;
+  cplx<R>* sm = stage + (STAGED ? Sh::STAGE : 0);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Sh::WORK);
 
   cg::cluster_group cluster = cg::this_cluster();
@@ -186,32 +204,55 @@ __global__ void __launch_bounds__(FusedShape<R, L, C>::THREADS, FusedShape<R, L,
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
 
-  if (tid == 0) mbar_init(bar);
+  if (STAGED && tid == 0) mbar_init(bar);
   __syncthreads();
   uint32_t parity = 0;
   long orb = cluster_id;
-  if (tid == 0 && orb < f.n_orb_total) bulk_load(stage, slab(orb), STAGE_BYTES, bar);
+  if (tid == 0 && orb < f.n_orb_total) {
+    if constexpr (STAGED) bulk_load(stage, slab(orb), STAGE_BYTES, bar);
+    else prefetch_l2(slab(orb), STAGE_BYTES);
+  }
 
   for (; orb < f.n_orb_total; orb += n_clusters) {
     const long conf = orb / f.batch;
     const uint64_t kb = f.off0 + (uint64_t)conf * f.conf_stride;  // field offset of this configuration
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> x[L];
-    mbar_wait_bounded(bar, parity, f.err);
-    parity ^= 1u;
-    // ---- 1. k(p), forward DFT along y from the staged slab: thread -> (xl, z)
+    if constexpr (STAGED) {
+      mbar_wait_bounded(bar, parity, f.err);
+      parity ^= 1u;
+    } else if (tid == 0 && orb + n_clusters < f.n_orb_total) {
+      prefetch_l2(slab(orb + n_clusters), STAGE_BYTES);
+    }
+    // ---- 1. k(p), forward DFT along y from the slab: thread -> (xl, z)
     {
       const int z = tid % L, xl = tid / L;
       const int site0 = (c * S + xl) * L * L + z;
+      if constexpr (STAGED) {
 #pragma unroll
-      for (int y = 0; y < L; ++y) x[y] = apply_kin<R, PK>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
+        for (int y = 0; y < L; ++y) x[y] = apply_kin<R, PK>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
+      } else {
+        const cplx<R>* src = slab(orb);
+#pragma unroll
+        for (int y = 0; y < L; ++y) {
+          cplx<R> v;
+          if constexpr (sizeof(R) == 4) {
+            float2 t = __ldcg(reinterpret_cast<const float2*>(src) + (xl * L + y) * L + z);
+            v = cplx<R>{t.x, t.y};
+          } else {
+            double2 t = __ldcg(reinterpret_cast<const double2*>(src) + (xl * L + y) * L + z);
+            v = cplx<R>{t.x, t.y};
+          }
+          x[y] = apply_kin<R, PK>(f, site0 + y * L, v);
+        }
+      }
       fft::dft<L, -1, R, PK>(x);
 #pragma unroll
       for (int y = 0; y < L; ++y) sm[off(y / S, xl, y % S, z)] = x[y];
     }
     __syncthreads();
     // the staging buffer is free: prefetch this cluster's next orbital
-    if (tid == 0 && orb + n_clusters < f.n_orb_total) {
+    if (STAGED && tid == 0 && orb + n_clusters < f.n_orb_total) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       bulk_load(stage, slab(orb + n_clusters), STAGE_BYTES, bar);
     }
@@ -492,10 +533,6 @@ __device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_
   return false;
 }
 
-// Prefetch of a global range into L2 by the bulk copy engine (no completion).
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
 
 // ------------------------------------------------ bulk-copy exchange variant
 // Same passes, but both exchanges move whole padded regions with the bulk
@@ -724,14 +761,16 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
 // KIND 0: one lane per pencil, exchange through peers' shared memory;
 // 1: two lanes per pencil; 2: bulk-copy exchange, staged slab; 3: bulk-copy
 // exchange, slab prefetched into L2; 4, 5, 6: kinds 0, 2, 3 with the packed
-// FP32x2 transforms (FP32 only).
+// FP32x2 transforms (FP32 only); 7, 8: kinds 0, 4 with the slab prefetched
+// into L2 instead of staged (four CTAs per SM).
 template <typename R, int L, int C, int KIND = 0>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
-  static_assert(KIND < 4 || sizeof(R) == 4, "packed transforms are FP32");
+  static_assert(KIND < 4 || KIND == 7 || sizeof(R) == 4, "packed transforms are FP32");
   constexpr int THREADS = KIND == 1 ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
   constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
                           : (KIND == 3 || KIND == 6) ? BulkShape<R, L, C, false>::SMEM
+                          : (KIND == 7 || KIND == 8) ? PullShape<R, L, C, false>::SMEM
                                                      : Sh::SMEM;
   void (*kern)(FusedArgs);
   if constexpr (KIND == 1) kern = fused_step_split_kernel<R, L, C>;
@@ -740,6 +779,8 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   else if constexpr (KIND == 4) kern = fused_step_kernel<R, L, C, true>;
   else if constexpr (KIND == 5) kern = fused_step_bulk_kernel<R, L, C, true, true>;
   else if constexpr (KIND == 6) kern = fused_step_bulk_kernel<R, L, C, false, true>;
+  else if constexpr (KIND == 7) kern = fused_step_kernel<R, L, C, false, false>;
+  else if constexpr (KIND == 8) kern = fused_step_kernel<R, L, C, true, false>;
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");
@@ -784,7 +825,8 @@ struct FusedVariant {
   int prec;  // nrcps_precision
   int L;
   int C;
-  int kind;  // 0: exchange through peers' shared memory; 1: lane split; 2/3: bulk-copy exchange; 4-6: packed
+  int kind;  // 0: exchange through peers' shared memory; 1: lane split; 2/3: bulk-copy exchange; 4-6: packed;
+             // 7/8: peer access with the slab prefetched into L2
   FusedLauncher fn;
 };
 
@@ -810,6 +852,8 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 24, 3, 0, launch_fused<float, 24, 3>},
     {NRCPS_F32, 24, 4, 0, launch_fused<float, 24, 4>},
     {NRCPS_F32, 32, 8, 4, launch_fused<float, 32, 8, 4>},
+    {NRCPS_F32, 32, 8, 7, launch_fused<float, 32, 8, 7>},
+    {NRCPS_F32, 32, 8, 8, launch_fused<float, 32, 8, 8>},
     {NRCPS_F32, 32, 8, 6, launch_fused<float, 32, 8, 6>},
     {NRCPS_F32, 32, 8, 5, launch_fused<float, 32, 8, 5>},
     {NRCPS_F32, 32, 8, 3, launch_fused<float, 32, 8, 3>},
@@ -828,6 +872,7 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F64, 24, 4, 2, launch_fused<double, 24, 4, 2>},
     {NRCPS_F64, 24, 4, 0, launch_fused<double, 24, 4>},
     {NRCPS_F64, 32, 16, 3, launch_fused<double, 32, 16, 3>},
+    {NRCPS_F64, 32, 16, 7, launch_fused<double, 32, 16, 7>},
     {NRCPS_F64, 32, 16, 0, launch_fused<double, 32, 16>},
     {NRCPS_F64, 32, 8, 0, launch_fused<double, 32, 8>},
     {NRCPS_F64, 32, 16, 2, launch_fused<double, 32, 16, 2>},

@@ -429,11 +429,15 @@ def test_packed_variants_agree(ctx, kind, L, cluster):
         ctx.set_option("fused.kind", -1)
 
 
-@pytest.mark.parametrize("kind", [5, 6])
-def test_packed_exchange_variants_are_bit_identical(ctx, kind):
-    psi, kinv, bits = _random_step_inputs(ctx, 32, 3, 5, "f32", seed=6)
+@pytest.mark.parametrize("kind,ref_kind,precision,cluster", [(5, 4, "f32", 8), (6, 4, "f32", 8), (8, 4, "f32", 8),
+                                                             (7, 0, "f32", 8), (7, 0, "f64", 16)])
+def test_same_arithmetic_variants_are_bit_identical(ctx, kind, ref_kind, precision, cluster):
+    """Variants that differ only in how the slab reaches shared memory or how
+    the exchange moves it run the same arithmetic: results agree bit for bit."""
+    psi, kinv, bits = _random_step_inputs(ctx, 32, 3, 5, precision, seed=6)
     try:
-        ctx.set_option("fused.kind", 4)
+        ctx.set_option("fused.cluster", cluster)
+        ctx.set_option("fused.kind", ref_kind)
         ref = psi.clone()
         nb.propagate(ref, 5, kinv, bits, 0.5, ctx=ctx)
         ctx.set_option("fused.kind", kind)
@@ -442,6 +446,7 @@ def test_packed_exchange_variants_are_bit_identical(ctx, kind):
         ctx.synchronize()
         assert torch.equal(q, ref)
     finally:
+        ctx.set_option("fused.cluster", 0)
         ctx.set_option("fused.kind", -1)
 
 

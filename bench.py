@@ -53,14 +53,22 @@ def parse():
     ap.add_argument("--split", type=int, default=-1, help="fused kernel lane split: -1 autotuned, 0, 1")
     ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 peer access, 1 split, 2 bulk staged, 3 bulk L2, 4-6 packed 0/2/3")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU path measurement")
+    ap.add_argument("--qr", type=int, default=-1, help="re-orthonormalise every k slices (-1: 8 for f32, 0 for f64)")
+    ap.add_argument("--precision-configs", type=int, default=64,
+                    help="configurations of the FP32-vs-FP64 precision report (0: skip)")
     return ap.parse_args()
+
+
+def qr_period(a):
+    return a.qr if a.qr >= 0 else (8 if a.precision == "f32" else 0)
 
 
 def workload(a, n_orb):
     return {"workload": f"batched ensemble L={a.L}^3 T={a.T} N={n_orb} Z2 a=0.5 RANLXS2 seed {a.seed}, "
-                        f"{a.configs} configs/step, {a.precision} propagation + FP64 LU",
+                        f"{a.configs} configs/step, {a.precision} propagation + FP64 LU, QR every {qr_period(a)}",
             "L": a.L, "T": a.T, "N": n_orb, "configs_per_step": a.configs, "field": "ZTWO", "rng": "RANLXS2",
-            "seed": a.seed, "precision": a.precision, "sources": "plane waves (Fermi sea E_F=%g)" % a.ef,
+            "seed": a.seed, "precision": a.precision, "qr_period": qr_period(a),
+            "sources": "plane waves (Fermi sea E_F=%g)" % a.ef,
             "l2": "inputs larger than L2 (orbitals %.1f GB)" % (a.configs * n_orb * a.L ** 3 * (8 if a.precision == "f32" else 16) / 1e9)}
 
 
@@ -216,6 +224,51 @@ def plain_fp64_gpu(a, ctx, idx, configs: int = 2, slices: int = 8):
             "sample": f"{configs} configurations x {slices} slices, L={a.L}^3 N={n}, FP64, class-API call structure"}
 
 
+# ------------------------------------------------- precision and statistics
+def stat_error(a, ctx, dets, ms_per_step, world):
+    """The second metric: statistical error of <C_N(tau)> = <|det S_N(tau)|^2>
+    from one step's configurations (binned jackknife on the device), scaled to
+    one GPU-second of this throughput (error ~ 1/sqrt(time))."""
+    import torch
+    import nrcps_b200 as nb
+    x = (dets[:, :, -1].abs() ** 2).to(torch.float64).contiguous()  # [n_conf, T]
+    mean, err, em, ee = nb.jackknife(x, 32, True, ctx)
+    mean, err, em, ee = (t.cpu().numpy() for t in (mean, err, em, ee))
+    t_mid = a.T // 2
+    rel = float(err[t_mid] / abs(mean[t_mid]))
+    gpu_s = ms_per_step / 1000.0 / world
+    return {"observable": f"C_N(tau) = <|det S_N(tau)|^2>, N={dets.shape[-1]}, tau={t_mid}",
+            "estimator": "plain", "configs": int(dets.shape[0]), "jackknife_bins": 32,
+            "rel_err": rel, "gpu_seconds": gpu_s, "rel_err_per_gpu_second": rel * gpu_s ** 0.5,
+            "E_eff_tau_mid": float(em[t_mid]), "E_eff_err_tau_mid": float(ee[t_mid])}
+
+
+def precision_report(a, ctx, idx):
+    """FP32 propagation (QR as the bench runs it) against the FP64 mode on the
+    same fields and configurations: per-slice relative error of
+    C_n(tau) = <|det S_n(tau)|^2> (max over n) and of the effective energy
+    E(tau) = log(C_N(tau)/C_N(tau+1)).  The FP64 mode is the one the parity
+    tests hold to 1e-12 of the oracle."""
+    import numpy as np
+    import nrcps_b200 as nb
+    n = a.precision_configs
+    out = {}
+    for prec, qr in (("f32", qr_period(a) if a.precision == "f32" else 8), ("f64", 0)):
+        job = nb.EnsembleJob(L=a.L, T=a.T, n_conf=n, seed=a.seed, precision=prec, fermi_energy=a.ef, qr_period=qr)
+        ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
+        d = ens.run(0).cpu().numpy()
+        ens.close()
+        out[prec] = (np.abs(d) ** 2).mean(0)  # [T, N]
+    c32, c64 = out["f32"], out["f64"]
+    rel_tau = np.max(np.abs(c32 - c64) / np.abs(c64), axis=1)
+    e32 = np.log(c32[:-1, -1] / c32[1:, -1])
+    e64 = np.log(c64[:-1, -1] / c64[1:, -1])
+    e_rel = np.abs(e32 - e64) / np.maximum(np.abs(e64), 1e-300)
+    return {"configs": n, "compare": "FP32 propagation (QR every %d) vs FP64 mode" % (qr_period(a) or 8),
+            "max_rel_err_C": float(rel_tau.max()), "rel_err_C_per_tau": [float("%.3e" % v) for v in rel_tau],
+            "max_rel_err_E_eff": float(e_rel.max()), "target": 1e-5}
+
+
 # -------------------------------------------------------------------- b200
 def run_b200(a):
     import ctypes
@@ -251,7 +304,7 @@ def run_b200(a):
     n_orb = len(idx)
     # each rank runs its own stream, seeded seed + 491 * rank (src/random/random.C:88)
     job = nb.EnsembleJob(L=a.L, T=a.T, n_conf=a.configs, seed=a.seed, rank=rank, precision=a.precision,
-                         fermi_energy=a.ef)
+                         fermi_energy=a.ef, qr_period=qr_period(a))
     ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
     corr = torch.zeros((a.T, n_orb), dtype=torch.float64, device=dev)
 
@@ -270,7 +323,7 @@ def run_b200(a):
         torch.cuda.synchronize(dev)
 
     for i in range(a.warmup):
-        step(i)
+        last_dets = step(i)
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
@@ -279,7 +332,7 @@ def run_b200(a):
     launches0 = ctx_launches = None
     start.record()
     for i in range(a.steps):
-        step(a.warmup + i)
+        last_dets = step(a.warmup + i)
     stop.record()
     barrier()
     clocks.stop()
@@ -359,6 +412,9 @@ def run_b200(a):
            "h2d_bytes_per_step": idx_host.numel() * 4, "d2h_bytes_per_step": dets_host.numel() * 16}
 
     plain = plain_fp64_gpu(a, ctx, idx) if rank == 0 and not a.no_plain else None
+    stat = stat_error(a, ctx, last_dets, ms / a.steps, world) if rank == 0 else None
+    del last_dets
+    prec_report = precision_report(a, ctx, idx) if rank == 0 and a.precision_configs > 0 else None
 
     if rank == 0:
         cb = None if a.no_cpu_baseline else cpu_baseline(a, a.cpu_sample_slices, n_orb)
@@ -367,7 +423,7 @@ def run_b200(a):
                 "vs_baseline": None, "dtype": a.precision, "data": "synthetic (device-drawn fields, plane-wave sources)",
                 "config": workload(a, n_orb), "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
                 "gpu_launches": launches_per_step * a.steps, "clocks": clocks.summary(),
-                "plain_fp64_gpu": plain,
+                "plain_fp64_gpu": plain, "precision_report": prec_report, "stat_error": stat,
                 "speedup_vs_plain_fp64_gpu": (value / world / plain["value"]) if plain else None}
         print(json.dumps(line))
     ens.close()

@@ -324,6 +324,25 @@ nrcps_status nrcps_ensemble_destroy(nrcps_ensemble *ens);
 /* Kernel launches issued by the last run (for launch accounting). */
 nrcps_status nrcps_ensemble_launches(const nrcps_ensemble *ens, long *launches);
 
+/* ---------------------------------------------------------- estimators
+ * Block accumulators of the production drivers in FP64, configurations added
+ * in index order: dev_dets = n_conf x T x nmeas complex (nrcps_ensemble_run
+ * layout); dev_corr = nmeas x T complex,
+ *   mode 0: corr[m][t] = sum_c |det|^2      (production/slater_det/main.C:208-211),
+ *   mode 1: corr[m][t] = sum_c det          (production/slater_det2_trapped/main-no_cum.C:205-207);
+ * n_cumulants = Nc in 0..8: dev_z = Nc x nmeas x T doubles,
+ *   z[k][m][t] = sum_c (log|det|)^(k+1)     (production/slater_det2_trapped/main-cum.C:219-233). */
+nrcps_status nrcps_accumulate(nrcps_context *ctx, const double *dev_dets, int n_conf, int T, int nmeas,
+                              int mode, int n_cumulants, double *dev_corr, double *dev_z);
+/* Binned jackknife (no counterpart in the reference, whose drivers write
+ * block averages for offline analysis): dev_x = n_samples x n_obs doubles;
+ * mean / err of every observable over n_bins bins of consecutive samples
+ * (remainder dropped).  With dev_eff_mean / dev_eff_err (n_obs - 1 each, or
+ * both NULL) the observables are read as C(t) of consecutive slices and the
+ * effective energies log(C(t) / C(t+1)) are estimated with jackknife errors. */
+nrcps_status nrcps_jackknife(nrcps_context *ctx, const double *dev_x, long n_samples, int n_obs, int n_bins,
+                             double *dev_mean, double *dev_err, double *dev_eff_mean, double *dev_eff_err);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -93,6 +93,8 @@ SIGNATURES = {
     "nrcps_ensemble_run": ([_P, _U64, _P], _I),
     "nrcps_ensemble_destroy": ([_P], _I),
     "nrcps_ensemble_launches": ([_P, _LP], _I),
+    "nrcps_accumulate": ([_P, _P, _I, _I, _I, _I, _I, _P, _P], _I),
+    "nrcps_jackknife": ([_P, _P, _L, _I, _I, _P, _P, _P, _P], _I),
 }
 
 _lib = None

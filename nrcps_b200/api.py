@@ -474,6 +474,39 @@ def slater_dets(S: torch.Tensor, psi1: Optional[torch.Tensor] = None, mode: int 
     return out
 
 
+def accumulate(dets: torch.Tensor, mode: str = "slater", n_cumulants: int = 0, ctx: Optional[Context] = None):
+    """Block sums of the production drivers on the device (FP64):
+    corr [nmeas, T] complex = sum_c |det|^2 (mode 'slater', main.C:208-211) or
+    sum_c det (mode 'slater2', main-no_cum.C:205-207), and for n_cumulants = Nc > 0
+    z [Nc, nmeas, T] = sum_c (log|det|)^(k+1) (main-cum.C:219-233).
+    dets: [n_conf, T, nmeas] complex128 on the device."""
+    ctx = ctx or default_context()
+    d = dets.to(torch.complex128).contiguous()
+    n_conf, T, nmeas = d.shape
+    corr = torch.empty((nmeas, T), dtype=torch.complex128, device=ctx.device)
+    z = torch.empty((max(n_cumulants, 0), nmeas, T), dtype=torch.float64, device=ctx.device)
+    ctx.check(lib().nrcps_accumulate(ctx.handle, _ptr(d), n_conf, T, nmeas, 0 if mode == "slater" else 1,
+                                     n_cumulants, _ptr(corr), _ptr(z) if n_cumulants > 0 else None), "accumulate")
+    return corr, z
+
+
+def jackknife(x: torch.Tensor, n_bins: int, effective_energy: bool = False, ctx: Optional[Context] = None):
+    """Binned jackknife on the device: x [n_samples, n_obs] FP64 -> (mean, err),
+    plus (E_eff, E_eff err) of log(C(t)/C(t+1)) when effective_energy."""
+    ctx = ctx or default_context()
+    x = x.to(torch.float64).contiguous()
+    n, n_obs = x.shape
+    mean = torch.empty(n_obs, dtype=torch.float64, device=ctx.device)
+    err = torch.empty_like(mean)
+    em = torch.empty(max(n_obs - 1, 1), dtype=torch.float64, device=ctx.device) if effective_energy else None
+    ee = torch.empty_like(em) if effective_energy else None
+    ctx.check(lib().nrcps_jackknife(ctx.handle, _ptr(x), n, n_obs, n_bins, _ptr(mean), _ptr(err), _ptr(em),
+                                    _ptr(ee)), "jackknife")
+    if effective_energy:
+        return mean, err, em[: n_obs - 1], ee[: n_obs - 1]
+    return mean, err
+
+
 class SlaterDet:
     """SlaterDet (src/slater_det/slater_det.C): S[s][t] = <src_s|prop_t>, det of leading minors."""
 

@@ -145,10 +145,18 @@ __device__ __forceinline__ cplx<R> twiddle(cplx<R> x) {
     else return cplx<R>{x.im, -x.re};
   } else {
     if constexpr (sizeof(R) == 4) {
-      constexpr CSf w = unit_root_f32(k, N);
-      constexpr float c = w.c;
-      constexpr float s = SIGN > 0 ? w.s : -w.s;
-      return cplx<R>{x.re * c - x.im * s, x.re * s + x.im * c};
+      // The root carried as an unevaluated float pair hi + lo (exact to
+      // ~1e-15): a single-float root is off by up to half an ulp in phase
+      // and modulus, the same error at every step, and drives a systematic
+      // drift of |det|^2 (~2e-6 per step at L = 32, N = 19).  The small
+      // terms are added first, the hi products last.
+      constexpr CS w = unit_root(k, N);
+      constexpr double sd = SIGN > 0 ? w.s : -w.s;
+      constexpr float ch = (float)w.c, cl = (float)(w.c - (double)(float)w.c);
+      constexpr float sh = (float)sd, sl = (float)(sd - (double)(float)sd);
+      const float re = fmaf(x.re, ch, fmaf(-x.im, sh, fmaf(x.re, cl, -x.im * sl)));
+      const float im = fmaf(x.re, sh, fmaf(x.im, ch, fmaf(x.re, sl, x.im * cl)));
+      return cplx<R>{re, im};
     } else {
       constexpr CS w = unit_root(k, N);
       constexpr R c = (R)w.c;
@@ -198,12 +206,17 @@ template <int SIGN, typename R>
 struct Butterfly<3, SIGN, R> {
   static __device__ __forceinline__ void run(cplx<R>* t) {
     constexpr R c = (R)-0.5;
-    // sin(2 pi / 3); in FP32 the float that keeps c^2 + s^2 closest to 1
-    constexpr R s = sizeof(R) == 4 ? (R)unit_root_f32(1, 3).s : (R)0.86602540378443864676372317075293618;
+    // sin(2 pi / 3), in FP32 as hi + lo (see twiddle())
+    constexpr double sd = 0.86602540378443864676372317075293618;
+    constexpr R sh = (R)sd;
+    constexpr R sl = (R)(sd - (double)(R)sd);
     cplx<R> u = add(t[1], t[2]);
     cplx<R> v = sub(t[1], t[2]);
     cplx<R> m{t[0].re + c * u.re, t[0].im + c * u.im};
-    cplx<R> iv = mul_i<SIGN>(cplx<R>{s * v.re, s * v.im});
+    cplx<R> sv;
+    if constexpr (sizeof(R) == 4) sv = cplx<R>{fmaf(v.re, sh, v.re * sl), fmaf(v.im, sh, v.im * sl)};
+    else sv = cplx<R>{sh * v.re, sh * v.im};
+    cplx<R> iv = mul_i<SIGN>(sv);
     t[0] = add(t[0], u);
     t[1] = add(m, iv);
     t[2] = sub(m, iv);
@@ -280,12 +293,20 @@ __device__ __forceinline__ cpk ptwiddle(cpk x) {
     else if constexpr (qs == 2) return cpk{psub(z, x.re), psub(z, x.im)};
     else return cpk{x.im, psub(z, x.re)};
   } else {
-    constexpr CSf w = unit_root_f32(k, N);
-    constexpr float c = w.c;
-    constexpr float s = SIGN > 0 ? w.s : -w.s;
-    const float2 u = __fmul2_rn(x.im, make_float2(-s, -s));
-    const float2 v = __fmul2_rn(x.re, make_float2(s, s));
-    return cpk{__ffma2_rn(x.re, make_float2(c, c), u), __ffma2_rn(x.im, make_float2(c, c), v)};
+    // hi + lo root as in twiddle() above
+    constexpr CS w = unit_root(k, N);
+    constexpr double sd = SIGN > 0 ? w.s : -w.s;
+    constexpr float ch = (float)w.c, cl = (float)(w.c - (double)(float)w.c);
+    constexpr float sh = (float)sd, sl = (float)(sd - (double)(float)sd);
+    float2 u = __fmul2_rn(x.im, make_float2(-sl, -sl));
+    u = __ffma2_rn(x.re, make_float2(cl, cl), u);
+    u = __ffma2_rn(x.im, make_float2(-sh, -sh), u);
+    u = __ffma2_rn(x.re, make_float2(ch, ch), u);
+    float2 v = __fmul2_rn(x.im, make_float2(cl, cl));
+    v = __ffma2_rn(x.re, make_float2(sl, sl), v);
+    v = __ffma2_rn(x.im, make_float2(ch, ch), v);
+    v = __ffma2_rn(x.re, make_float2(sh, sh), v);
+    return cpk{u, v};
   }
 }
 
@@ -323,11 +344,13 @@ template <int SIGN>
 struct PButterfly<3, SIGN> {
   static __device__ __forceinline__ void run(cpk* t) {
     constexpr float c = -0.5f;
-    constexpr float s = unit_root_f32(1, 3).s;
+    constexpr double sd = 0.86602540378443864676372317075293618;
+    constexpr float sh = (float)sd, sl = (float)(sd - (double)(float)sd);
     cpk u = padd(t[1], t[2]);
     cpk v = psub(t[1], t[2]);
     cpk m{__ffma2_rn(u.re, make_float2(c, c), t[0].re), __ffma2_rn(u.im, make_float2(c, c), t[0].im)};
-    cpk sv{__fmul2_rn(v.re, make_float2(s, s)), __fmul2_rn(v.im, make_float2(s, s))};
+    cpk sv{__ffma2_rn(v.re, make_float2(sh, sh), __fmul2_rn(v.re, make_float2(sl, sl))),
+           __ffma2_rn(v.im, make_float2(sh, sh), __fmul2_rn(v.im, make_float2(sl, sl)))};
     t[0] = padd(t[0], u);
     if constexpr (SIGN > 0) {  // m +- i sv
       t[1] = cpk{psub(m.re, sv.im), padd(m.im, sv.re)};

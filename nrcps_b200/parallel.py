@@ -67,6 +67,17 @@ def block_rows(corr, world: int, unload_period: int = 1) -> List[str]:
     return rows
 
 
+def block_rows_cumulants(z, world: int, unload_period: int = 1) -> List[List[str]]:
+    """The cumulant files' rows for one block (results/z<k+1>.<m+1>,
+    production/slater_det2_trapped/main-cum.C:263-270): per cumulant k and
+    measured minor m one line of T values '%.15e ' (real part), averaged over
+    world * unload_period."""
+    zz = z.cpu().numpy() if isinstance(z, torch.Tensor) else np.asarray(z)
+    block = float(world * unload_period)
+    return [["".join("%.*e " % (PREC, v / block) for v in zz[k, m]) for m in range(zz.shape[1])]
+            for k in range(zz.shape[0])]
+
+
 def write_block(files: Iterable, corr, world: int, unload_period: int = 1) -> None:
     """Appends one block row to each results/slater.<n> stream (rank 0 only)."""
     for f, row in zip(files, block_rows(corr, world, unload_period)):

@@ -298,6 +298,33 @@ def minor_det(S: np.ndarray, n: int, t0: int = -1, psi1=None, log: bool = False)
     return complex(out[0], out[1])
 
 
+# ------------------------------------------------------------ estimators
+def block_sums(dets: np.ndarray, mode: str = "slater", n_cumulants: int = 0):
+    """The production drivers' per-block accumulation, configuration by
+    configuration in index order (pure Python loops; small inputs only):
+    corr[m][t] += tmp * conj(tmp)            production/slater_det/main.C:208-211 (mode 'slater')
+    corr[m][t] += slat                       production/slater_det2_trapped/main-no_cum.C:205-207
+    cum[0] = log(abs(slat)); cum[k] = cum[0] * cum[k-1]; z[k][m][t] += cum[k]
+                                             production/slater_det2_trapped/main-cum.C:219-233
+    dets [n_conf, T, nmeas] complex -> corr [nmeas, T] complex, z [Nc, nmeas, T] real."""
+    d = np.asarray(dets, dtype=np.complex128)
+    n_conf, T, nmeas = d.shape
+    corr = np.zeros((nmeas, T), dtype=np.complex128)
+    z = np.zeros((n_cumulants, nmeas, T))
+    for c in range(n_conf):
+        for t in range(T):
+            for m in range(nmeas):
+                v = d[c, t, m]
+                corr[m, t] += (v * np.conj(v)).real if mode == "slater" else v
+                if n_cumulants:
+                    cum = np.log(abs(v))
+                    p = cum
+                    for k in range(n_cumulants):
+                        z[k, m, t] += p
+                        p = cum * p
+    return corr, z
+
+
 # ---------------------------------------------------------------- ensemble
 class _OJob(ctypes.Structure):
     _fields_ = [

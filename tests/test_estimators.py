@@ -1,0 +1,78 @@
+"""Block accumulators, cumulant sums, their result rows and the jackknife.
+
+CPU: the oracle's restatement of the drivers' accumulation against a
+vectorised numpy form, and the result-file rows.  GPU: the device kernels
+(nrcps_accumulate, nrcps_jackknife) against the oracle and a direct numpy
+jackknife.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from nrcps_b200 import parallel
+
+
+def _dets(n_conf, T, nmeas, seed):
+    rs = np.random.default_rng(seed)
+    return rs.standard_normal((n_conf, T, nmeas)) + 1j * rs.standard_normal((n_conf, T, nmeas))
+
+
+def _np_jackknife(x, n_bins, eff=False):
+    per = x.shape[0] // n_bins
+    x = x[: per * n_bins]
+    tot = x.sum(0)
+    loo = (tot[None, :] - x.reshape(n_bins, per, -1).sum(1)) / (x.shape[0] - per)
+    mu = tot / x.shape[0]
+    f = (n_bins - 1) / n_bins
+    err = np.sqrt(f * ((loo - mu) ** 2).sum(0))
+    if not eff:
+        return mu, err
+    e0 = np.log(tot[:-1] / tot[1:])
+    bs = x.reshape(n_bins, per, -1).sum(1)
+    eb = np.log((tot[None, :-1] - bs[:, :-1]) / (tot[None, 1:] - bs[:, 1:]))
+    return mu, err, e0, np.sqrt(f * ((eb - e0) ** 2).sum(0))
+
+
+def test_oracle_block_sums_match_numpy():
+    d = _dets(7, 5, 6, 1)
+    corr, z = O.block_sums(d, "slater2", 4)
+    assert np.allclose(corr, d.sum(0).T, rtol=1e-14)
+    l = np.log(np.abs(d))
+    for k in range(4):
+        assert np.allclose(z[k], (l ** (k + 1)).sum(0).T, rtol=1e-13)
+    corr0, _ = O.block_sums(d, "slater", 0)
+    assert np.allclose(corr0.real, (np.abs(d) ** 2).sum(0).T, rtol=1e-14)
+
+
+def test_cumulant_rows_format():
+    z = np.arange(2 * 3 * 4, dtype=float).reshape(2, 3, 4) + 0.5
+    rows = parallel.block_rows_cumulants(z, world=2, unload_period=1)
+    assert len(rows) == 2 and len(rows[0]) == 3
+    assert rows[1][2] == "".join("%.15e " % (v / 2.0) for v in z[1, 2])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,nc", [("slater", 0), ("slater2", 6), ("slater", 3)])
+def test_device_accumulate_matches_oracle(mode, nc):
+    import torch
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    d = _dets(33, 9, 8, 2)
+    corr, z = nb.accumulate(torch.from_numpy(d).to(ctx.device), mode, nc, ctx)
+    rc, rz = O.block_sums(d, mode, nc)
+    assert np.allclose(corr.cpu().numpy(), rc, rtol=1e-13, atol=0)
+    if nc:
+        assert np.allclose(z.cpu().numpy(), rz, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_device_jackknife_matches_numpy():
+    import torch
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    rs = np.random.default_rng(3)
+    x = np.exp(-0.1 * np.arange(12))[None, :] * (1.0 + 0.1 * rs.standard_normal((1003, 12)))
+    mu, err, em, ee = nb.jackknife(torch.from_numpy(x).to(ctx.device), 17, True, ctx)
+    rmu, rerr, rem, ree = _np_jackknife(x, 17, True)
+    for a, b in ((mu, rmu), (err, rerr), (em, rem), (ee, ree)):
+        assert np.allclose(a.cpu().numpy(), b, rtol=1e-10, atol=0)

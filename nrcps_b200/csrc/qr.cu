@@ -16,56 +16,101 @@
 
 namespace nrcps {
 
-// G[c][i][j] = sum_p conj(psi_{c,i}(p)) psi_{c,j}(p); one block per (c, j).
-template <typename R>
-__global__ void __launch_bounds__(256) gram_kernel(const void* __restrict__ psi, int N, long vol,
-                                                   double* __restrict__ G) {
-  const long cj = blockIdx.x;
-  const long c = cj / N;
-  const int j = (int)(cj % N);
+// G[c][i][j] for i <= j (the upper triangle the Cholesky reads), one block
+// per configuration reading its orbitals once: tiles of GT sites of all N
+// orbitals go through shared memory (rows padded by one element so that the
+// rows a warp reads fall in different banks); each thread accumulates 2 x 2
+// blocks (i, i+1) x (j, j+1) of G over a quarter of each tile's sites, in R
+// within a tile and in FP64 across tiles; the four quarters are summed at
+// the end.
+constexpr int GT = 128;
+template <typename R, int MAXB>
+__global__ void __launch_bounds__(256) gram_tile_kernel(const void* __restrict__ psi, int N, long vol,
+                                                        double* __restrict__ G) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  cplx<R>* tile = reinterpret_cast<cplx<R>*>(gsm);  // [N][GT + 1]
+  const long c = blockIdx.x;
   const cplx<R>* base = reinterpret_cast<const cplx<R>*>(psi) + (size_t)c * N * vol;
-  __shared__ double red[8][2][8];
-  for (int i0 = 0; i0 < N; i0 += 8) {
-    double ar[8], ai[8];
+  const int nb = (N + 1) / 2;                // 2-row blocks
+  const int nblk = nb * (nb + 1) / 2;        // upper-triangular block pairs
+  const int lane64 = threadIdx.x & 63, grp = threadIdx.x >> 6;
+  // MAXB: 2-row block pairs per thread, ceil(nblk / 64): 2 for N <= 22, 3 for N <= 32, 9 for N <= 64
+  double acc[MAXB][8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) ar[k] = ai[k] = 0.0;
-    for (long p = threadIdx.x; p < vol; p += blockDim.x) {
-      cplx<R> q = base[(size_t)j * vol + p];
-      const double qr = q.re, qi = q.im;
+  for (int b = 0; b < MAXB; ++b)
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (i0 + k < N) {
-          cplx<R> a = base[(size_t)(i0 + k) * vol + p];
-          ar[k] += (double)a.re * qr + (double)a.im * qi;
-          ai[k] += (double)a.re * qi - (double)a.im * qr;
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-      for (int o = 16; o > 0; o >>= 1) {
-        ar[k] += __shfl_down_sync(0xffffffffu, ar[k], o);
-        ai[k] += __shfl_down_sync(0xffffffffu, ai[k], o);
-      }
-    if ((threadIdx.x & 31) == 0)
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        red[threadIdx.x >> 5][0][k] = ar[k];
-        red[threadIdx.x >> 5][1][k] = ai[k];
-      }
+    for (int k = 0; k < 8; ++k) acc[b][k] = 0.0;
+  for (long p0 = 0; p0 < vol; p0 += GT) {
+    const int ts = (int)((vol - p0) < GT ? (vol - p0) : GT);
     __syncthreads();
-    if (threadIdx.x < 8 && i0 + (int)threadIdx.x < N) {
-      const int k = threadIdx.x;
-      double sr = 0, si = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-        sr += red[w][0][k];
-        si += red[w][1][k];
-      }
-      double* g = G + 2 * ((c * N + (i0 + k)) * (long)N + j);
-      g[0] = sr;
-      g[1] = si;
+    for (int e = threadIdx.x; e < N * GT; e += blockDim.x) {
+      const int i = e / GT, s = e - i * GT;
+      tile[i * (GT + 1) + s] = s < ts ? base[(size_t)i * vol + p0 + s] : cplx<R>{(R)0, (R)0};
     }
     __syncthreads();
+#pragma unroll
+    for (int b = 0; b < MAXB; ++b) {
+      const int blk = lane64 + 64 * b;
+      if (blk >= nblk) break;
+      // blk -> (bi, bj), bi <= bj, row-major over the upper triangle
+      int bi = 0, rem = blk;
+      while (rem >= nb - bi) {
+        rem -= nb - bi;
+        ++bi;
+      }
+      const int bj = bi + rem;
+      const int i0 = 2 * bi, j0 = 2 * bj;
+      const int i1 = i0 + 1 < N ? i0 + 1 : i0, j1 = j0 + 1 < N ? j0 + 1 : j0;
+      R s[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) s[k] = (R)0;
+      for (int q = grp; q < GT; q += 4) {
+        const cplx<R> a0 = tile[i0 * (GT + 1) + q], a1 = tile[i1 * (GT + 1) + q];
+        const cplx<R> b0 = tile[j0 * (GT + 1) + q], b1 = tile[j1 * (GT + 1) + q];
+        // conj(a) b
+        s[0] += a0.re * b0.re + a0.im * b0.im;
+        s[1] += a0.re * b0.im - a0.im * b0.re;
+        s[2] += a0.re * b1.re + a0.im * b1.im;
+        s[3] += a0.re * b1.im - a0.im * b1.re;
+        s[4] += a1.re * b0.re + a1.im * b0.im;
+        s[5] += a1.re * b0.im - a1.im * b0.re;
+        s[6] += a1.re * b1.re + a1.im * b1.im;
+        s[7] += a1.re * b1.im - a1.im * b1.re;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[b][k] += (double)s[k];
+    }
+  }
+  // sum the four site quarters through shared memory, write the upper triangle
+  __syncthreads();
+  double* red = reinterpret_cast<double*>(gsm);  // [nblk][8] (fits: tile area >= 9 KB)
+  for (int g = 0; g < 4; ++g) {
+    if (grp == g) {
+#pragma unroll
+      for (int b = 0; b < MAXB; ++b) {
+        const int blk = lane64 + 64 * b;
+        if (blk >= nblk) break;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) red[blk * 8 + k] = (g == 0 ? 0.0 : red[blk * 8 + k]) + acc[b][k];
+      }
+    }
+    __syncthreads();
+  }
+  for (int blk = threadIdx.x; blk < nblk; blk += blockDim.x) {
+    int bi = 0, rem = blk;
+    while (rem >= nb - bi) {
+      rem -= nb - bi;
+      ++bi;
+    }
+    const int bj = bi + rem;
+    for (int u = 0; u < 2; ++u)
+      for (int v = 0; v < 2; ++v) {
+        const int i = 2 * bi + u, j = 2 * bj + v;
+        if (i >= N || j >= N || i > j) continue;
+        double* g = G + 2 * ((c * N + i) * (long)N + j);
+        g[0] = red[blk * 8 + 4 * u + 2 * v];
+        g[1] = red[blk * 8 + 4 * u + 2 * v + 1];
+      }
   }
 }
 
@@ -198,12 +243,29 @@ static nrcps_status launch_apply(nrcps_context* ctx, void* psi, int N, long vol,
 nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
                                  double* G, double* logR) {
   if (N > 64) return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "QR re-orthonormalisation supports N <= 64");
-  if (prec == NRCPS_F64)
-    gram_kernel<double><<<(unsigned)((long)nconf * N), 256, 0, ctx->stream>>>(psi, N, vol, G);
-  else
-    gram_kernel<float><<<(unsigned)((long)nconf * N), 256, 0, ctx->stream>>>(psi, N, vol, G);
-  ctx->launches++;
-  NRCPS_TRY(check_launch(ctx, "gram_kernel"));
+  {
+    const size_t esz = prec == NRCPS_F64 ? sizeof(cplx<double>) : sizeof(cplx<float>);
+    size_t sh = esz * (size_t)N * (GT + 1);
+    const size_t red = sizeof(double) * 8 * 528;
+    if (sh < red) sh = red;
+    // N <= 64 rows of GT + 1 FP64 complex values: up to 132 KB of shared memory
+    const int big = (int)(sizeof(cplx<double>) * 64 * (GT + 1));
+    auto launch = [&](auto kern) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+      kern<<<(unsigned)nconf, 256, sh, ctx->stream>>>(psi, N, vol, G);
+    };
+    if (prec == NRCPS_F64) {
+      if (N <= 22) launch(gram_tile_kernel<double, 2>);
+      else if (N <= 32) launch(gram_tile_kernel<double, 3>);
+      else launch(gram_tile_kernel<double, 9>);
+    } else {
+      if (N <= 22) launch(gram_tile_kernel<float, 2>);
+      else if (N <= 32) launch(gram_tile_kernel<float, 3>);
+      else launch(gram_tile_kernel<float, 9>);
+    }
+    ctx->launches++;
+    NRCPS_TRY(check_launch(ctx, "gram_tile_kernel"));
+  }
   chol_inv_kernel<<<grid_for(nconf, 64), 64, 0, ctx->stream>>>(G, N, nconf, logR);
   ctx->launches++;
   NRCPS_TRY(check_launch(ctx, "chol_inv_kernel"));

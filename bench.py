@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 peer access, 1 split, 2 bulk staged, 3 bulk L2, 4-6 packed 0/2/3")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU path measurement")
     ap.add_argument("--qr", type=int, default=-1, help="re-orthonormalise every k slices (-1: 8 for f32, 0 for f64)")
+    ap.add_argument("--workload", default="batched", choices=["batched", "uneven"],
+                    help="batched: the L=32 ensemble (default); uneven: 512 jobs of random (L, N, T) in one launch")
+    ap.add_argument("--jobs", type=int, default=512, help="jobs of the uneven workload")
     ap.add_argument("--precision-configs", type=int, default=64,
                     help="configurations of the FP32-vs-FP64 precision report (0: skip)")
     return ap.parse_args()
@@ -433,10 +436,65 @@ def run_b200(a):
     return 0
 
 
+# ------------------------------------------------------------ uneven batch
+def uneven_jobs(n_jobs: int, seed: int = 99):
+    """The uneven workload: per job L in {16, 24, 32, 48}, N in {7, 19, 33}
+    (closed shells |n|^2 <= 1, 2, 4) and T in {32, 64, 128}, each drawn
+    uniformly from `seed`; one configuration per job."""
+    import numpy as np
+    import nrcps_b200 as nb
+    rs = np.random.default_rng(seed)
+    shell = {7: 1.5, 19: 2.5, 33: 4.5}  # E_F between shells, in units of (2 pi / L)^2 / 2
+    jobs = []
+    for _ in range(n_jobs):
+        L = int(rs.choice([16, 24, 32, 48]))
+        N = int(rs.choice([7, 19, 33]))
+        T = int(rs.choice([32, 64, 128]))
+        ef = 0.5 * (2 * np.pi / L) ** 2 * shell[N]
+        jobs.append(nb.BatchJob(L=L, T=T, n_conf=1, fermi_energy=ef))
+    return jobs
+
+
+def run_uneven(a):
+    """512 jobs of uneven (L, N, T), Gaussian fields a = 0.3, FP32 orbitals and
+    FP64 determinants, every time loop in one graph launch per run."""
+    import torch
+    import nrcps_b200 as nb
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    ctx = nb.Context(0)
+    jobs = uneven_jobs(a.jobs)
+    b = nb.Batch(jobs, seed=99, field="GAUSS", a=0.3, precision=a.precision, ctx=ctx)
+    slices = sum(j.T * j.n_conf for j in jobs)
+    for _ in range(a.warmup):
+        b.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        b.run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    shapes = sorted({(j.L, n, ) for j, n in zip(jobs, b.n_orb)})
+    line = {"metric": "uneven batch config·slices/s", "value": slices / (ms / 1000.0), "unit": UNIT, "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": a.precision, "data": "synthetic (device-drawn Gaussian fields)",
+            "config": {"workload": f"{len(jobs)} jobs, L in 16/24/32/48, N in 7/19/33, T in 32/64/128 drawn from "
+                                   f"seed 99, Gaussian phi a=0.3, one graph launch per step (fields drawn before it)",
+                       "jobs": len(jobs), "config_slices_per_step": slices, "groups": len(shapes)},
+            "gpu_launches_in_graph": b.launches()}
+    print(json.dumps(line))
+    b.close()
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "uneven":
+        return run_uneven(a)
     return run_b200(a)
 
 

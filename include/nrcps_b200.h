@@ -220,6 +220,10 @@ typedef struct {
   uint64_t conf_stride; /* elements (mode 0/2) or bits (mode 1) between configurations */
   double a;
   const double *dev_pos; /* may be NULL */
+  /* may be NULL; else a device array of nconf offsets that replaces
+   * conf * conf_stride (configurations whose fields are not evenly spaced,
+   * as in a batch of jobs of different sizes): k = bit0 + conf_base[conf] + site */
+  const uint64_t *dev_conf_base;
 } nrcps_position_factor;
 nrcps_status nrcps_propagate(nrcps_context *ctx, void *psi, int batch, int nconf, const int dims[3],
                              const double *dev_kin, const nrcps_position_factor *w,
@@ -323,6 +327,43 @@ nrcps_status nrcps_ensemble_run(nrcps_ensemble *ens, uint64_t first_conf, double
 nrcps_status nrcps_ensemble_destroy(nrcps_ensemble *ens);
 /* Kernel launches issued by the last run (for launch accounting). */
 nrcps_status nrcps_ensemble_launches(const nrcps_ensemble *ens, long *launches);
+
+/* --------------------------------------------------------------- batch
+ * Jobs of different lattice size, particle number and time extent advanced
+ * together, the time loops of all jobs in one CUDA graph launch (no
+ * counterpart in the reference, whose drivers run one system per process:
+ * production/slater_det/main.C:185-220).  Every job: plane-wave sources
+ * (pw_index, n_orb lattice indices), the local interaction (1 + a phi)/V,
+ * Kinetic with the given xi table (L^3 entries), measurement mode 0.  Jobs
+ * with equal (L, n_orb) share launches; fields come from one generator
+ * stream in job order (job j, configuration k, slice t reads sites
+ * base_j + (k T_j + t) L_j^3 ...), and every run continues the stream. */
+typedef struct {
+  int L;
+  int n_orb;
+  int T;
+  int n_conf;
+  const int *pw_index; /* host */
+  const double *kin_xi; /* host */
+} nrcps_batch_job;
+typedef struct {
+  int rng_kind;
+  long seed;
+  int field_kind;
+  int precision; /* nrcps_precision of the orbitals */
+  double a;
+  int qr_period; /* 0: none */
+} nrcps_batch_params;
+typedef struct nrcps_batch nrcps_batch;
+nrcps_status nrcps_batch_create(nrcps_context *ctx, const nrcps_batch_params *params, const nrcps_batch_job *jobs,
+                                int njobs, nrcps_batch **batch);
+/* Output of a run: one device buffer of *doubles doubles; job j's
+ * determinants are [n_conf][T][n_orb] complex at *offset (nrcps_batch_layout).
+ * *launches = kernel launches inside the graph of one run. */
+nrcps_status nrcps_batch_output_size(const nrcps_batch *batch, long *doubles, long *launches);
+nrcps_status nrcps_batch_layout(const nrcps_batch *batch, int job, long *offset, long *doubles);
+nrcps_status nrcps_batch_run(nrcps_batch *batch, double *dev_out);
+nrcps_status nrcps_batch_destroy(nrcps_batch *batch);
 
 /* ---------------------------------------------------------- estimators
  * Block accumulators of the production drivers in FP64, configurations added

@@ -35,7 +35,8 @@ class NrcpsError(RuntimeError):
 
 class PositionFactor(ctypes.Structure):
     _fields_ = [("field_mode", ctypes.c_int), ("dev_field", ctypes.c_void_p), ("bit0", ctypes.c_uint64),
-                ("conf_stride", ctypes.c_uint64), ("a", ctypes.c_double), ("dev_pos", ctypes.c_void_p)]
+                ("conf_stride", ctypes.c_uint64), ("a", ctypes.c_double), ("dev_pos", ctypes.c_void_p),
+                ("dev_conf_base", ctypes.c_void_p)]
 
 
 class Job(ctypes.Structure):
@@ -44,6 +45,16 @@ class Job(ctypes.Structure):
                 ("mode", ctypes.c_int), ("precision", ctypes.c_int), ("plane_wave", ctypes.c_int),
                 ("use_potential", ctypes.c_int), ("qr_period", ctypes.c_int), ("a", ctypes.c_double),
                 ("local_interaction", ctypes.c_int)]
+
+
+class BatchJob(ctypes.Structure):
+    _fields_ = [("L", ctypes.c_int), ("n_orb", ctypes.c_int), ("T", ctypes.c_int), ("n_conf", ctypes.c_int),
+                ("pw_index", ctypes.POINTER(ctypes.c_int)), ("kin_xi", ctypes.POINTER(ctypes.c_double))]
+
+
+class BatchParams(ctypes.Structure):
+    _fields_ = [("rng_kind", ctypes.c_int), ("seed", ctypes.c_long), ("field_kind", ctypes.c_int),
+                ("precision", ctypes.c_int), ("a", ctypes.c_double), ("qr_period", ctypes.c_int)]
 
 
 # Every exported symbol with its argument and result types.
@@ -94,6 +105,11 @@ SIGNATURES = {
     "nrcps_ensemble_destroy": ([_P], _I),
     "nrcps_ensemble_launches": ([_P, _LP], _I),
     "nrcps_accumulate": ([_P, _P, _I, _I, _I, _I, _I, _P, _P], _I),
+    "nrcps_batch_create": ([_P, _P, _P, _I, ctypes.POINTER(_P)], _I),
+    "nrcps_batch_output_size": ([_P, _LP, _LP], _I),
+    "nrcps_batch_layout": ([_P, _I, _LP, _LP], _I),
+    "nrcps_batch_run": ([_P, _P], _I),
+    "nrcps_batch_destroy": ([_P], _I),
     "nrcps_jackknife": ([_P, _P, _L, _I, _I, _P, _P, _P, _P], _I),
 }
 

@@ -571,6 +571,80 @@ class EnsembleJob:
         return (self.L, self.L, self.L)
 
 
+@dataclass
+class BatchJob:
+    """One job of a Batch: an L^3 lattice, T slices, n_conf configurations,
+    plane-wave sources (the Fermi sea of `fermi_energy`, or an explicit
+    lattice-index list)."""
+    L: int
+    T: int
+    n_conf: int = 1
+    fermi_energy: float = 0.1
+    pw_index: Optional[list] = None
+
+
+class Batch:
+    """nrcps_batch: jobs of different L, N and T, all time loops in one graph
+    launch; fields from one generator stream in job order."""
+
+    def __init__(self, jobs: Sequence[BatchJob], rng: str = "RANLXS2", seed: int = 99, field: str = "GAUSS",
+                 a: float = 0.3, precision: str = "f32", qr_period: int = 0, kin_dt: float = 0.5,
+                 cutoff: float = 2.0, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.jobs = list(jobs)
+        n = len(self.jobs)
+        self._keep = []
+        arr = (C.BatchJob * n)()
+        self.n_orb = []
+        for i, jb in enumerate(self.jobs):
+            dims = (jb.L,) * 3
+            idx = jb.pw_index if jb.pw_index is not None else momenta(dims, "PERFECT", 1.0, jb.fermi_energy, cutoff)[0]
+            idx = np.ascontiguousarray(np.asarray(idx, dtype=np.int32))
+            xi = np.ascontiguousarray(kinetic_table(dims, "PERFECT", 1.0, kin_dt, cutoff))
+            self._keep += [idx, xi]
+            self.n_orb.append(int(idx.size))
+            arr[i].L, arr[i].n_orb, arr[i].T, arr[i].n_conf = jb.L, idx.size, jb.T, jb.n_conf
+            arr[i].pw_index = idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+            arr[i].kin_xi = xi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        p = C.BatchParams()
+        p.rng_kind, p.seed, p.field_kind = C.RNG_KINDS[rng], seed, C.FIELD_KINDS[field]
+        p.precision, p.a, p.qr_period = _prec(precision), a, qr_period
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().nrcps_batch_create(self.ctx.handle, ctypes.byref(p), arr, n, ctypes.byref(h)),
+                       "batch_create")
+        self.handle = h
+        size = ctypes.c_long()
+        self.ctx.check(lib().nrcps_batch_output_size(h, ctypes.byref(size), None), "batch_output_size")
+        self.out = torch.empty(size.value // 2, dtype=torch.complex128, device=self.ctx.device)
+        self.layout = []
+        for i in range(n):
+            off, sz = ctypes.c_long(), ctypes.c_long()
+            self.ctx.check(lib().nrcps_batch_layout(h, i, ctypes.byref(off), ctypes.byref(sz)), "batch_layout")
+            self.layout.append((off.value // 2, sz.value // 2))
+
+    def run(self):
+        """One run (the next window of the stream); returns one [n_conf, T, N]
+        complex128 device view per job."""
+        self.ctx.check(lib().nrcps_batch_run(self.handle, _ptr(self.out)), "batch_run")
+        return [self.out[o:o + s].view(jb.n_conf, jb.T, n) for (o, s), jb, n in zip(self.layout, self.jobs, self.n_orb)]
+
+    def launches(self) -> int:
+        v = ctypes.c_long()
+        self.ctx.check(lib().nrcps_batch_output_size(self.handle, None, ctypes.byref(v)), "batch_output_size")
+        return v.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().nrcps_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Ensemble:
     """nrcps_ensemble: every configuration of a run advanced together, time loop in a CUDA graph."""
 

@@ -44,6 +44,7 @@ struct FusedArgs {
   const void* field;
   uint64_t off0;          // element/bit offset of configuration 0
   uint64_t conf_stride;
+  const uint64_t* conf_base;  // optional per-configuration offsets (replace conf * conf_stride)
   double a;
   double vol;
   double w_plus, w_minus;  // (1 + a)/V and (1 - a)/V for Z2 fields
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
 
   for (; orb < f.n_orb_total; orb += n_clusters) {
     const long conf = orb / f.batch;
-    const uint64_t kb = f.off0 + (uint64_t)conf * f.conf_stride;  // field offset of this configuration
+    const uint64_t kb = f.off0 + (f.conf_base ? __ldg(f.conf_base + conf) : (uint64_t)conf * f.conf_stride);  // field offset of this configuration
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> x[L];
     if constexpr (STAGED) {
@@ -390,7 +391,7 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
 
   for (; orb < f.n_orb_total; orb += n_clusters) {
     const long conf = orb / f.batch;
-    const uint64_t kb = f.off0 + (uint64_t)conf * f.conf_stride;
+    const uint64_t kb = f.off0 + (f.conf_base ? __ldg(f.conf_base + conf) : (uint64_t)conf * f.conf_stride);
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> v[H];
     mbar_wait_bounded(bar, parity, f.err);
@@ -630,7 +631,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
 
   for (; orb < f.n_orb_total; orb += n_clusters) {
     const long conf = orb / f.batch;
-    const uint64_t kb = f.off0 + (uint64_t)conf * f.conf_stride;
+    const uint64_t kb = f.off0 + (f.conf_base ? __ldg(f.conf_base + conf) : (uint64_t)conf * f.conf_stride);
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> x[L];
     if constexpr (STAGED) {
@@ -1013,6 +1014,7 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   f.field = w->dev_field;
   f.off0 = w->bit0;
   f.conf_stride = w->conf_stride;
+  f.conf_base = w->dev_conf_base;
   f.a = w->a;
   f.vol = (double)d[0] * d[1] * d[2];
   f.w_plus = (1.0 + f.a) / f.vol;

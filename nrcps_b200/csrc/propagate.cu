@@ -30,6 +30,7 @@ struct FieldArgs {
   const void* field;
   uint64_t bit0;         // element (mode 0/2) or bit (mode 1) offset of configuration 0
   uint64_t conf_stride;  // elements or bits between configurations
+  const uint64_t* conf_base;  // optional per-configuration offsets (replace conf * conf_stride)
   double a;
   double vol;
   const double* pos;     // optional static real factor
@@ -39,7 +40,7 @@ struct FieldArgs {
 template <typename R>
 __device__ __forceinline__ cplx<R> field_factor(const FieldArgs& f, long conf, long site) {
   cplx<R> w;
-  const uint64_t k = f.bit0 + (uint64_t)conf * f.conf_stride + (uint64_t)site;
+  const uint64_t k = f.bit0 + (f.conf_base ? f.conf_base[conf] : (uint64_t)conf * f.conf_stride) + (uint64_t)site;
   if (f.mode == 0) {
     double2 v = reinterpret_cast<const double2*>(f.field)[k];
     w = cplx<R>{(R)v.x, (R)v.y};
@@ -360,6 +361,7 @@ nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf,
   f.field = w->dev_field;
   f.bit0 = w->bit0;
   f.conf_stride = w->conf_stride;
+  f.conf_base = w->dev_conf_base;
   f.a = w->a;
   f.vol = (double)vol_of(d);
   f.pos = w->dev_pos;

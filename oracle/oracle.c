@@ -777,3 +777,48 @@ int o_run_ensemble(const o_job *job, const double *sources, double *dets) {
   free(opp);
   return bad;
 }
+
+/* Jobs in sequence with one generator (see oracle.h).  Follows the driver
+ * loop of production/slater_det/main.C:185-220 per configuration, with the
+ * single-coupling interaction written as its position-space factor. */
+void o_run_batch(int njobs, const int *L, const int *T, const int *nconf, const int *N, const int *const *idx,
+                 int rng_kind, long seed, int field_type, double a, double kin_dt, double cutoff_sq,
+                 double *const *dets) {
+  o_rng rng;
+  o_rng_init(&rng, rng_kind, seed);
+  for (int j = 0; j < njobs; ++j) {
+    const int dims[3] = {L[j], L[j], L[j]};
+    const long vol = (long)L[j] * L[j] * L[j];
+    const int n = N[j];
+    double *xi = (double *)malloc(sizeof(double) * vol);
+    double *lat = (double *)malloc(sizeof(double) * 2 * vol);
+    double *fld = (double *)malloc(sizeof(double) * 2 * vol);
+    double *psi = (double *)malloc(sizeof(double) * 2 * vol * n);
+    double *src = (double *)calloc(2 * vol * n, sizeof(double));
+    double *S = (double *)malloc(sizeof(double) * 2 * n * n);
+    o_kinetic_xi(dims, 2 /* PERFECT */, 1.0, kin_dt, cutoff_sq, xi);
+    for (int m = 0; m < n; ++m) src[2 * ((long)m * vol + idx[j][m])] = 1.0;
+    for (int k = 0; k < nconf[j]; ++k) {
+      memcpy(psi, src, sizeof(double) * 2 * vol * n);
+      for (int t = 0; t < T[j]; ++t) {
+        o_field_slices(&rng, field_type, vol, 1, lat);
+        double *row = dets[j] + 2 * ((long)k * T[j] + t) * n;
+        o_project(vol, n, src, n, psi, S);
+        for (int m = 0; m < n; ++m) o_minor_det(S, n, m + 1, -1, NULL, 0, row + 2 * m);
+        for (long x = 0; x < vol; ++x) {
+          fld[2 * x] = (1.0 + a * lat[2 * x]) / (double)vol;
+          fld[2 * x + 1] = (a * lat[2 * x + 1]) / (double)vol;
+        }
+        o_kinetic_evolve(vol, n, psi, xi);
+        o_interaction_evolve(dims, n, psi, fld);
+        o_kinetic_evolve(vol, n, psi, xi);
+      }
+    }
+    free(xi);
+    free(lat);
+    free(fld);
+    free(psi);
+    free(src);
+    free(S);
+  }
+}

@@ -128,6 +128,16 @@ typedef struct {
  * dets = configs * T * nmeas complex (nmeas = N or 2N). */
 int o_run_ensemble(const o_job *job, const double *sources, double *dets);
 
+/* Jobs run one after another by one process with ONE generator (the stream
+ * semantics of nrcps_batch): job j = (L_j, T_j, n_conf_j) with plane-wave
+ * sources idx_j (N_j lattice indices), local interaction fld = (1 + a phi)/V,
+ * Kinetic xi from (disp PERFECT, mass 1, dt, cutoff_sq); dets_j =
+ * [n_conf_j][T_j][N_j] complex.  Slice t of configuration k of job j is the
+ * (k T_j + t)-th field drawn after all earlier jobs' fields. */
+void o_run_batch(int njobs, const int *L, const int *T, const int *nconf, const int *N, const int *const *idx,
+                 int rng_kind, long seed, int field_type, double a, double kin_dt, double cutoff_sq,
+                 double *const *dets);
+
 #ifdef __cplusplus
 }
 #endif

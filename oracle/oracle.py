@@ -78,6 +78,10 @@ def lib():
         L.o_minor_det.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, dp]
         L.o_fft3d.argtypes = [dp, ip, ctypes.c_int, ctypes.c_int]
         L.o_run_ensemble.argtypes = [ctypes.c_void_p, dp, dp]
+        pp = ctypes.POINTER(ctypes.POINTER(ctypes.c_int))
+        L.o_run_batch.argtypes = [ctypes.c_int, ip, ip, ip, ip, pp, ctypes.c_int, ctypes.c_long, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
         L.o_run_ensemble.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -296,6 +300,26 @@ def minor_det(S: np.ndarray, n: int, t0: int = -1, psi1=None, log: bool = False)
     out = np.zeros(2)
     lib().o_minor_det(_dp(S.view(np.float64)), N, n, t0, _dp(p1.view(np.float64)), int(log), _dp(out))
     return complex(out[0], out[1])
+
+
+# ----------------------------------------------------------------- batch
+def run_batch(jobs, rng: str, seed: int, field: str, a: float, kin_dt: float = 0.5, cutoff: float = 2.0):
+    """Jobs one after another with one generator (o_run_batch): jobs = list of
+    (L, T, n_conf, plane-wave index list); returns one [n_conf, T, N] complex
+    array per job."""
+    n = len(jobs)
+    Ls = (ctypes.c_int * n)(*[j[0] for j in jobs])
+    Ts = (ctypes.c_int * n)(*[j[1] for j in jobs])
+    Cs = (ctypes.c_int * n)(*[j[2] for j in jobs])
+    Ns = (ctypes.c_int * n)(*[len(j[3]) for j in jobs])
+    idx = [np.ascontiguousarray(np.asarray(j[3], dtype=np.int32)) for j in jobs]
+    idx_p = (ctypes.POINTER(ctypes.c_int) * n)(*[i.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) for i in idx])
+    outs = [np.zeros((j[2], j[1], len(j[3])), dtype=np.complex128) for j in jobs]
+    out_p = (ctypes.POINTER(ctypes.c_double) * n)(*[_dp(o.view(np.float64)) for o in outs])
+    c = cutoff * PI
+    lib().o_run_batch(n, Ls, Ts, Cs, Ns, idx_p, RNG_KINDS[rng], seed, FIELD_TYPES[field], ctypes.c_double(a),
+                      ctypes.c_double(kin_dt), ctypes.c_double(c * c), out_p)
+    return outs
 
 
 # ------------------------------------------------------------ estimators

@@ -1,0 +1,94 @@
+"""Uneven batches: jobs of different L, N and T in one graph launch, fields
+from one generator stream in job order.
+
+CPU: the oracle's batch runner (o_run_batch) against the oracle's pinned
+ensemble driver for one job, and the stream order across jobs.  GPU: the
+device batch in FP64 against the oracle within 1e-12, and the FP32 batch at
+the uneven-batch shapes against the FP64 batch.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+FP64_REL = 1e-12
+
+
+def _rel(a, b):
+    """Relative error per (configuration, slice) row of determinants, against
+    the row's largest magnitude (a leading minor can be pure cancellation)."""
+    return np.max(np.max(np.abs(a - b), axis=-1) / np.max(np.abs(b), axis=-1))
+
+
+def _pw(L, ef):
+    idx, _, _ = O.momenta((L,) * 3, "PERFECT", 1.0, ef, (2 * O.PI) ** 2)
+    return list(idx)
+
+
+def test_oracle_batch_single_job_equals_ensemble_driver():
+    """One Z2 job through o_run_batch (local factor (1 + a phi)/V) against
+    o_run_ensemble (Interaction::Initialize with one coupling, a = c V)."""
+    L, T = 8, 5
+    dims = (L,) * 3
+    itab = O.interaction_table(dims, 1.0, [0.019894367886486918], 1.0, (2 * O.PI) ** 2)
+    a = float(itab[0] * L ** 3)
+    idx = _pw(L, 0.35)
+    (b,) = O.run_batch([(L, T, 2, idx)], "RANLXS2", 1234, "ZTWO", a)
+    ref = O.run_ensemble(O.Job(L=L, T=T, configs=2, seed=1234), O.plane_wave_sources(dims, idx))
+    # the ensemble driver draws one extra field after each configuration's last
+    # slice (the reference's Refresh at the end of every slice); the batch does
+    # not -- configuration 0 agrees exactly
+    assert _rel(b[0], ref[0]) < 1e-13
+
+
+def test_oracle_batch_stream_order():
+    """Job 0's determinants do not depend on the jobs after it; job 1's fields
+    continue the stream where job 0's ended."""
+    j0, j1 = (8, 4, 1, _pw(8, 0.35)), (8, 3, 1, _pw(8, 0.12))
+    alone = O.run_batch([j0], "RANLXS2", 7, "GAUSS", 0.3)
+    both = O.run_batch([j0, j1], "RANLXS2", 7, "GAUSS", 0.3)
+    assert np.array_equal(alone[0], both[0])
+    swapped = O.run_batch([j1, j0], "RANLXS2", 7, "GAUSS", 0.3)
+    assert not np.allclose(swapped[1], both[0])
+
+
+_JOBS = [(8, 6, 2, 0.35), (16, 4, 1, 0.1), (8, 3, 3, 0.12), (16, 7, 1, 0.13), (8, 5, 1, 0.35)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("field", ["GAUSS", "ZTWO"])
+def test_device_batch_fp64_matches_oracle(field):
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    jobs = [nb.BatchJob(L=L, T=T, n_conf=c, fermi_energy=ef) for L, T, c, ef in _JOBS]
+    b = nb.Batch(jobs, seed=99, field=field, a=0.3, precision="f64", ctx=ctx)
+    got = [d.cpu().numpy() for d in b.run()]
+    refs = O.run_batch([(L, T, c, _pw(L, ef)) for L, T, c, ef in _JOBS], "RANLXS2", 99, field, 0.3)
+    for g, r in zip(got, refs):
+        assert g.shape == r.shape
+        assert _rel(g, r) < FP64_REL
+    # the second run continues the stream: it equals the jobs run after a copy of themselves
+    got2 = [d.cpu().numpy() for d in b.run()]
+    refs2 = O.run_batch([(L, T, c, _pw(L, ef)) for L, T, c, ef in _JOBS] * 2, "RANLXS2", 99, field, 0.3)
+    for g, r in zip(got2, refs2[len(_JOBS):]):
+        assert _rel(g, r) < FP64_REL
+    b.close()
+
+
+@pytest.mark.gpu
+def test_device_batch_uneven_shapes_fp32_vs_fp64():
+    """Uneven shapes (L in 16, 24, 32; N in 7, 19, 33; T in 8, 16): FP32
+    orbitals against the FP64 batch on the same stream, 1e-5 relative."""
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    shell = {7: 1.5, 19: 2.5, 33: 4.5}  # E_F between closed shells, units of (2 pi / L)^2 / 2
+    spec = [(16, 8, 7), (24, 16, 19), (32, 8, 33), (16, 16, 19), (32, 16, 7)]
+    jobs = [nb.BatchJob(L=L, T=T, n_conf=2, fermi_energy=0.5 * (2 * np.pi / L) ** 2 * shell[N]) for L, T, N in spec]
+    out = {}
+    for prec in ("f32", "f64"):
+        b = nb.Batch(jobs, seed=99, field="GAUSS", a=0.3, precision=prec, qr_period=8 if prec == "f32" else 0,
+                     ctx=ctx)
+        out[prec] = [(np.abs(d.cpu().numpy()) ** 2).mean(0) for d in b.run()]
+        b.close()
+    for a, r in zip(out["f32"], out["f64"]):
+        assert _rel(a, r) < 1e-5

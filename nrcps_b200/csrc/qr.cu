@@ -117,7 +117,11 @@ __global__ void __launch_bounds__(256) gram_tile_kernel(const void* __restrict__
 // Per configuration: Cholesky G = R^H R (R upper), Rinv = R^{-1}, and
 // logR[c][i] += log R_ii.  One thread per configuration; G is overwritten
 // with Rinv.  A non-positive pivot marks the configuration with NaN in logR.
-__global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double* __restrict__ logR) {
+// f32_apply: the orbitals are FP32 and Rinv will be applied rounded to FP32;
+// the leading-minor identity det S_n(Psi) = det S_n(Psi Rinv) / prod_{i<n}
+// Rinv_ii then holds for the ROUNDED diagonal, so logR accumulates
+// -log(float(Rinv_ii)) instead of log R_ii.
+__global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double* __restrict__ logR, int f32_apply) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nconf; c += gridDim.x * blockDim.x) {
     double* g = G + 2L * c * N * N;
     auto re = [&](int i, int j) -> double& { return g[2 * (i * N + j)]; };
@@ -150,7 +154,8 @@ __global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double
       for (int i = 0; i < N; ++i) logR[(long)c * N + i] = nan("");
       continue;
     }
-    for (int i = 0; i < N; ++i) logR[(long)c * N + i] += log(re(i, i));
+    if (!f32_apply)
+      for (int i = 0; i < N; ++i) logR[(long)c * N + i] += log(re(i, i));
     // Rinv (upper triangular) by back substitution, column by column, into
     // the lower-left (unused) storage is not possible for complex R; invert
     // in place row by row from the bottom: Rinv_ii = 1/R_ii,
@@ -169,25 +174,29 @@ __global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double
       }
       re(i, i) = 1.0 / rii;
     }
+    if (f32_apply)
+      for (int i = 0; i < N; ++i) logR[(long)c * N + i] -= log((double)(float)re(i, i));
   }
 }
 
 // psi_{c,t}(p) <- sum_{i <= t} psi_{c,i}(p) Rinv[i][t]; one thread per site,
-// all N orbitals of a configuration in registers (N <= 64).
+// all N orbitals of a configuration in registers (N <= 64), arithmetic in R
+// (FP32 orbitals: Rinv rounded to FP32, see chol_inv_kernel).
 template <typename R, int NMAX>
 __global__ void __launch_bounds__(128) apply_rinv_kernel(void* __restrict__ psi, int N, long vol, int nconf,
                                                           const double* __restrict__ Rinv) {
-  extern __shared__ double rs[];  // 2 N^2 doubles of this block's configuration
+  extern __shared__ double rs_raw[];  // 2 N^2 values of R of this block's configuration
+  R* rs = reinterpret_cast<R*>(rs_raw);
   const long sites_per_block = blockDim.x;
   const long blocks_per_conf = (vol + sites_per_block - 1) / sites_per_block;
   const long c = blockIdx.x / blocks_per_conf;
   if (c >= nconf) return;
   const long p = (blockIdx.x % blocks_per_conf) * sites_per_block + threadIdx.x;
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) rs[e] = Rinv[2L * c * N * N + e];
+  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) rs[e] = (R)Rinv[2L * c * N * N + e];
   __syncthreads();
   if (p >= vol) return;
   cplx<R>* base = reinterpret_cast<cplx<R>*>(psi) + (size_t)c * N * vol + p;
-  double xr[NMAX], xi[NMAX];
+  R xr[NMAX], xi[NMAX];
 #pragma unroll
   for (int i = 0; i < NMAX; ++i)
     if (i < N) {
@@ -198,10 +207,10 @@ __global__ void __launch_bounds__(128) apply_rinv_kernel(void* __restrict__ psi,
 #pragma unroll
   for (int t = NMAX - 1; t >= 0; --t) {
     if (t >= N) continue;
-    double sr = 0, si = 0;
+    R sr = 0, si = 0;
 #pragma unroll
     for (int i = 0; i <= t; ++i) {
-      const double ar = rs[2 * (i * N + t)], ai = rs[2 * (i * N + t) + 1];
+      const R ar = rs[2 * (i * N + t)], ai = rs[2 * (i * N + t) + 1];
       sr += xr[i] * ar - xi[i] * ai;
       si += xr[i] * ai + xi[i] * ar;
     }
@@ -266,7 +275,7 @@ nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol,
     ctx->launches++;
     NRCPS_TRY(check_launch(ctx, "gram_tile_kernel"));
   }
-  chol_inv_kernel<<<grid_for(nconf, 64), 64, 0, ctx->stream>>>(G, N, nconf, logR);
+  chol_inv_kernel<<<grid_for(nconf, 64), 64, 0, ctx->stream>>>(G, N, nconf, logR, prec == NRCPS_F32);
   ctx->launches++;
   NRCPS_TRY(check_launch(ctx, "chol_inv_kernel"));
   if (N <= 8) return launch_apply<8>(ctx, psi, N, vol, nconf, prec, G);

@@ -365,6 +365,40 @@ nrcps_status nrcps_batch_layout(const nrcps_batch *batch, int job, long *offset,
 nrcps_status nrcps_batch_run(nrcps_batch *batch, double *dev_out);
 nrcps_status nrcps_batch_destroy(nrcps_batch *batch);
 
+/* ------------------------------------------- learned control variate
+ * Kernels of the control-variate network (no counterpart in the reference;
+ * nrcps_b200/cv.py drives them): a 3-layer 3x3x3 periodic convolution net
+ * over block means of the field slices, BF16 conv weights and activations,
+ * FP32 accumulation, an MLP head predicting log C(tau).  Tensors are per
+ * sample contiguous (act[b][c][s], s = z + G (y + G x)). */
+/* x[b][t][q] = mean of phi = +-1 over the (L/G)^3 sites of cell q of slice t
+ * of configuration b (BF16); bit bit0 + (b T + t) L^3 + site of dev_bits is
+ * phi = +1. */
+nrcps_status nrcps_cv_coarse_z2(nrcps_context *ctx, const uint32_t *dev_bits, uint64_t bit0, int L, int T, int G,
+                                int B, void *dev_x);
+/* Z = conv(in) + bias (FP32), A = tanh(Z) (BF16); Cout = 16; W BF16 [Cout][Cin][27]. */
+nrcps_status nrcps_cv_conv_forward(nrcps_context *ctx, const void *dev_in, int Cin, int Cout, int G, int B,
+                                   const void *dev_W, const float *dev_bias, float *dev_Z, void *dev_A);
+/* dW, db from dZ and the layer input; with dev_dZin (Cin = 16) also the data
+ * gradient times tanh' of the input activations dev_Ain. */
+nrcps_status nrcps_cv_conv_backward(nrcps_context *ctx, const float *dev_dZ, const void *dev_in, const void *dev_Ain,
+                                    int Cin, int Cout, int G, int B, const void *dev_W, float *dev_dW, float *dev_db,
+                                    float *dev_dZin);
+/* pool (mean over sites) + tanh hidden layer (H) + linear output (T). */
+nrcps_status nrcps_cv_head_forward(nrcps_context *ctx, const void *dev_A3, int C, int G, int B, const float *W1,
+                                   const float *b1, int H, const float *W2, const float *b2, int T, float *P,
+                                   float *Hact, float *Y);
+/* loss 0.5 mean (Y - target)^2 (per-sample sums in loss_parts), head weight
+ * gradients and dZ3 of the last conv layer. */
+nrcps_status nrcps_cv_head_backward(nrcps_context *ctx, const float *Y, const float *target, int T, int B,
+                                    const float *Hact, int H, const float *W2, const float *W1, int C,
+                                    const void *dev_A3, int G, const float *P, float *dY, float *dZh, float *dZ3,
+                                    float *loss_parts, float *dW2, float *db2, float *dW1, float *db1);
+/* Adam on FP32 master weights (bias-corrected, step >= 1); bf16_copy (may be
+ * NULL) receives the updated weights in BF16. */
+nrcps_status nrcps_cv_adam(nrcps_context *ctx, float *w, const float *g, float *m, float *v, long n, float lr,
+                           float beta1, float beta2, float eps, int step, void *bf16_copy);
+
 /* ---------------------------------------------------------- estimators
  * Block accumulators of the production drivers in FP64, configurations added
  * in index order: dev_dets = n_conf x T x nmeas complex (nrcps_ensemble_run

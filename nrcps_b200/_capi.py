@@ -110,6 +110,14 @@ SIGNATURES = {
     "nrcps_batch_layout": ([_P, _I, _LP, _LP], _I),
     "nrcps_batch_run": ([_P, _P], _I),
     "nrcps_batch_destroy": ([_P], _I),
+    "nrcps_cv_coarse_z2": ([_P, _P, _U64, _I, _I, _I, _I, _P], _I),
+    "nrcps_cv_conv_forward": ([_P, _P, _I, _I, _I, _I, _P, _P, _P, _P], _I),
+    "nrcps_cv_conv_backward": ([_P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P], _I),
+    "nrcps_cv_head_forward": ([_P, _P, _I, _I, _I, _P, _P, _I, _P, _P, _I, _P, _P, _P], _I),
+    "nrcps_cv_head_backward": ([_P, _P, _P, _I, _I, _P, _I, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P,
+                                _P], _I),
+    "nrcps_cv_adam": ([_P, _P, _P, _P, _P, _L, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _I,
+                       _P], _I),
     "nrcps_jackknife": ([_P, _P, _L, _I, _I, _P, _P, _P, _P], _I),
 }
 

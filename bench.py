@@ -54,8 +54,13 @@ def parse():
     ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 peer access, 1 split, 2 bulk staged, 3 bulk L2, 4-6 packed 0/2/3")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU path measurement")
     ap.add_argument("--qr", type=int, default=-1, help="re-orthonormalise every k slices (-1: 8 for f32, 0 for f64)")
-    ap.add_argument("--workload", default="batched", choices=["batched", "uneven"],
-                    help="batched: the L=32 ensemble (default); uneven: 512 jobs of random (L, N, T) in one launch")
+    ap.add_argument("--workload", default="batched", choices=["batched", "uneven", "cv"],
+                    help="batched: the L=32 ensemble (default); uneven: 512 jobs of random (L, N, T) in one launch; "
+                         "cv: the learned control variate against the plain estimator")
+    ap.add_argument("--cv-train", type=int, default=65536, help="cv: training pairs (seeds 1000.. in blocks of 1024)")
+    ap.add_argument("--cv-eval", type=int, default=8192, help="cv: evaluation configurations")
+    ap.add_argument("--cv-extra", type=int, default=1 << 20, help="cv: extra field draws for <g>")
+    ap.add_argument("--cv-epochs", type=int, default=6)
     ap.add_argument("--jobs", type=int, default=512, help="jobs of the uneven workload")
     ap.add_argument("--precision-configs", type=int, default=64,
                     help="configurations of the FP32-vs-FP64 precision report (0: skip)")
@@ -489,12 +494,90 @@ def run_uneven(a):
     return 0
 
 
+# ------------------------------------------------------- control variate
+def run_cv(a):
+    """The learned control variate at the batched shape (L=32, T=64, N=19,
+    Z2 a=0.5): training pairs from seeds 1000.. (1024 configurations per
+    seed), a calibration block for c(tau), an evaluation block from a fresh
+    seed, <g> from extra field draws; statistical error of <C_N(tau)> per
+    GPU-second for the plain and the control-variate estimators."""
+    import math
+    import time as _t
+    import torch
+    import nrcps_b200 as nb
+    from nrcps_b200 import cv
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    ctx = nb.Context(0)
+    L, T, ef, G = a.L, a.T, a.ef, 8
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = _t.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, _t.perf_counter() - t0
+
+    # training pairs: 1024 configurations per seed, seeds 1000, 1001, ...
+    Xs, Cs, t_gen = [], [], 0.0
+    for i in range(0, a.cv_train, 1024):
+        (X, C), el = timed(lambda: cv.generate_pairs(L, T, ef, 1000 + i // 1024, min(1024, a.cv_train - i),
+                                                     chunk=1024, G=G, precision=a.precision,
+                                                     qr_period=qr_period(a), ctx=ctx))
+        Xs.append(X)
+        Cs.append(C)
+        t_gen += el
+    X, C = torch.cat(Xs), torch.cat(Cs)
+    n_cal = max(1024, X.shape[0] // 8)
+    net = cv.ControlVariateNet(cv.NetShape(T=T, G=G), seed=0, ctx=ctx)
+    losses, t_train = timed(lambda: net.fit(X[:-n_cal], torch.log(C[:-n_cal]), epochs=a.cv_epochs, batch=256,
+                                            lr=2e-3))
+    c = cv.cv_coefficient(C[-n_cal:].cpu(), torch.exp(net.predict_logC(X[-n_cal:])))
+    del X, Xs
+    # evaluation block: a seed never used for training
+    (Xe, Ce), t_eval = timed(lambda: cv.generate_pairs(L, T, ef, 2000, a.cv_eval, chunk=1024, G=G,
+                                                       precision=a.precision, qr_period=qr_period(a), ctx=ctx))
+    ge, t_inf = timed(lambda: torch.exp(net.predict_logC(Xe)))
+    gm, gm_err, t_extra = cv.extra_fields_mean_g(net, L, 3000, 0, a.cv_extra, chunk=8192, ctx=ctx)
+    Ce = Ce.cpu()
+    plain, plain_err, est, est_err = cv.estimators(Ce, ge, c, gm, gm_err)
+    var_ratio = (Ce - c * ge).var(0) / Ce.var(0)
+    t_plain = t_eval                           # propagation + measurement of the evaluation block
+    t_cv = t_eval + t_inf + t_extra            # + inference on it + the extra draws for <g>
+    tau = T // 2
+    rel_plain = float(plain_err[tau] / plain[tau])
+    rel_cv = float(est_err[tau] / est[tau])
+    z = ((est - plain).abs() / (plain_err ** 2 + est_err ** 2).sqrt())[1:]
+    line = {"metric": "statistical error of <C_N(tau)> per GPU-second (control variate vs plain)",
+            "value": rel_cv * math.sqrt(t_cv), "unit": "relative error x sqrt(GPU s)", "higher_is_better": False,
+            "n_gpus": 1, "dtype": a.precision, "data": "synthetic (device-drawn fields)",
+            "config": {"workload": f"L={L}^3 T={T} N={len(nb.momenta((L,) * 3, 'PERFECT', 1.0, ef, 2.0)[0])} "
+                                   f"Z2 a=0.5; train {a.cv_train} pairs "
+                                   f"(seeds 1000..), eval {a.cv_eval} configs (seed 2000), <g> from {a.cv_extra} "
+                                   f"extra fields (seed 3000), net 3x conv3d(16, k3) on {G}^3 block means + MLP",
+                       "tau": tau},
+            "plain": {"rel_err": rel_plain, "gpu_seconds": t_plain, "rel_err_per_gpu_second": rel_plain *
+                      math.sqrt(t_plain)},
+            "control_variate": {"rel_err": rel_cv, "gpu_seconds": t_cv, "rel_err_per_gpu_second": rel_cv *
+                                math.sqrt(t_cv)},
+            "variance_ratio_median_over_tau": float(var_ratio[1:].median()),
+            "variance_ratio_tau_mid": float(var_ratio[tau]),
+            "unbiasedness_max_z_over_tau": float(z.max()),
+            "training": {"pairs": int(C.shape[0]), "epochs": a.cv_epochs, "loss_first": losses[0],
+                         "loss_last": losses[-1], "generation_s": t_gen, "training_s": t_train},
+            "extra_fields": {"count": a.cv_extra, "gpu_seconds": t_extra}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
     if a.workload == "uneven":
         return run_uneven(a)
+    if a.workload == "cv":
+        return run_cv(a)
     return run_b200(a)
 
 

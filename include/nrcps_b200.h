@@ -365,6 +365,37 @@ nrcps_status nrcps_batch_layout(const nrcps_batch *batch, int job, long *offset,
 nrcps_status nrcps_batch_run(nrcps_batch *batch, double *dev_out);
 nrcps_status nrcps_batch_destroy(nrcps_batch *batch);
 
+/* ----------------------------------------------------------- branching
+ * The multilevel branching driver (production/two_body-branched/main.C:23-80,
+ * MultiLevel): trees of `levels` levels, `branches` children per node and
+ * `steps` slices per level (T = levels * steps); prop1 / prop2 start from
+ * sources2 (2 x V complex, host), every node restarts its children from its
+ * end state, and corr[t] accumulates TwoBody::Run(prop1, prop2) /
+ * branches^(d+1) over the nodes of depth d = t / steps.  Hamiltonians
+ * [K, (V), I, (V), K] with the local interaction (1 + a phi)/V (the driver's
+ * Interaction3 is not in the reference's headers); fields are the slices the
+ * reference's depth-first walk draws from one stream. */
+typedef struct {
+  int dims[3];
+  int levels;
+  int branches;
+  int steps;
+  int rng_kind;
+  long seed;
+  int field_kind;
+  int precision;
+  double a;
+} nrcps_branch_params;
+typedef struct nrcps_branch nrcps_branch;
+/* kin_xi: V xi values; pot: V potential values or NULL; w / opposite: the
+ * TwoBody tables (nrcps_two_body_tables). */
+nrcps_status nrcps_branch_create(nrcps_context *ctx, const nrcps_branch_params *params, const double *kin_xi,
+                                 const double *pot, const double *sources2, const double *w, const int *opposite,
+                                 nrcps_branch **branch);
+/* The next tree; dev_corr (T complex doubles, device) accumulates its sums. */
+nrcps_status nrcps_branch_run(nrcps_branch *branch, double *dev_corr);
+nrcps_status nrcps_branch_destroy(nrcps_branch *branch);
+
 /* ------------------------------------------- learned control variate
  * Kernels of the control-variate network (no counterpart in the reference;
  * nrcps_b200/cv.py drives them): a 3-layer 3x3x3 periodic convolution net

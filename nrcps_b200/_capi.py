@@ -52,6 +52,12 @@ class BatchJob(ctypes.Structure):
                 ("pw_index", ctypes.POINTER(ctypes.c_int)), ("kin_xi", ctypes.POINTER(ctypes.c_double))]
 
 
+class BranchParams(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int * 3), ("levels", ctypes.c_int), ("branches", ctypes.c_int),
+                ("steps", ctypes.c_int), ("rng_kind", ctypes.c_int), ("seed", ctypes.c_long),
+                ("field_kind", ctypes.c_int), ("precision", ctypes.c_int), ("a", ctypes.c_double)]
+
+
 class BatchParams(ctypes.Structure):
     _fields_ = [("rng_kind", ctypes.c_int), ("seed", ctypes.c_long), ("field_kind", ctypes.c_int),
                 ("precision", ctypes.c_int), ("a", ctypes.c_double), ("qr_period", ctypes.c_int)]
@@ -110,6 +116,9 @@ SIGNATURES = {
     "nrcps_batch_layout": ([_P, _I, _LP, _LP], _I),
     "nrcps_batch_run": ([_P, _P], _I),
     "nrcps_batch_destroy": ([_P], _I),
+    "nrcps_branch_create": ([_P, _P, _P, _P, _P, _P, _P, ctypes.POINTER(_P)], _I),
+    "nrcps_branch_run": ([_P, _P], _I),
+    "nrcps_branch_destroy": ([_P], _I),
     "nrcps_cv_coarse_z2": ([_P, _P, _U64, _I, _I, _I, _I, _P], _I),
     "nrcps_cv_conv_forward": ([_P, _P, _I, _I, _I, _I, _P, _P, _P, _P], _I),
     "nrcps_cv_conv_backward": ([_P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P], _I),

@@ -571,6 +571,54 @@ class EnsembleJob:
         return (self.L, self.L, self.L)
 
 
+class Branching:
+    """The multilevel branching driver (production/two_body-branched/main.C:23-80)
+    on the device: run() walks one tree and returns its corr[t] contributions."""
+
+    def __init__(self, L: int, levels: int, branches: int, steps: int, sources2: np.ndarray, rng: str = "RANLXS2",
+                 seed: int = 1234, field: str = "ZTWO", a: float = 0.5, precision: str = "f64",
+                 wavefunc: str = "TGND", wf_disp: str = "STANDARD", wf_mass: float = 1.0,
+                 wf_lambda: float = 0.176776695, kin_dt: float = 0.5, cutoff: float = 2.0,
+                 potential: Optional[np.ndarray] = None, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        dims = (L, L, L)
+        self.T = levels * steps
+        p = C.BranchParams()
+        p.dims[:] = dims
+        p.levels, p.branches, p.steps = levels, branches, steps
+        p.rng_kind, p.seed, p.field_kind = C.RNG_KINDS[rng], seed, C.FIELD_KINDS[field]
+        p.precision, p.a = _prec(precision), a
+        xi = np.ascontiguousarray(kinetic_table(dims, "PERFECT", 1.0, kin_dt, cutoff))
+        w, opp = two_body_tables(dims, wavefunc, wf_disp, wf_mass, wf_lambda, cutoff)
+        src = np.ascontiguousarray(np.asarray(sources2, dtype=np.complex128).reshape(2, -1))
+        pot = None if potential is None else np.ascontiguousarray(potential, dtype=np.float64)
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().nrcps_branch_create(
+            self.ctx.handle, ctypes.byref(p), xi.ctypes.data_as(ctypes.c_void_p),
+            pot.ctypes.data_as(ctypes.c_void_p) if pot is not None else None,
+            src.view(np.float64).ctypes.data_as(ctypes.c_void_p),
+            np.ascontiguousarray(w, dtype=np.float64).ctypes.data_as(ctypes.c_void_p),
+            np.ascontiguousarray(opp, dtype=np.int32).ctypes.data_as(ctypes.c_void_p), ctypes.byref(h)),
+            "branch_create")
+        self.handle = h
+
+    def run(self) -> torch.Tensor:
+        corr = torch.zeros(self.T, dtype=torch.complex128, device=self.ctx.device)
+        self.ctx.check(lib().nrcps_branch_run(self.handle, _ptr(corr)), "branch_run")
+        return corr
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().nrcps_branch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 @dataclass
 class BatchJob:
     """One job of a Batch: an L^3 lattice, T slices, n_conf configurations,

@@ -822,3 +822,79 @@ void o_run_batch(int njobs, const int *L, const int *T, const int *nconf, const 
     free(S);
   }
 }
+
+/* ---------------------------------------------- multilevel branching */
+typedef struct {
+  const int *dims;
+  long vol;
+  int levels, branches, steps;
+  o_rng *rng;
+  int field_type;
+  double a;
+  const double *xi, *wf;
+  const int *opp;
+  double *lat, *fld, *corr;
+} o_branch_ctx;
+
+/* MultiLevel (production/two_body-branched/main.C:23-80) */
+static void o_multilevel(o_branch_ctx *b, int level, double *p1, double *p2) {
+  if (level <= 0) return;
+  const long vol = b->vol;
+  const int T = b->levels * b->steps;
+  double *s1 = (double *)malloc(sizeof(double) * 2 * vol);
+  double *s2 = (double *)malloc(sizeof(double) * 2 * vol);
+  memcpy(s1, p1, sizeof(double) * 2 * vol);
+  memcpy(s2, p2, sizeof(double) * 2 * vol);
+  const double norm = pow((double)b->branches, (double)(b->levels - level + 1));
+  for (int i = 0; i < b->branches; ++i) {
+    memcpy(p1, s1, sizeof(double) * 2 * vol);
+    memcpy(p2, s2, sizeof(double) * 2 * vol);
+    for (int s = 0; s < b->steps; ++s) {
+      const int t = T - (level - 1) * b->steps - (b->steps - s);
+      double phi[2];
+      o_pair_matrix(vol, 1, p1, p2, b->wf, b->opp, phi);
+      b->corr[2 * t] += phi[0] / norm;
+      b->corr[2 * t + 1] += phi[1] / norm;
+      for (long x = 0; x < vol; ++x) {
+        b->fld[2 * x] = (1.0 + b->a * b->lat[2 * x]) / (double)vol;
+        b->fld[2 * x + 1] = (b->a * b->lat[2 * x + 1]) / (double)vol;
+      }
+      o_kinetic_evolve(vol, 1, p1, b->xi);
+      o_interaction_evolve(b->dims, 1, p1, b->fld);
+      o_kinetic_evolve(vol, 1, p1, b->xi);
+      o_kinetic_evolve(vol, 1, p2, b->xi);
+      o_interaction_evolve(b->dims, 1, p2, b->fld);
+      o_kinetic_evolve(vol, 1, p2, b->xi);
+      o_field_slices(b->rng, b->field_type, vol, 1, b->lat); /* lattice->Refresh() */
+    }
+    o_multilevel(b, level - 1, p1, p2);
+  }
+  free(s1);
+  free(s2);
+}
+
+void o_run_branching(const int dims[3], int levels, int branches, int steps, int trees, int rng_kind, long seed,
+                     int field_type, double a, double kin_dt, double cutoff_sq, const double *sources2,
+                     const double *wf, const int *opp, double *corr) {
+  const long vol = (long)dims[0] * dims[1] * dims[2];
+  o_rng rng;
+  o_rng_init(&rng, rng_kind, seed);
+  double *xi = (double *)malloc(sizeof(double) * vol);
+  double *lat = (double *)malloc(sizeof(double) * 2 * vol);
+  double *fld = (double *)malloc(sizeof(double) * 2 * vol);
+  double *p1 = (double *)malloc(sizeof(double) * 2 * vol);
+  double *p2 = (double *)malloc(sizeof(double) * 2 * vol);
+  o_kinetic_xi(dims, 2 /* PERFECT */, 1.0, kin_dt, cutoff_sq, xi);
+  o_field_slices(&rng, field_type, vol, 1, lat); /* the Lattice constructor's draw */
+  o_branch_ctx b = {dims, vol, levels, branches, steps, &rng, field_type, a, xi, wf, opp, lat, fld, corr};
+  for (int r = 0; r < trees; ++r) {
+    memcpy(p1, sources2, sizeof(double) * 2 * vol);
+    memcpy(p2, sources2 + 2 * vol, sizeof(double) * 2 * vol);
+    o_multilevel(&b, levels, p1, p2);
+  }
+  free(xi);
+  free(lat);
+  free(fld);
+  free(p1);
+  free(p2);
+}

@@ -134,6 +134,18 @@ int o_run_ensemble(const o_job *job, const double *sources, double *dets);
  * Kinetic xi from (disp PERFECT, mass 1, dt, cutoff_sq); dets_j =
  * [n_conf_j][T_j][N_j] complex.  Slice t of configuration k of job j is the
  * (k T_j + t)-th field drawn after all earlier jobs' fields. */
+/* The multilevel branching driver (production/two_body-branched/main.C:23-80,
+ * MultiLevel) for `trees` trees of depth `levels`, `branches` branches per
+ * node and `steps` steps per level, T = levels * steps: corr[t] (complex,
+ * summed over trees) accumulates TwoBody::Run(prop1, prop2) / branches^(d+1)
+ * over the nodes of depth d = t / steps.  Hamiltonians [K, I, K] with the
+ * local interaction (1 + a phi)/V (the reference driver's Interaction3 and
+ * Propagator::SetSource no longer exist in its headers); fields from one
+ * generator in the recursion's order. */
+void o_run_branching(const int dims[3], int levels, int branches, int steps, int trees, int rng_kind, long seed,
+                     int field_type, double a, double kin_dt, double cutoff_sq, const double *sources2,
+                     const double *wf, const int *opp, double *corr);
+
 void o_run_batch(int njobs, const int *L, const int *T, const int *nconf, const int *N, const int *const *idx,
                  int rng_kind, long seed, int field_type, double a, double kin_dt, double cutoff_sq,
                  double *const *dets);

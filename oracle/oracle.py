@@ -78,6 +78,9 @@ def lib():
         L.o_minor_det.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, dp]
         L.o_fft3d.argtypes = [dp, ip, ctypes.c_int, ctypes.c_int]
         L.o_run_ensemble.argtypes = [ctypes.c_void_p, dp, dp]
+        L.o_run_branching.argtypes = [ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_long, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, dp, dp, ip, dp]
         pp = ctypes.POINTER(ctypes.POINTER(ctypes.c_int))
         L.o_run_batch.argtypes = [ctypes.c_int, ip, ip, ip, ip, pp, ctypes.c_int, ctypes.c_long, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -300,6 +303,23 @@ def minor_det(S: np.ndarray, n: int, t0: int = -1, psi1=None, log: bool = False)
     out = np.zeros(2)
     lib().o_minor_det(_dp(S.view(np.float64)), N, n, t0, _dp(p1.view(np.float64)), int(log), _dp(out))
     return complex(out[0], out[1])
+
+
+# ------------------------------------------------------------- branching
+def run_branching(L: int, levels: int, branches: int, steps: int, trees: int, rng: str, seed: int, field: str,
+                  a: float, sources2: np.ndarray, wf: np.ndarray, opp: np.ndarray, kin_dt: float = 0.5,
+                  cutoff: float = 2.0) -> np.ndarray:
+    """MultiLevel trees (o_run_branching): corr [levels * steps] complex, summed over trees."""
+    dims = np.array([L, L, L], dtype=np.int32)
+    src = np.ascontiguousarray(sources2, dtype=np.complex128).reshape(2, -1)
+    corr = np.zeros(levels * steps, dtype=np.complex128)
+    c = cutoff * PI
+    lib().o_run_branching(dims.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), levels, branches, steps, trees,
+                          RNG_KINDS[rng], seed, FIELD_TYPES[field], a, kin_dt, c * c, _dp(src.view(np.float64)),
+                          _dp(np.ascontiguousarray(wf, dtype=np.float64)),
+                          np.ascontiguousarray(opp, dtype=np.int32).ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                          _dp(corr.view(np.float64)))
+    return corr
 
 
 # ----------------------------------------------------------------- batch

@@ -247,6 +247,16 @@ nrcps_status nrcps_overlap_planewave(nrcps_context *ctx, const int *dev_index, i
 nrcps_status nrcps_pair_matrix(nrcps_context *ctx, const void *dev_psi1, const void *dev_psi2, int n,
                                int nconf, long vol, const double *dev_w, const int *dev_opposite,
                                nrcps_precision prec, double *dev_phi);
+/* GeneralizedTwoBody::Run(prop1, prop2, R) (src/two_body/noarch/two_body_run.C:45-75),
+ * the Oh-projected pair contraction, for every orbital pair of nconf
+ * configurations: phi[c][s][t] = sum_l sum_i wl[l][i] psi1_{c,s}(shift[l][i])
+ * psi2_{c,t}(opposite(i)), l < nterms (the subshell vectors of OhGroup);
+ * the caller folds wl[l][i] = OhGroup::GetWeight(R, l) * half_site_wavefunc[l][i]
+ * and passes shift_indices (nterms x V) as GeneralizedTwoBody builds them
+ * (src/two_body/two_body.C:226-284). */
+nrcps_status nrcps_shifted_pair_matrix(nrcps_context *ctx, const void *dev_psi1, const void *dev_psi2, int n,
+                                       int nconf, long vol, int nterms, const int *dev_shift, const double *dev_wl,
+                                       const int *dev_opposite, nrcps_precision prec, double *dev_phi);
 /* Cuda::InnerProduct (src/utils/cuda/cuda_utils.cu:88-127) as the
  * reference's GPU build calls it: kets and bras are device arrays of nf
  * device pointers to V complex FP64 vectors; dev_mat[t + nf*s] =

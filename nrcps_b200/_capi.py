@@ -116,6 +116,7 @@ SIGNATURES = {
     "nrcps_batch_layout": ([_P, _I, _LP, _LP], _I),
     "nrcps_batch_run": ([_P, _P], _I),
     "nrcps_batch_destroy": ([_P], _I),
+    "nrcps_shifted_pair_matrix": ([_P, _P, _P, _I, _I, _L, _I, _P, _P, _P, _I, _P], _I),
     "nrcps_branch_create": ([_P, _P, _P, _P, _P, _P, _P, ctypes.POINTER(_P)], _I),
     "nrcps_branch_run": ([_P, _P], _I),
     "nrcps_branch_destroy": ([_P], _I),

@@ -571,6 +571,44 @@ class EnsembleJob:
         return (self.L, self.L, self.L)
 
 
+class GeneralizedTwoBody:
+    """GeneralizedTwoBody::Run (src/two_body/noarch/two_body_run.C:45-75) on the
+    device.  The tables are the reference class's own (built on the host by
+    its OhGroup, src/two_body/two_body.C:209-288): shift [nterms, V],
+    half_site_wavefunc [nterms, V], opposite [V], weights [nterms, 10]
+    (OhGroup::GetWeight(R, l))."""
+
+    def __init__(self, shift, half_site_wavefunc, opposite, weights, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        dev = self.ctx.device
+        self.shift = torch.as_tensor(np.ascontiguousarray(shift, dtype=np.int32), device=dev)
+        self.hsw = torch.as_tensor(np.ascontiguousarray(half_site_wavefunc, dtype=np.float64), device=dev)
+        self.opp = torch.as_tensor(np.ascontiguousarray(opposite, dtype=np.int32), device=dev)
+        self.weights = np.asarray(weights, dtype=np.float64)
+        self._wl = {}
+
+    def _folded(self, rep: int) -> torch.Tensor:
+        if rep not in self._wl:
+            w = torch.as_tensor(self.weights[:, rep], device=self.ctx.device)
+            self._wl[rep] = (self.hsw * w[:, None]).contiguous()
+        return self._wl[rep]
+
+    def run_matrix(self, props1: torch.Tensor, props2: torch.Tensor, rep: int) -> torch.Tensor:
+        """phi[c][s][t] for props [nconf, n, V] (or [n, V]) in representation rep (0 = A1g)."""
+        p1 = props1.reshape(-1, props1.shape[-2] if props1.dim() >= 2 else 1, props1.shape[-1]).contiguous()
+        p2 = props2.reshape(p1.shape).contiguous()
+        nconf, n, vol = p1.shape
+        phi = torch.empty((nconf, n, n), dtype=torch.complex128, device=self.ctx.device)
+        prec = C.F64 if p1.dtype == torch.complex128 else C.F32
+        self.ctx.check(lib().nrcps_shifted_pair_matrix(self.ctx.handle, _ptr(p1), _ptr(p2), n, nconf, vol,
+                                                       self.shift.shape[0], _ptr(self.shift), _ptr(self._folded(rep)),
+                                                       _ptr(self.opp), prec, _ptr(phi)), "shifted_pair_matrix")
+        return phi
+
+    def run(self, prop1: torch.Tensor, prop2: torch.Tensor, rep: int) -> complex:
+        return complex(self.run_matrix(prop1.reshape(1, 1, -1), prop2.reshape(1, 1, -1), rep).cpu().item())
+
+
 class Branching:
     """The multilevel branching driver (production/two_body-branched/main.C:23-80)
     on the device: run() walks one tree and returns its corr[t] contributions."""

@@ -118,6 +118,54 @@ __global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1
   }
 }
 
+// GeneralizedTwoBody::Run (src/two_body/noarch/two_body_run.C:45-75) batched:
+// phi[c][s][t] = sum_l sum_i wl[l][i] psi1_{c,s}(shift[l][i]) psi2_{c,t}(opp(i))
+// with wl[l][i] = weight(R, l) * half_site_wavefunc[l][i] folded by the
+// caller.  One block per (conf, s, t); the term loop is outermost, as in the
+// reference.
+template <typename R>
+__global__ void __launch_bounds__(256) shifted_pair_kernel(const void* __restrict__ psi1,
+                                                           const void* __restrict__ psi2, int n, long vol, int nterms,
+                                                           const int* __restrict__ shift,
+                                                           const double* __restrict__ wl,
+                                                           const int* __restrict__ opp, double* __restrict__ phi) {
+  const long e = blockIdx.x;  // (conf * n + s) * n + t
+  const long conf = e / ((long)n * n);
+  const int s = (int)((e / n) % n), t = (int)(e % n);
+  const char* a = reinterpret_cast<const char*>(psi1) + (size_t)(conf * n + s) * vol * 2 * sizeof(R);
+  const char* b = reinterpret_cast<const char*>(psi2) + (size_t)(conf * n + t) * vol * 2 * sizeof(R);
+  double re = 0.0, im = 0.0;
+  for (int l = 0; l < nterms; ++l) {
+    const int* sh = shift + (size_t)l * vol;
+    const double* w = wl + (size_t)l * vol;
+    for (long i = threadIdx.x; i < vol; i += blockDim.x) {
+      cplx<R> x = ld<R>(a, sh[i]), y = ld<R>(b, opp[i]);
+      const double wi = w[i];
+      re += ((double)x.re * y.re - (double)x.im * y.im) * wi;
+      im += ((double)x.re * y.im + (double)x.im * y.re) * wi;
+    }
+  }
+  __shared__ double red[2][8];
+  for (int off = 16; off > 0; off >>= 1) {
+    re += __shfl_down_sync(0xffffffffu, re, off);
+    im += __shfl_down_sync(0xffffffffu, im, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = re;
+    red[1][threadIdx.x >> 5] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sr = 0, si = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      sr += red[0][k];
+      si += red[1][k];
+    }
+    phi[2 * e] = sr;
+    phi[2 * e + 1] = si;
+  }
+}
+
 // ------------------------------------------------- pointer-array variants
 // mat[t + nf*s] = <kets[s] | bras[t]> (the layout of Cuda::InnerProduct,
 // src/utils/cuda/cuda_utils_kernels.cu:4-48), FP64, one block per (s, t).
@@ -554,6 +602,26 @@ extern "C" nrcps_status nrcps_pair_matrix(nrcps_context* ctx, const void* dev_ps
   NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_w && dev_opposite && dev_phi && n >= 0 && nconf >= 0 && vol > 0,
                 "nrcps_pair_matrix: bad arguments");
   return pair_impl(ctx, dev_psi1, dev_psi2, n, nconf, vol, dev_w, dev_opposite, prec, dev_phi);
+}
+
+extern "C" nrcps_status nrcps_shifted_pair_matrix(nrcps_context* ctx, const void* dev_psi1, const void* dev_psi2,
+                                                  int n, int nconf, long vol, int nterms, const int* dev_shift,
+                                                  const double* dev_wl, const int* dev_opposite,
+                                                  nrcps_precision prec, double* dev_phi) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_shift && dev_wl && dev_opposite && dev_phi && n >= 0 &&
+                         nconf >= 0 && vol > 0 && nterms > 0,
+                "nrcps_shifted_pair_matrix: bad arguments");
+  const long blocks = (long)nconf * n * n;
+  if (blocks == 0) return NRCPS_OK;
+  if (prec == NRCPS_F64)
+    shifted_pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(dev_psi1, dev_psi2, n, vol, nterms,
+                                                                          dev_shift, dev_wl, dev_opposite, dev_phi);
+  else
+    shifted_pair_kernel<float><<<(unsigned)blocks, 256, 0, ctx->stream>>>(dev_psi1, dev_psi2, n, vol, nterms,
+                                                                         dev_shift, dev_wl, dev_opposite, dev_phi);
+  ctx->launches++;
+  return check_launch(ctx, "shifted_pair_kernel");
 }
 
 extern "C" nrcps_status nrcps_inner_product_ptrs(nrcps_context* ctx, const double* const* dev_kets,

@@ -305,6 +305,24 @@ def minor_det(S: np.ndarray, n: int, t0: int = -1, psi1=None, log: bool = False)
     return complex(out[0], out[1])
 
 
+# ----------------------------------------------------- generalized pair
+def generalized_pair(p1: np.ndarray, p2: np.ndarray, shift: np.ndarray, hsw: np.ndarray, opp: np.ndarray,
+                     weights_R: np.ndarray) -> complex:
+    """GeneralizedTwoBody::Run(prop1, prop2, R) (src/two_body/noarch/two_body_run.C:45-75):
+    sum over subshell vectors l (outer) and sites i (inner) of
+    weight(R, l) * prop1[shift[l][i]] * prop2[opp[i]] * hsw[l][i], accumulated
+    in that order (pure Python loops: small lattices only)."""
+    re = im = 0.0
+    a, b = np.asarray(p1, dtype=np.complex128), np.asarray(p2, dtype=np.complex128)
+    for l in range(shift.shape[0]):
+        w = float(weights_R[l])
+        for i in range(shift.shape[1]):
+            x, y, h = a[shift[l, i]], b[opp[i]], float(hsw[l, i])
+            re += w * (x.real * y.real - x.imag * y.imag) * h
+            im += w * (x.real * y.imag + x.imag * y.real) * h
+    return complex(re, im)
+
+
 # ------------------------------------------------------------- branching
 def run_branching(L: int, levels: int, branches: int, steps: int, trees: int, rng: str, seed: int, field: str,
                   a: float, sources2: np.ndarray, wf: np.ndarray, opp: np.ndarray, kin_dt: float = 0.5,

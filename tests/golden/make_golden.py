@@ -149,12 +149,57 @@ def sho_coefficients(ref: str) -> dict:
     return out
 
 
+# GeneralizedTwoBody (src/two_body/two_body.C:209-288) cases: L, distinct
+# vector, wave function, lambda, seed of the random propagators
+OHPAIR_CASES = [(8, (1, 0, 0), "TGND", 0.25, 3), (8, (1, 1, 2), "PAIR1", 0.5, 4), (6, (1, 2, 3), "TGND", 0.3, 5),
+                (8, (0, 0, 0), "UNIFORM", 0.1, 6)]
+
+
+def ohpair_cases(tmp: str) -> dict:
+    """Tables, random propagators and Run / Run2 for every OctahedralRep,
+    from the reference's GeneralizedTwoBody (oracle/ref_build/ohpair_dump.cc)."""
+    out = {}
+    for k, (L, vec, wf, lam, seed) in enumerate(OHPAIR_CASES):
+        path = os.path.join(tmp, f"oh{k}.bin")
+        subprocess.run([os.path.join(REPO, "oracle", "_ref", "ohpair_dump"), f"L={L}", "vec=%d,%d,%d" % vec,
+                        f"wf={wf}", f"lambda={lam!r}", f"seed={seed}", f"out={path}"], check=True,
+                       capture_output=True)
+        b = open(path, "rb").read()
+        nt, vol = np.frombuffer(b[:8], np.int32)
+        o = 8
+        take = lambda dt, n: (np.frombuffer(b[o:o + n * np.dtype(dt).itemsize], dt).copy(),  # noqa: E731
+                              o + n * np.dtype(dt).itemsize)
+        opp, o = take(np.int32, vol)
+        shift, o = take(np.int32, nt * vol)
+        hsw, o = take(np.float64, nt * vol)
+        wts, o = take(np.float64, nt * 10)
+        props, o = take(np.float64, 4 * vol)
+        run, o = take(np.float64, 20)
+        run2, o = take(np.float64, 20)
+        out[f"c{k}_L"] = np.int64(L)
+        out[f"c{k}_opp"] = opp
+        out[f"c{k}_shift"] = shift.reshape(nt, vol)
+        out[f"c{k}_hsw"] = hsw.reshape(nt, vol)
+        out[f"c{k}_weights"] = wts.reshape(nt, 10)
+        out[f"c{k}_props"] = props.view(np.complex128).reshape(2, vol)
+        out[f"c{k}_run"] = run.view(np.complex128)
+        out[f"c{k}_run2"] = run2.view(np.complex128)
+    out["cases"] = np.int64(len(OHPAIR_CASES))
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default="", help="regenerate one fixture only (ohpair)")
     a = ap.parse_args()
-    if not os.path.exists(REF_BIN):
+    if not os.path.exists(REF_BIN) or not os.path.exists(os.path.join(REPO, "oracle", "_ref", "ohpair_dump")):
         subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "oracle", "ref_build"), f"REF={a.ref}"])
+    if a.only == "ohpair" or not a.only:
+        with tempfile.TemporaryDirectory() as tmp:
+            np.savez_compressed(os.path.join(HERE, "ohpair.npz"), **ohpair_cases(tmp))
+        if a.only:
+            return
     np.savez_compressed(os.path.join(HERE, "ranlx_kat.npz"), **parse_ranlx_kat(a.ref))
     json.dump(parse_ludcmp_kat(a.ref), open(os.path.join(HERE, "ludcmp_kat.json"), "w"), indent=1)
     sho = sho_coefficients(a.ref)

@@ -24,11 +24,19 @@ namespace nrcps {
 // within a tile and in FP64 across tiles; the four quarters are summed at
 // the end.
 constexpr int GT = 128;
-template <typename R, int MAXB>
+__device__ __forceinline__ void cp_async_elem(void* dst, const void* src, int bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  if (bytes == 16) asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+
+// DB: double-buffered tiles (the next tile's asynchronous copies overlap the
+// current tile's products); else one tile buffer.
+template <typename R, int MAXB, bool DB = false>
 __global__ void __launch_bounds__(256) gram_tile_kernel(const void* __restrict__ psi, int N, long vol,
                                                         double* __restrict__ G) {
   extern __shared__ __align__(16) unsigned char gsm[];
-  cplx<R>* tile = reinterpret_cast<cplx<R>*>(gsm);  // [N][GT + 1]
+  cplx<R>* tiles = reinterpret_cast<cplx<R>*>(gsm);  // [DB ? 2 : 1][N][GT + 1]
   const long c = blockIdx.x;
   const cplx<R>* base = reinterpret_cast<const cplx<R>*>(psi) + (size_t)c * N * vol;
   const int nb = (N + 1) / 2;                // 2-row blocks
@@ -40,14 +48,31 @@ __global__ void __launch_bounds__(256) gram_tile_kernel(const void* __restrict__
   for (int b = 0; b < MAXB; ++b)
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[b][k] = 0.0;
-  for (long p0 = 0; p0 < vol; p0 += GT) {
+  auto fill = [&](long p0, cplx<R>* t) {
     const int ts = (int)((vol - p0) < GT ? (vol - p0) : GT);
-    __syncthreads();
     for (int e = threadIdx.x; e < N * GT; e += blockDim.x) {
       const int i = e / GT, s = e - i * GT;
-      tile[i * (GT + 1) + s] = s < ts ? base[(size_t)i * vol + p0 + s] : cplx<R>{(R)0, (R)0};
+      if (!DB || s >= ts) t[i * (GT + 1) + s] = s < ts ? base[(size_t)i * vol + p0 + s] : cplx<R>{(R)0, (R)0};
+      else cp_async_elem(t + i * (GT + 1) + s, base + (size_t)i * vol + p0 + s, (int)sizeof(cplx<R>));
     }
-    __syncthreads();
+    if (DB) asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  const size_t tsz = (size_t)N * (GT + 1);
+  if (DB) fill(0, tiles);
+  int buf = 0;
+  for (long p0 = 0; p0 < vol; p0 += GT, buf ^= 1) {
+    cplx<R>* tile = tiles + (DB ? buf : 0) * tsz;
+    if (DB) {
+      __syncthreads();  // every thread is done with the tile the next copies overwrite
+      if (p0 + GT < vol) fill(p0 + GT, tiles + (buf ^ 1) * tsz);
+      else asm volatile("cp.async.commit_group;" ::: "memory");
+      asm volatile("cp.async.wait_group 1;" ::: "memory");  // every group but the newest has landed
+      __syncthreads();
+    } else {
+      __syncthreads();
+      fill(p0, tile);
+      __syncthreads();
+    }
 #pragma unroll
     for (int b = 0; b < MAXB; ++b) {
       const int blk = lane64 + 64 * b;
@@ -254,23 +279,24 @@ nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol,
   if (N > 64) return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "QR re-orthonormalisation supports N <= 64");
   {
     const size_t esz = prec == NRCPS_F64 ? sizeof(cplx<double>) : sizeof(cplx<float>);
-    size_t sh = esz * (size_t)N * (GT + 1);
+    const size_t tile_bytes = esz * (size_t)N * (GT + 1);
+    const bool db = 2 * tile_bytes <= 200 * 1024;
+    size_t sh = db ? 2 * tile_bytes : tile_bytes;
     const size_t red = sizeof(double) * 8 * 528;
     if (sh < red) sh = red;
-    // N <= 64 rows of GT + 1 FP64 complex values: up to 132 KB of shared memory
-    const int big = (int)(sizeof(cplx<double>) * 64 * (GT + 1));
     auto launch = [&](auto kern) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       kern<<<(unsigned)nconf, 256, sh, ctx->stream>>>(psi, N, vol, G);
     };
     if (prec == NRCPS_F64) {
-      if (N <= 22) launch(gram_tile_kernel<double, 2>);
-      else if (N <= 32) launch(gram_tile_kernel<double, 3>);
-      else launch(gram_tile_kernel<double, 9>);
+      if (N <= 22) launch(gram_tile_kernel<double, 2, true>);
+      else if (N <= 32) launch(gram_tile_kernel<double, 3, true>);
+      else if (db) launch(gram_tile_kernel<double, 9, true>);
+      else launch(gram_tile_kernel<double, 9, false>);
     } else {
-      if (N <= 22) launch(gram_tile_kernel<float, 2>);
-      else if (N <= 32) launch(gram_tile_kernel<float, 3>);
-      else launch(gram_tile_kernel<float, 9>);
+      if (N <= 22) launch(gram_tile_kernel<float, 2, true>);
+      else if (N <= 32) launch(gram_tile_kernel<float, 3, true>);
+      else launch(gram_tile_kernel<float, 9, true>);
     }
     ctx->launches++;
     NRCPS_TRY(check_launch(ctx, "gram_tile_kernel"));

@@ -54,6 +54,42 @@ __global__ void coarse_z2_kernel(const uint32_t* __restrict__ bits, uint64_t bit
   }
 }
 
+// Same block means when every z-row starts on a 32-bit word (L % 32 == 0,
+// bit0 % 32 == 0) and f divides 32: one thread per (configuration, slice,
+// qx, qy) column of G cells reads the f^2 rows of its column one word at a
+// time and counts the +1 sites of each f-bit group with popc -- one load per
+// 32 sites instead of one per site.
+__global__ void coarse_z2_rows_kernel(const uint32_t* __restrict__ bits, uint64_t bit0, int L, int T, int G, int B,
+                                      __nv_bfloat16* __restrict__ x) {
+  const long V = (long)L * L * L;
+  const int GS = G * G * G, f = L / G, per_word = 32 / f, words = L / 32;
+  const uint32_t mask = f >= 32 ? 0xffffffffu : ((1u << f) - 1u);
+  const long total = (long)B * T * G * G;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int qy = (int)(e % G), qx = (int)((e / G) % G);
+    const long ct = e / ((long)G * G);
+    int cnt[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) cnt[q] = 0;
+    for (int a = 0; a < f; ++a)
+      for (int b2 = 0; b2 < f; ++b2) {
+        const uint64_t r0 = bit0 + (uint64_t)ct * V + (uint64_t)L * ((uint64_t)(qy * f + b2) + (uint64_t)L * (qx * f + a));
+        const uint32_t* row = bits + (r0 >> 5);
+        for (int w = 0; w < words; ++w) {
+          const uint32_t word = __ldg(row + w);
+#pragma unroll
+          for (int g = 0; g < 16; ++g)
+            if (g < per_word) cnt[w * per_word + g] += __popc((word >> (g * f)) & mask);
+        }
+      }
+    const float inv = 1.0f / (float)(f * f * f);
+    const long o = ct * GS + (long)G * (qy + (long)G * qx);
+#pragma unroll
+    for (int qz = 0; qz < 16; ++qz)
+      if (qz < G) x[o + qz] = __float2bfloat16((float)(2 * cnt[qz] - f * f * f) * inv);
+  }
+}
+
 // ------------------------------------------------------------- conv fwd
 // One block per sample; the sample's input and the layer's weights in
 // shared memory (BF16); each thread computes all Cout outputs of its sites.
@@ -290,6 +326,14 @@ extern "C" nrcps_status nrcps_cv_coarse_z2(nrcps_context* ctx, const uint32_t* d
                 "nrcps_cv_coarse_z2: bad arguments (G must divide L)");
   const long total = (long)B * T * G * G * G;
   if (total == 0) return NRCPS_OK;
+  const int f = L / G;
+  if (L % 32 == 0 && bit0 % 32 == 0 && 32 % f == 0 && G <= 16) {
+    const long cols = (long)B * T * G * G;
+    coarse_z2_rows_kernel<<<grid_for(cols, 256, (long)ctx->sm_count * 32), 256, 0, ctx->stream>>>(
+        dev_bits, bit0, L, T, G, B, reinterpret_cast<__nv_bfloat16*>(dev_x));
+    ctx->launches++;
+    return check_launch(ctx, "coarse_z2_rows_kernel");
+  }
   coarse_z2_kernel<<<grid_for(total, 256, (long)ctx->sm_count * 32), 256, 0, ctx->stream>>>(
       dev_bits, bit0, L, T, G, B, reinterpret_cast<__nv_bfloat16*>(dev_x));
   ctx->launches++;

@@ -4,6 +4,7 @@ context's stream, after warm-up), one JSON line per measurement.
     python -m nrcps_b200.kernel_bench step    --L 32 --orbitals 19456 [--kind K --cluster C] [--precision f32]
     python -m nrcps_b200.kernel_bench overlap --L 32 --ns 19 --nconf 1024 [--tc 1|0]
     python -m nrcps_b200.kernel_bench dets    --N 19 --nconf 4096
+    python -m nrcps_b200.kernel_bench cv      --T 64 --batch 256
 
 step:    one transfer-matrix step (nrcps_propagate, Z2 field, a = 0.5) over
          `orbitals` orbitals in batches of 19; GB/s counts one read and one
@@ -12,6 +13,9 @@ overlap: S = <src|psi> for FP32 orbitals with dense FP64 sources
          (nrcps_overlap); GB/s counts one read of psi, TFLOP/s the useful
          8 ns nt V complex multiply-adds per configuration.
 dets:    determinants of all N leading minors of nconf FP64 matrices.
+cv:      one training step (forward, backward, Adam) and one inference pass
+         of the control-variate network on random inputs; TFLOP/s counts the
+         conv multiply-adds (2 flops each; backward twice the forward).
 """
 from __future__ import annotations
 
@@ -97,9 +101,31 @@ def bench_dets(ctx: Context, N: int, nconf: int, reps: int) -> dict:
             "matrices_per_s": round(nconf / ms * 1e3, 1)}
 
 
+def bench_cv(ctx: Context, T: int, batch: int, reps: int) -> dict:
+    from .cv import ControlVariateNet, NetShape
+    s = NetShape(T=T, G=8)
+    net = ControlVariateNet(s, seed=0, ctx=ctx)
+    g = torch.Generator(device=ctx.device).manual_seed(3)
+    x = (torch.rand((batch, T, s.GS), device=ctx.device, generator=g) * 2 - 1).to(torch.bfloat16)
+    y = torch.randn((batch, T), device=ctx.device, generator=g)
+
+    def train():
+        net.forward(x)
+        net.backward(x, y)
+        net.adam()
+
+    ms_train = _time(train, reps)
+    ms_fwd = _time(lambda: net.forward(x), reps)
+    ctx.synchronize()
+    macs = batch * s.GS * s.C * 27 * (T + 2 * s.C)  # three conv layers
+    return {"kernel": "cv", "T": T, "batch": batch, "train_step_ms": round(ms_train, 4),
+            "forward_ms": round(ms_fwd, 4), "forward_TFLOPs": round(2 * macs / ms_fwd / 1e9, 2),
+            "train_TFLOPs": round(6 * macs / ms_train / 1e9, 2)}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["step", "overlap", "dets"])
+    ap.add_argument("what", choices=["step", "overlap", "dets", "cv"])
     ap.add_argument("--L", type=int, default=32)
     ap.add_argument("--orbitals", type=int, default=19456)
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
@@ -110,12 +136,16 @@ def main(argv=None) -> int:
     ap.add_argument("--tc", type=int, default=1)
     ap.add_argument("--N", type=int, default=19)
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--T", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=256)
     a = ap.parse_args(argv)
     ctx = Context(0)
     if a.what == "step":
         r = bench_step(ctx, a.L, a.orbitals, a.precision, a.kind, a.cluster, a.reps)
     elif a.what == "overlap":
         r = bench_overlap(ctx, a.L, a.ns, a.nconf, a.tc, a.reps)
+    elif a.what == "cv":
+        r = bench_cv(ctx, a.T, a.batch, a.reps)
     else:
         r = bench_dets(ctx, a.N, a.nconf, a.reps)
     print(json.dumps(r), flush=True)

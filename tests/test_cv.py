@@ -100,3 +100,23 @@ def test_training_and_control_variate_on_a_small_ensemble():
     assert float(var_ratio.median()) < 0.5
     z = (est - plain).abs() / (plain_err ** 2 + est_err ** 2).sqrt()
     assert float(z[1:].max()) < 4.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,G", [(32, 8), (16, 4), (8, 4)])
+def test_coarse_field_block_means(L, G):
+    """Block means of the Z2 field against numpy (the word-at-a-time kernel
+    at L = 32, the per-site kernel otherwise)."""
+    import torch
+    import nrcps_b200 as nb
+    from nrcps_b200 import cv
+    ctx = nb.default_context()
+    B, T = 2, 3
+    bits = nb.draw_z2_bits("RANLXS2", 17, 0, B * T * L ** 3, ctx)
+    got = cv.coarse_fields(bits, 0, L, T, G, B, ctx).float().cpu().numpy()
+    w = bits.cpu().numpy().astype(np.uint32)
+    allbits = np.unpackbits(w.view(np.uint8), bitorder="little")[: B * T * L ** 3].astype(np.float64)
+    phi = (2 * allbits - 1).reshape(B, T, L, L, L)
+    f = L // G
+    ref = phi.reshape(B, T, G, f, G, f, G, f).mean(axis=(3, 5, 7)).reshape(B, T, G ** 3)
+    assert np.array_equal(got, ref.astype(np.float32).astype(np.float64))

@@ -116,11 +116,20 @@ def bench_cv(ctx: Context, T: int, batch: int, reps: int) -> dict:
 
     ms_train = _time(train, reps)
     ms_fwd = _time(lambda: net.forward(x), reps)
+    # feature extraction at L = 32: Z2 bits of `batch` configurations, then block means
+    from .api import draw_z2_bits
+    from .cv import coarse_fields
+    L = 32
+    nbits = batch * T * L ** 3
+    bits = draw_z2_bits("RANLXS2", 1, 0, nbits, ctx)
+    ms_draw = _time(lambda: draw_z2_bits("RANLXS2", 1, 0, nbits, ctx), reps)
+    ms_coarse = _time(lambda: coarse_fields(bits, 0, L, T, s.G, batch, ctx), reps)
     ctx.synchronize()
     macs = batch * s.GS * s.C * 27 * (T + 2 * s.C)  # three conv layers
     return {"kernel": "cv", "T": T, "batch": batch, "train_step_ms": round(ms_train, 4),
             "forward_ms": round(ms_fwd, 4), "forward_TFLOPs": round(2 * macs / ms_fwd / 1e9, 2),
-            "train_TFLOPs": round(6 * macs / ms_train / 1e9, 2)}
+            "train_TFLOPs": round(6 * macs / ms_train / 1e9, 2), "z2_draw_ms": round(ms_draw, 4),
+            "coarse_ms": round(ms_coarse, 4), "coarse_GBs": round(nbits / 8 / ms_coarse / 1e6, 1)}
 
 
 def main(argv=None) -> int:

@@ -417,6 +417,23 @@ nrcps_status nrcps_branch_destroy(nrcps_branch *branch);
  * phi = +1. */
 nrcps_status nrcps_cv_coarse_z2(nrcps_context *ctx, const uint32_t *dev_bits, uint64_t bit0, int L, int T, int G,
                                 int B, void *dev_x);
+/* The same features for B fresh uniform Z2 fields (numbers first ..
+ * first + B - 1 of the stream `seed`), drawn directly: the block mean of
+ * n = (L/G)^3 independent +-1 sites is (2 c - n)/n with c the set bits of n
+ * Philox4x32-10 bits (counter (cell lo, cell hi, word / 4, 0x5A32), key
+ * seed).  For the control variate's mean <g> over the field distribution. */
+nrcps_status nrcps_cv_sample_z2_features(nrcps_context *ctx, uint64_t seed, uint64_t first, int L, int T, int G,
+                                         int B, void *dev_x);
+/* Inference of the whole network on the tcgen05 tensor cores, one kernel:
+ * three conv layers (BF16 MMAs, FP32 accumulation in TMEM, BF16
+ * activations), mean pool and head; y[b][t] = standardised prediction.
+ * G = 8; Cin a multiple of 16 up to 64; H <= 64; T <= 256.  dev_W[l] BF16
+ * [16][cin][27], dev_bias[l] FP32 [16] for l = 0..2 (device pointers held in
+ * host arrays). */
+nrcps_status nrcps_cv_forward_tc(nrcps_context *ctx, const void *dev_x, int Cin, int G, int B,
+                                 const void *const *dev_W, const float *const *dev_bias, const float *dev_hw,
+                                 const float *dev_hb, int H, const float *dev_ow, const float *dev_ob, int T,
+                                 float *dev_y);
 /* Z = conv(in) + bias (FP32), A = tanh(Z) (BF16); Cout = 16; W BF16 [Cout][Cin][27]. */
 nrcps_status nrcps_cv_conv_forward(nrcps_context *ctx, const void *dev_in, int Cin, int Cout, int G, int B,
                                    const void *dev_W, const float *dev_bias, float *dev_Z, void *dev_A);

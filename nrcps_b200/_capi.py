@@ -121,6 +121,8 @@ SIGNATURES = {
     "nrcps_branch_run": ([_P, _P], _I),
     "nrcps_branch_destroy": ([_P], _I),
     "nrcps_cv_coarse_z2": ([_P, _P, _U64, _I, _I, _I, _I, _P], _I),
+    "nrcps_cv_sample_z2_features": ([_P, _U64, _U64, _I, _I, _I, _I, _P], _I),
+    "nrcps_cv_forward_tc": ([_P, _P, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _I, _P], _I),
     "nrcps_cv_conv_forward": ([_P, _P, _I, _I, _I, _I, _P, _P, _P, _P], _I),
     "nrcps_cv_conv_backward": ([_P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P], _I),
     "nrcps_cv_head_forward": ([_P, _P, _I, _I, _I, _P, _P, _I, _P, _P, _I, _P, _P, _P], _I),

@@ -90,6 +90,53 @@ __global__ void coarse_z2_rows_kernel(const uint32_t* __restrict__ bits, uint64_
   }
 }
 
+// ------------------------------------------------- direct feature draws
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of two
+// 32x32 -> 64-bit products with the key bumped by the Weyl constants.
+struct U4 {
+  uint32_t x, y, z, w;
+};
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// Block means of a uniform Z2 field drawn directly: the n = f^3 sites of a
+// cell are n independent fair bits, so the mean is (2 popc - n)/n.  Cell
+// g = ((first + b) T + t) G^3 + q takes word i from output i % 4 of the
+// Philox call with counter (lo g, hi g, i / 4, 0x5A32), key = seed; the last
+// word keeps its n mod 32 low bits.  One thread per cell.
+__global__ void sample_z2_features_kernel(uint64_t seed, uint64_t first, int T, int GS, int n, long total,
+                                          __nv_bfloat16* __restrict__ x) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  const int words = (n + 31) / 32;
+  const float inv = 1.0f / (float)n;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const uint64_t g = first * (uint64_t)T * (uint64_t)GS + (uint64_t)e;
+    int cnt = 0;
+    for (int grp = 0; grp * 4 < words; ++grp) {
+      const U4 o = philox4x32_10(U4{(uint32_t)g, (uint32_t)(g >> 32), (uint32_t)grp, 0x5A32u}, k0, k1);
+      const uint32_t w4[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int i = grp * 4 + j;
+        if (i < words) {
+          const int rem = n - 32 * i;
+          cnt += __popc(rem < 32 ? (w4[j] & ((1u << rem) - 1u)) : w4[j]);
+        }
+      }
+    }
+    x[e] = __float2bfloat16((float)(2 * cnt - n) * inv);
+  }
+}
+
 // ------------------------------------------------------------- conv fwd
 // One block per sample; the sample's input and the layer's weights in
 // shared memory (BF16); each thread computes all Cout outputs of its sites.
@@ -338,6 +385,20 @@ extern "C" nrcps_status nrcps_cv_coarse_z2(nrcps_context* ctx, const uint32_t* d
       dev_bits, bit0, L, T, G, B, reinterpret_cast<__nv_bfloat16*>(dev_x));
   ctx->launches++;
   return check_launch(ctx, "coarse_z2_kernel");
+}
+
+extern "C" nrcps_status nrcps_cv_sample_z2_features(nrcps_context* ctx, uint64_t seed, uint64_t first, int L, int T,
+                                                    int G, int B, void* dev_x) {
+  if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
+  NRCPS_REQUIRE(ctx, dev_x && L > 0 && G > 0 && L % G == 0 && T > 0 && B >= 0,
+                "nrcps_cv_sample_z2_features: bad arguments (G must divide L)");
+  const int f = L / G;
+  const long total = (long)B * T * G * G * G;
+  if (total == 0) return NRCPS_OK;
+  sample_z2_features_kernel<<<grid_for(total, 256, (long)ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+      seed, first, T, G * G * G, f * f * f, total, reinterpret_cast<__nv_bfloat16*>(dev_x));
+  ctx->launches++;
+  return check_launch(ctx, "sample_z2_features_kernel");
 }
 
 extern "C" nrcps_status nrcps_cv_conv_forward(nrcps_context* ctx, const void* dev_in, int Cin, int Cout, int G,

@@ -116,6 +116,27 @@ class ControlVariateNet:
                   "cv head")
         return b["y"]
 
+    def tc_inference_supported(self) -> bool:
+        s = self.s
+        return s.G == 8 and s.T % 16 == 0 and s.T <= 64 and s.C == 16 and s.H <= 64
+
+    def infer(self, x: torch.Tensor) -> torch.Tensor:
+        """Standardised predictions [B, T] for inference: one tensor-core kernel
+        (nrcps_cv_forward_tc) for the whole network where the shape allows it
+        (G = 8, T a multiple of 16 up to 64), else the layer-by-layer kernels
+        of forward().  No activations are kept for a backward pass."""
+        if not self.tc_inference_supported():
+            return self.forward(x)
+        s, ctx = self.s, self.ctx
+        B = x.shape[0]
+        P = self.params
+        y = torch.empty((B, s.T), dtype=torch.float32, device=ctx.device)
+        W = (ctypes.c_void_p * 3)(*[self.bf16[k].data_ptr() for k in ("w1", "w2", "w3")])
+        bias = (ctypes.c_void_p * 3)(*[P[k].data_ptr() for k in ("b1", "b2", "b3")])
+        ctx.check(lib().nrcps_cv_forward_tc(ctx.handle, _p(x), s.T, s.G, B, W, bias, _p(P["hw"]), _p(P["hb"]), s.H,
+                                            _p(P["ow"]), _p(P["ob"]), s.T, _p(y)), "cv forward (tensor cores)")
+        return y
+
     def backward(self, x: torch.Tensor, target: torch.Tensor) -> float:
         """Gradients of 0.5 mean (y - target)^2 after forward(x); returns the loss."""
         s, L, ctx = self.s, lib(), self.ctx
@@ -174,7 +195,7 @@ class ControlVariateNet:
         """Predicted log C(tau) [n, T] (FP64, de-standardised)."""
         out = []
         for i in range(0, X.shape[0], chunk):
-            y = self.forward(X[i:i + chunk].contiguous()).double().cpu()
+            y = self.infer(X[i:i + chunk].contiguous()).double().cpu()
             out.append(y * self.sigma + self.mu)
         return torch.cat(out)
 
@@ -185,6 +206,15 @@ def coarse_fields(bits: torch.Tensor, bit0: int, L: int, T: int, G: int, n: int,
     slice t of configuration c is bits bit0 + (c T + t) L^3 ..."""
     x = torch.empty((n, T, G ** 3), dtype=torch.bfloat16, device=ctx.device)
     ctx.check(lib().nrcps_cv_coarse_z2(ctx.handle, _p(bits), bit0, L, T, G, n, _p(x)), "cv coarse")
+    return x
+
+
+def sample_z2_features(seed: int, first: int, L: int, T: int, G: int, n: int, ctx: Context) -> torch.Tensor:
+    """Block means [n, T, G^3] BF16 of n fresh uniform Z2 fields (numbers
+    first .. first + n - 1 of the Philox stream `seed`), drawn directly from
+    their exact distribution: the mean of (L/G)^3 independent +-1 sites."""
+    x = torch.empty((n, T, G ** 3), dtype=torch.bfloat16, device=ctx.device)
+    ctx.check(lib().nrcps_cv_sample_z2_features(ctx.handle, seed, first, L, T, G, n, _p(x)), "cv sample features")
     return x
 
 
@@ -212,9 +242,16 @@ def generate_pairs(L: int, T: int, fermi_energy: float, seed: int, n_conf: int, 
 
 
 def extra_fields_mean_g(net: ControlVariateNet, L: int, seed: int, first_conf: int, n_fields: int,
-                        chunk: int = 8192, ctx: Optional[Context] = None):
+                        chunk: int = 8192, ctx: Optional[Context] = None, sampler: str = "philox"):
     """<g(tau)> over n_fields extra field draws (no propagation): mean and
-    standard error of exp(predicted log C) per tau, and the GPU seconds."""
+    standard error of exp(predicted log C) per tau, and the GPU seconds.
+
+    sampler "philox" draws the block-mean features directly from their exact
+    distribution (sample_z2_features); "ranlux" draws whole RANLXS2 fields
+    and coarse-grains them (the generator of the ensemble, 2 M bits per
+    field).  Both give independent fields of the same distribution."""
+    if sampler not in ("philox", "ranlux"):
+        raise ValueError(f"unknown sampler {sampler!r}")
     ctx = ctx or net.ctx
     T, G, V = net.s.T, net.s.G, L ** 3
     s1 = torch.zeros(T, dtype=torch.float64)
@@ -223,8 +260,11 @@ def extra_fields_mean_g(net: ControlVariateNet, L: int, seed: int, first_conf: i
     t0 = time.perf_counter()
     for c0 in range(first_conf, first_conf + n_fields, chunk):
         m = min(chunk, first_conf + n_fields - c0)
-        bits = draw_z2_bits("RANLXS2", seed, c0 * T * V, m * T * V, ctx)
-        x = coarse_fields(bits, 0, L, T, G, m, ctx)
+        if sampler == "philox":
+            x = sample_z2_features(seed, c0, L, T, G, m, ctx)
+        else:
+            bits = draw_z2_bits("RANLXS2", seed, c0 * T * V, m * T * V, ctx)
+            x = coarse_fields(bits, 0, L, T, G, m, ctx)
         g = torch.exp(net.predict_logC(x, chunk=m))
         s1 += g.sum(0)
         s2 += (g ** 2).sum(0)

@@ -116,6 +116,7 @@ def bench_cv(ctx: Context, T: int, batch: int, reps: int) -> dict:
 
     ms_train = _time(train, reps)
     ms_fwd = _time(lambda: net.forward(x), reps)
+    ms_tc = _time(lambda: net.infer(x), reps)
     # feature extraction at L = 32: Z2 bits of `batch` configurations, then block means
     from .api import draw_z2_bits
     from .cv import coarse_fields
@@ -128,6 +129,7 @@ def bench_cv(ctx: Context, T: int, batch: int, reps: int) -> dict:
     macs = batch * s.GS * s.C * 27 * (T + 2 * s.C)  # three conv layers
     return {"kernel": "cv", "T": T, "batch": batch, "train_step_ms": round(ms_train, 4),
             "forward_ms": round(ms_fwd, 4), "forward_TFLOPs": round(2 * macs / ms_fwd / 1e9, 2),
+            "infer_tc_ms": round(ms_tc, 4), "infer_tc_TFLOPs": round(2 * macs / ms_tc / 1e9, 2),
             "train_TFLOPs": round(6 * macs / ms_train / 1e9, 2), "z2_draw_ms": round(ms_draw, 4),
             "coarse_ms": round(ms_coarse, 4), "coarse_GBs": round(nbits / 8 / ms_coarse / 1e6, 1)}
 

@@ -120,3 +120,88 @@ def test_coarse_field_block_means(L, G):
     f = L // G
     ref = phi.reshape(B, T, G, f, G, f, G, f).mean(axis=(3, 5, 7)).reshape(B, T, G ** 3)
     assert np.array_equal(got, ref.astype(np.float32).astype(np.float64))
+
+
+def test_philox_known_answers():
+    """The oracle's Philox4x32-10 against the published known-answer vectors."""
+    from oracle import philox
+    for ctr, key, want in philox.PHILOX_KATS:
+        got = philox.philox4x32_10(*[np.uint32(c) for c in ctr], np.uint32(key[0]), np.uint32(key[1]))
+        assert tuple(int(v) for v in got) == want
+
+
+def test_sampled_features_have_the_block_mean_distribution():
+    """Oracle features at L=8, G=4 (8 sites per cell): the counts are
+    Binomial(8, 1/2) (chi-square over the 9 values)."""
+    from math import comb
+    from oracle import philox
+    x = philox.z2_block_features(5, 0, 8, 16, 4, 64)
+    c = np.rint((x.ravel() * 8 + 8) / 2).astype(int)
+    obs = np.bincount(c, minlength=9)
+    exp = np.array([comb(8, k) for k in range(9)]) / 256.0 * c.size
+    chi2 = float(((obs - exp) ** 2 / exp).sum())
+    assert chi2 < 30.0  # 8 degrees of freedom: p ~ 2e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,G,T,B,first", [(32, 8, 8, 6, 0), (8, 4, 5, 7, 3), (24, 8, 3, 4, 11), (48, 8, 2, 3, 1 << 33)])
+def test_device_feature_sampler_matches_oracle(L, G, T, B, first):
+    """nrcps_cv_sample_z2_features bit-exact against the oracle (1, 8, 27
+    and 216 bits per cell; a field number above 2^32)."""
+    import nrcps_b200 as nb
+    from nrcps_b200 import cv
+    from oracle import philox
+    ctx = nb.default_context()
+    seed = (7 << 32) | 3000
+    got = cv.sample_z2_features(seed, first, L, T, G, B, ctx).float().cpu().numpy()
+    want = philox.z2_block_features(seed, first, L, T, G, B)
+    assert np.array_equal(got.astype(np.float64), want)
+
+
+@pytest.mark.gpu
+def test_sampled_features_match_coarse_grained_ranlux_fields():
+    """The direct draws and the block means of RANLXS2 fields have the same
+    distribution at L=32, G=8 (per-cell mean and variance of 4096 x 8 x 512
+    values each; variance 1/64 for both)."""
+    import nrcps_b200 as nb
+    from nrcps_b200 import cv
+    ctx = nb.default_context()
+    L, T, G, B = 32, 8, 8, 4096
+    a = cv.sample_z2_features(11, 0, L, T, G, B, ctx).double()
+    bits = nb.draw_z2_bits("RANLXS2", 11, 0, B * T * L ** 3, ctx)
+    b = cv.coarse_fields(bits, 0, L, T, G, B, ctx).double()
+    n = a.numel()
+    for v in (a, b):
+        assert abs(float(v.mean())) < 5 * (1 / 64 / n) ** 0.5
+        assert abs(float(v.var()) - 1 / 64) < 5 * (2 / 64 ** 2 / n) ** 0.5
+    assert set(torch_unique(a)) <= {k / 32 for k in range(-32, 33)}
+
+
+def torch_unique(t):
+    return [float(v) for v in t.unique().cpu()]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("T,B", [(64, 6), (16, 5), (48, 3), (32, 300)])
+def test_tensor_core_inference_matches_reference(T, B):
+    """nrcps_cv_forward_tc (the whole network in one tcgen05 kernel) against
+    the CPU reference with the same BF16 roundings (5e-3 of the norm; FP32
+    accumulation in another order) and against the layer-by-layer CUDA-core
+    kernels; B = 300 runs several samples per CTA."""
+    import torch
+    import nrcps_b200 as nb
+    from nrcps_b200.cv import ControlVariateNet, NetShape
+    ctx = nb.default_context()
+    net = ControlVariateNet(NetShape(T=T, G=8), seed=5, ctx=ctx)
+    rs = np.random.default_rng(T + B)
+    for k in ("b1", "b2", "b3", "hb", "ob"):  # non-zero biases
+        net.params[k].copy_(torch.from_numpy(0.1 * rs.standard_normal(net.params[k].shape)).float())
+    assert net.tc_inference_supported()
+    x = torch.from_numpy(rs.uniform(-1, 1, (B, T, 512)).astype(np.float32)).to(torch.bfloat16).to(ctx.device)
+    y_tc = net.infer(x).cpu().numpy().astype(np.float64)
+    y_cc = net.forward(x).cpu().numpy().astype(np.float64)
+    p = {k: v.cpu().numpy().astype(np.float64) for k, v in net.params.items()}
+    n = min(B, 8)
+    y_ref, _ = R.forward(p, x[:n].float().cpu().numpy().astype(np.float64), 8, bf16=True)
+    assert _norm_err(y_tc[:n], y_ref) < 5e-3
+    assert _norm_err(y_tc, y_cc) < 5e-3

@@ -98,6 +98,8 @@ const char *nrcps_version(void);
  *                      half-length DFTs per instruction; FP32 only); 7, 8:
  *                      kinds 0, 4 with the slab prefetched into L2 instead
  *                      of staged in shared memory (four CTAs per SM);
+ *                      9, 10: kinds 6, 3 with the CTA's slab of the
+ *                      kinetic table resident in shared memory (FP32);
  *   "overlap.tc"       1 (default): dense-source overlaps of FP32 orbitals
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the

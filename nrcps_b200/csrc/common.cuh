@@ -97,7 +97,7 @@ struct Context {
   int fused_enabled = 1;  // single-pass cluster kernel where a variant exists
   int fused_cluster = 0;  // 0: autotuned / default cluster size
   int fused_split = -1;   // -1: autotuned; 0: one lane per pencil; 1: two lanes per pencil
-  int fused_kind = -1;    // -1: autotuned; else the fused kernel's kind (0..8)
+  int fused_kind = -1;    // -1: autotuned; else the fused kernel's kind (0..10)
   int lu_warp = 1;        // 1: warp-per-minor determinant kernel for N <= 64; 0: thread-per-minor kernel
   int overlap_tc = 1;     // 1: tensor-core overlap for FP32 orbitals where the shape allows; 0: CUDA cores
   // TF32 hi / lo split of the sources for nrcps_overlap's tensor-core path (grown on demand)

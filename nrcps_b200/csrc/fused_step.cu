@@ -556,14 +556,15 @@ __device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_
 // (its work mbarrier) it knows that slot s of this CTA has been read out;
 // the same holds for region r of work with CTA r.  Every mbarrier wait is
 // bounded.
-template <typename R, int L, int C, bool STAGED = true>
+template <typename R, int L, int C, bool STAGED = true, bool KSM = false>
 struct BulkShape {
   using Base = FusedShape<R, L, C>;
   static constexpr int THREADS = Base::THREADS;
   static constexpr uint32_t REGION_BYTES = (uint32_t)(Base::REGION * sizeof(cplx<R>));
   static constexpr uint32_t XBYTES = (uint32_t)(C * REGION_BYTES);       // one exchange, received
   static constexpr uint32_t STAGE_BYTES = (uint32_t)(Base::STAGE * sizeof(cplx<R>));
-  static constexpr size_t SMEM = 128 + (STAGED ? STAGE_BYTES : 0) + 2 * (size_t)XBYTES;
+  static constexpr uint32_t KIN_BYTES = KSM ? (uint32_t)(Base::STAGE * sizeof(float2)) : 0u;  // slab of k(p)
+  static constexpr size_t SMEM = 128 + (STAGED ? STAGE_BYTES : 0) + 2 * (size_t)XBYTES + KIN_BYTES;
   static constexpr int CTAS = (int)(228 * 1024 / (SMEM + 1024));
   static constexpr int WANT = (384 / THREADS) < 1 ? 1 : 384 / THREADS;
   static constexpr int MIN_BLOCKS = CTAS < 1 ? 1 : (CTAS > WANT ? WANT : CTAS);
@@ -582,11 +583,16 @@ __device__ __forceinline__ void bulk_to_peer(uint32_t dst, const void* src, uint
 
 // STAGED = false: no stage buffer; the next slab is prefetched into L2 and
 // pass 1 reads it from there (two buffers instead of three per CTA).
-template <typename R, int L, int C, bool STAGED, bool PK = false>
-__global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape<R, L, C, STAGED>::MIN_BLOCKS)
+// KSM (FP32): the CTA's slab of the kinetic table (hi, lo) stays in shared
+// memory for the whole launch -- the slab index c of a CTA never changes, so
+// passes 1 and 5 read k(p) there instead of from L2.
+template <typename R, int L, int C, bool STAGED, bool PK = false, bool KSM = false>
+__global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
+                                  BulkShape<R, L, C, STAGED, KSM>::MIN_BLOCKS)
     fused_step_bulk_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
-  using Bs = BulkShape<R, L, C, STAGED>;
+  using Bs = BulkShape<R, L, C, STAGED, KSM>;
+  static_assert(!KSM || sizeof(R) == 4, "the resident kinetic slab is the FP32 (hi, lo) table");
   static_assert(C > 1, "the exchange is between CTAs of a cluster");
   constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION;
   constexpr int V = L * L * L;
@@ -597,6 +603,16 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
   cplx<R>* stage = reinterpret_cast<cplx<R>*>(smem_raw + 128);
   cplx<R>* work = stage + (STAGED ? Sh::STAGE : 0);
   cplx<R>* recv = work + Sh::WORK;
+  float2* kin_s = reinterpret_cast<float2*>(recv + Sh::WORK);  // KSM: k(p) of sites c S L^2 + i
+  // k(p) x for global site `site` = c S L^2 + `local`
+  auto kin = [&](int site, int local, cplx<R> v) -> cplx<R> {
+    if constexpr (KSM) {
+      const float2 k = kin_s[local];
+      return scale_w<R, PK>(v, k.x, k.y);
+    } else {
+      return apply_kin<R, PK>(f, site, v);
+    }
+  };
 
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
@@ -621,6 +637,8 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
+  if constexpr (KSM)
+    for (int i = tid; i < Sh::STAGE; i += Bs::THREADS) kin_s[i] = __ldg(f.kin_f + (size_t)c * Sh::STAGE + i);
   cluster.sync();  // every CTA's mbarriers are initialised before any copy targets them
   uint32_t parity = 0;
   long orb = cluster_id;
@@ -645,7 +663,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
       const int site0 = (c * S + xl) * L * L + z;
       if constexpr (STAGED) {
 #pragma unroll
-        for (int y = 0; y < L; ++y) x[y] = apply_kin<R, PK>(f, site0 + y * L, stage[(xl * L + y) * L + z]);
+        for (int y = 0; y < L; ++y) x[y] = kin(site0 + y * L, (xl * L + y) * L + z, stage[(xl * L + y) * L + z]);
       } else {
         const cplx<R>* src = slab(orb);
 #pragma unroll
@@ -658,7 +676,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
             double2 t = __ldcg(reinterpret_cast<const double2*>(src) + (xl * L + y) * L + z);
             v = cplx<R>{t.x, t.y};
           }
-          x[y] = apply_kin<R, PK>(f, site0 + y * L, v);
+          x[y] = kin(site0 + y * L, (xl * L + y) * L + z, v);
         }
       }
       fft::dft<L, -1, R, PK>(x);
@@ -745,7 +763,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
       fft::dft<L, +1, R, PK>(x);
 #pragma unroll
       for (int y = 0; y < L; ++y) {
-        cplx<R> v = apply_kin<R, PK>(f, site0 + y * L, x[y]);
+        cplx<R> v = kin(site0 + y * L, (xl * L + y) * L + z, x[y]);
         if constexpr (sizeof(R) == 4)
           __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(v.re, v.im));
         else
@@ -763,14 +781,16 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED>::THREADS, BulkShape
 // 1: two lanes per pencil; 2: bulk-copy exchange, staged slab; 3: bulk-copy
 // exchange, slab prefetched into L2; 4, 5, 6: kinds 0, 2, 3 with the packed
 // FP32x2 transforms (FP32 only); 7, 8: kinds 0, 4 with the slab prefetched
-// into L2 instead of staged (four CTAs per SM).
+// into L2 instead of staged (four CTAs per SM); 9, 10: kinds 6, 3 with the
+// CTA's slab of the kinetic table resident in shared memory (FP32 only).
 template <typename R, int L, int C, int KIND = 0>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
-  static_assert(KIND < 4 || KIND == 7 || sizeof(R) == 4, "packed transforms are FP32");
+  static_assert(KIND < 4 || KIND == 7 || sizeof(R) == 4, "packed transforms and the resident k(p) slab are FP32");
   constexpr int THREADS = KIND == 1 ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
   constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
                           : (KIND == 3 || KIND == 6) ? BulkShape<R, L, C, false>::SMEM
+                          : (KIND == 9 || KIND == 10) ? BulkShape<R, L, C, false, true>::SMEM
                           : (KIND == 7 || KIND == 8) ? PullShape<R, L, C, false>::SMEM
                                                      : Sh::SMEM;
   void (*kern)(FusedArgs);
@@ -780,6 +800,8 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   else if constexpr (KIND == 4) kern = fused_step_kernel<R, L, C, true>;
   else if constexpr (KIND == 5) kern = fused_step_bulk_kernel<R, L, C, true, true>;
   else if constexpr (KIND == 6) kern = fused_step_bulk_kernel<R, L, C, false, true>;
+  else if constexpr (KIND == 9) kern = fused_step_bulk_kernel<R, L, C, false, true, true>;
+  else if constexpr (KIND == 10) kern = fused_step_bulk_kernel<R, L, C, false, false, true>;
   else if constexpr (KIND == 7) kern = fused_step_kernel<R, L, C, false, false>;
   else if constexpr (KIND == 8) kern = fused_step_kernel<R, L, C, true, false>;
   else kern = fused_step_kernel<R, L, C>;
@@ -827,7 +849,7 @@ struct FusedVariant {
   int L;
   int C;
   int kind;  // 0: exchange through peers' shared memory; 1: lane split; 2/3: bulk-copy exchange; 4-6: packed;
-             // 7/8: peer access with the slab prefetched into L2
+             // 7/8: peer access with the slab prefetched into L2; 9/10: kinds 6/3 with k(p) resident
   FusedLauncher fn;
 };
 
@@ -844,12 +866,16 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 16, 1, 4, launch_fused<float, 16, 1, 4>},
     {NRCPS_F32, 16, 1, 0, launch_fused<float, 16, 1>},
     {NRCPS_F32, 16, 2, 2, launch_fused<float, 16, 2, 2>},
+    {NRCPS_F32, 16, 2, 9, launch_fused<float, 16, 2, 9>},
+    {NRCPS_F32, 16, 2, 10, launch_fused<float, 16, 2, 10>},
     {NRCPS_F32, 16, 2, 0, launch_fused<float, 16, 2>},
     {NRCPS_F32, 16, 1, 1, launch_fused<float, 16, 1, 1>},
     {NRCPS_F32, 24, 3, 5, launch_fused<float, 24, 3, 5>},
     {NRCPS_F32, 24, 4, 4, launch_fused<float, 24, 4, 4>},
     {NRCPS_F32, 24, 3, 2, launch_fused<float, 24, 3, 2>},
     {NRCPS_F32, 24, 4, 2, launch_fused<float, 24, 4, 2>},
+    {NRCPS_F32, 24, 4, 9, launch_fused<float, 24, 4, 9>},
+    {NRCPS_F32, 24, 4, 10, launch_fused<float, 24, 4, 10>},
     {NRCPS_F32, 24, 3, 0, launch_fused<float, 24, 3>},
     {NRCPS_F32, 24, 4, 0, launch_fused<float, 24, 4>},
     {NRCPS_F32, 32, 8, 4, launch_fused<float, 32, 8, 4>},
@@ -858,6 +884,8 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 32, 8, 6, launch_fused<float, 32, 8, 6>},
     {NRCPS_F32, 32, 8, 5, launch_fused<float, 32, 8, 5>},
     {NRCPS_F32, 32, 8, 3, launch_fused<float, 32, 8, 3>},
+    {NRCPS_F32, 32, 8, 9, launch_fused<float, 32, 8, 9>},
+    {NRCPS_F32, 32, 8, 10, launch_fused<float, 32, 8, 10>},
     {NRCPS_F32, 32, 16, 3, launch_fused<float, 32, 16, 3>},
     {NRCPS_F32, 32, 8, 0, launch_fused<float, 32, 8>},
     {NRCPS_F32, 32, 8, 2, launch_fused<float, 32, 8, 2>},

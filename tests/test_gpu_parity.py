@@ -430,11 +430,33 @@ def test_packed_variants_agree(ctx, kind, L, cluster):
 
 
 @pytest.mark.parametrize("kind,ref_kind,precision,cluster", [(5, 4, "f32", 8), (6, 4, "f32", 8), (8, 4, "f32", 8),
-                                                             (7, 0, "f32", 8), (7, 0, "f64", 16)])
+                                                             (7, 0, "f32", 8), (7, 0, "f64", 16), (9, 4, "f32", 8),
+                                                             (10, 0, "f32", 8)])
 def test_same_arithmetic_variants_are_bit_identical(ctx, kind, ref_kind, precision, cluster):
     """Variants that differ only in how the slab reaches shared memory or how
     the exchange moves it run the same arithmetic: results agree bit for bit."""
     psi, kinv, bits = _random_step_inputs(ctx, 32, 3, 5, precision, seed=6)
+    try:
+        ctx.set_option("fused.cluster", cluster)
+        ctx.set_option("fused.kind", ref_kind)
+        ref = psi.clone()
+        nb.propagate(ref, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.set_option("fused.kind", kind)
+        q = psi.clone()
+        nb.propagate(q, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.synchronize()
+        assert torch.equal(q, ref)
+    finally:
+        ctx.set_option("fused.cluster", 0)
+        ctx.set_option("fused.kind", -1)
+
+
+@pytest.mark.parametrize("kind,ref_kind,L,cluster", [(10, 0, 16, 2), (10, 0, 24, 4), (9, 4, 24, 4), (9, 5, 32, 8)])
+def test_resident_kinetic_slab_variants(ctx, kind, ref_kind, L, cluster):
+    """Kinds 9 and 10 read k(p) from the CTA's resident slab in shared
+    memory instead of L2: the same values and arithmetic as kinds 6 and 3,
+    so they agree bit for bit with the kernels of the same transform order."""
+    psi, kinv, bits = _random_step_inputs(ctx, L, 3, 5, "f32", seed=7)
     try:
         ctx.set_option("fused.cluster", cluster)
         ctx.set_option("fused.kind", ref_kind)

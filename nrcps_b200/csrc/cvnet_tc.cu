@@ -16,9 +16,10 @@
 // the unshifted one, so every tap reads the same buffer through another
 // descriptor.
 //
-// Per sample: layer 1 streams the input through two buffers of 16 channels
-// (threads gather the features into the padded layout while the previous
-// chunk's MMAs run); each epilogue reads the accumulators (tcgen05.ld), adds
+// Per sample: layer 1 streams the input in chunks of 16 channels: the bulk
+// copy engine brings each 16 KiB chunk into shared memory two chunks ahead,
+// threads transpose it into one of two padded operand buffers while the
+// previous chunk's MMAs run; each epilogue reads the accumulators (tcgen05.ld), adds
 // the bias, applies tanh, rounds to BF16 and writes every periodic copy of
 // the site into the next layer's padded input; layer 3's epilogue sums into
 // the mean pool, and the head (tanh hidden layer, linear output) finishes
@@ -26,7 +27,8 @@
 // activations); FP32 accumulation in another order.
 //
 // One persistent CTA per SM (the weights of all three layers stay in shared
-// memory), 4 warps; thread 0 issues the MMAs.  Every mbarrier wait is
+// memory), 8 warps (warp w drains TMEM lanes 32 (w % 4).. for channels
+// 8 (w / 4)..); thread 0 issues the bulk copies and the MMAs.  Every mbarrier wait is
 // bounded: a timeout sets the error flag, the CTA drains its MMAs (bounded),
 // frees its TMEM and returns.
 #include <cuda_bf16.h>
@@ -46,7 +48,8 @@ constexpr int GRID_BYTES = ROWS * ROW_BYTES;  // 16320: one group of 8 channels
 constexpr int BUF_BYTES = 2 * GRID_BYTES;   // 16 channels: one K step of 16
 constexpr int TILES = 5;                    // M tiles of 16 rows
 constexpr int WK_BYTES = 512;               // weights of one (tap, K step): 2 K groups x 16 co x 16 B
-constexpr int THREADS = 128;
+constexpr int THREADS = 256;             // 8 warps: warp w reads TMEM lanes 32 (w % 4).., channels 8 (w / 4)..
+constexpr int STG_BYTES = 16 * GS * 2;      // one raw chunk: 16 channels x 512 sites BF16
 constexpr int MAX_CIN = 64;
 constexpr int MAX_H = 64;
 constexpr int MAX_T = 256;
@@ -70,7 +73,8 @@ struct Args {
 
 __host__ __device__ constexpr size_t smem_bytes(int cin) {
   // weights (all layers) + 2 layer-1 input buffers + 1 activation buffer + pool/head scratch + barriers
-  return (size_t)27 * (cin / 16 + 2) * WK_BYTES + 3 * (size_t)BUF_BYTES + 16 * 4 + MAX_H * 4 + 64;
+  return (size_t)27 * (cin / 16 + 2) * WK_BYTES + 3 * (size_t)BUF_BYTES + 2 * (size_t)STG_BYTES + 16 * 4 +
+         MAX_H * 4 + 64;
 }
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -110,17 +114,14 @@ __device__ __forceinline__ void commit(uint64_t* bar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // byte offset of padded entry (x', y', z') of one channel group's grid
@@ -165,11 +166,15 @@ __global__ void __launch_bounds__(THREADS, 1) cv_forward_tc_kernel(Args g) {
   unsigned char* buf0 = wsm + (size_t)27 * (nks1 + 2) * WK_BYTES;
   unsigned char* buf1 = buf0 + BUF_BYTES;
   unsigned char* act = buf1 + BUF_BYTES;                      // layer-2 input (A1)
-  float* pool = reinterpret_cast<float*>(act + BUF_BYTES);    // [16]
+  unsigned char* stg0 = act + BUF_BYTES;                      // raw 16-channel chunks (bulk-copy landing zones)
+  unsigned char* stg1 = stg0 + STG_BYTES;
+  float* pool = reinterpret_cast<float*>(stg1 + STG_BYTES);   // [16]
   float* hid = pool + 16;                                     // [MAX_H]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(hid + MAX_H);  // [0], [1]: layer-1 buffers; [2]: layer done
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3);
+  // bars[0], [1]: MMAs of the layer-1 buffers; [2]: MMAs of layers 2, 3; [3], [4]: staged chunks landed
+  uint64_t* bars = reinterpret_cast<uint64_t*>(hid + MAX_H);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 5);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quad = warp & 3, half = warp >> 2;  // TMEM lanes 32 quad.., channels 8 half..
 
   // ---- one-time setup: weights in the operand layout, zeroed guard rows, barriers, TMEM
   const int wl_off[3] = {0, 27 * nks1 * WK_BYTES, 27 * (nks1 + 1) * WK_BYTES};
@@ -197,7 +202,7 @@ __global__ void __launch_bounds__(THREADS, 1) cv_forward_tc_kernel(Args g) {
     *reinterpret_cast<uint4*>(grid + (r ? 101 : 0) * ROW_BYTES + i * 16) = make_uint4(0, 0, 0, 0);
   }
   if (tid == 0) {
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 5; ++i)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(bars + i)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -213,11 +218,11 @@ __global__ void __launch_bounds__(THREADS, 1) cv_forward_tc_kernel(Args g) {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const uint32_t wbase = su32(wsm);
-  uint32_t ph[3] = {0, 0, 0};  // parities of the three barriers
-  int pending[3] = {0, 0, 0};  // commits on bars[0..2] not yet waited for
+  uint32_t ph[5] = {0, 0, 0, 0, 0};   // parities of the barriers
+  int pending[5] = {0, 0, 0, 0, 0};   // arrivals expected on bars[i] and not yet waited for
   bool ok = true;
-  // waits for the commit on bars[i]; the outcome is made block-uniform
-  auto wait_commit = [&](int i) {
+  // waits for the pending phase of bars[i]; the outcome is made block-uniform
+  auto wait_bar = [&](int i) {
     const bool done = bar_wait(bars + i, ph[i], g.err);
     if (done) {
       ph[i] ^= 1u;
@@ -226,9 +231,30 @@ __global__ void __launch_bounds__(THREADS, 1) cv_forward_tc_kernel(Args g) {
     return __syncthreads_and(done) != 0;
   };
 
-  // gathers channels c0 .. c0 + 15 of sample b into a padded buffer
-  auto fill = [&](unsigned char* dst, long b, int c0) {
-    const __nv_bfloat16* xs = g.x + ((size_t)b * g.Cin + c0) * GS;
+  // chunk q of this CTA: sample blockIdx.x + (q / nks1) gridDim.x, channels 16 (q % nks1) ..
+  const long n_chunks = g.B > blockIdx.x ? ((g.B - 1 - blockIdx.x) / gridDim.x + 1) * nks1 : 0;
+  auto chunk_src = [&](long q) {
+    const long b = blockIdx.x + (q / nks1) * (long)gridDim.x;
+    return reinterpret_cast<const unsigned char*>(g.x) + ((size_t)b * g.Cin + 16 * (q % nks1)) * GS * 2;
+  };
+  // one thread: bulk copy of chunk q (16 KiB contiguous) into stage q % 2
+  auto load_chunk = [&](long q) {
+    uint64_t* bar = bars + 3 + (q & 1);
+    unsigned char* dst = (q & 1) ? stg1 : stg0;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"((uint32_t)STG_BYTES)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     su32(dst)),
+                 "l"(chunk_src(q)), "r"((uint32_t)STG_BYTES), "r"(su32(bar))
+                 : "memory");
+  };
+  if (tid == 0)
+    for (long q = 0; q < 2 && q < n_chunks; ++q) load_chunk(q);
+  for (long q = 0; q < 2 && q < n_chunks; ++q) pending[3 + q] = 1;
+
+  // staged chunk (16 channels x 512 sites) -> padded operand grid of 2 channel groups
+  auto transpose = [&](unsigned char* dst, const unsigned char* src) {
+    const unsigned short* xs = reinterpret_cast<const unsigned short*>(src);
     for (int e = tid; e < 2 * 1000; e += THREADS) {
       const int kg = e / 1000, p = e % 1000;
       const int xp = p / 100, yp = (p / 10) % 10, zp = p % 10;
@@ -236,73 +262,73 @@ __global__ void __launch_bounds__(THREADS, 1) cv_forward_tc_kernel(Args g) {
       const int s = z + G * (y + G * x);
       uint32_t pk[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const unsigned short lo = __bfloat16_as_ushort(xs[(size_t)(8 * kg + 2 * i) * GS + s]);
-        const unsigned short hi = __bfloat16_as_ushort(xs[(size_t)(8 * kg + 2 * i + 1) * GS + s]);
-        pk[i] = (uint32_t)lo | ((uint32_t)hi << 16);
-      }
+      for (int i = 0; i < 4; ++i)
+        pk[i] = (uint32_t)xs[(8 * kg + 2 * i) * GS + s] | ((uint32_t)xs[(8 * kg + 2 * i + 1) * GS + s] << 16);
       *reinterpret_cast<uint4*>(dst + kg * GRID_BYTES + entry_off(xp, yp, zp)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
   };
 
-  // accumulators of this thread's row of tile j -> bias, tanh, BF16
+  // accumulators of this thread's row and channel half of tile j -> bias, tanh, BF16
   auto activations = [&](int j, const float* bias, float* a) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + 16 * j, a);
+    tmem_ld8(tmem + ((uint32_t)(32 * quad) << 16) + 16 * j + 8 * half, a);
 #pragma unroll
-    for (int co = 0; co < C; ++co) a[co] = __bfloat162float(__float2bfloat16(tanhf(a[co] + bias[co])));
+    for (int co = 0; co < 8; ++co) a[co] = __bfloat162float(__float2bfloat16(tanhf(a[co] + bias[co])));
   };
 
+  long q = 0;  // next chunk
   for (long b = blockIdx.x; b < g.B && ok; b += gridDim.x) {
-    // ---------------- layer 1: K steps of 16 channels through two buffers
-    for (int ks = 0; ks < nks1 && ok; ++ks) {
+    // ---------------- layer 1: K steps of 16 channels through two operand buffers
+    for (int ks = 0; ks < nks1 && ok; ++ks, ++q) {
       const int bi = ks & 1;
       unsigned char* buf = bi ? buf1 : buf0;
       if (pending[bi]) {  // the MMAs that read this buffer two steps ago
-        ok = wait_commit(bi);
+        ok = wait_bar(bi);
         if (!ok) break;
       }
-      fill(buf, b, 16 * ks);
+      ok = wait_bar(3 + (int)(q & 1));  // chunk q landed
+      if (!ok) break;
+      transpose(buf, (q & 1) ? stg1 : stg0);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
+        if (q + 2 < n_chunks) load_chunk(q + 2);  // the stage is free again
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         issue_layer_step(tmem, su32(buf), wbase + wl_off[0] + ks * WK_BYTES, nks1 * WK_BYTES, ks == 0);
         commit(bars + bi);
       }
+      if (q + 2 < n_chunks) pending[3 + (int)(q & 1)] = 1;
       pending[bi] = 1;
     }
     if (!ok) break;
     for (int bi = 0; bi < 2 && ok; ++bi)
-      if (pending[bi]) ok = wait_commit(bi);
+      if (pending[bi]) ok = wait_bar(bi);
     if (!ok) break;
     // ---------------- layers 2 and 3
     for (int layer = 1; layer < 3; ++layer) {
       // epilogue of the previous layer into the next input: A1 -> act, A2 -> buf0
       unsigned char* dst = layer == 1 ? act : buf0;
-      float bias[C];
+      float bias[8];
 #pragma unroll
-      for (int co = 0; co < C; ++co) bias[co] = __ldg(g.b[layer - 1] + co);
+      for (int co = 0; co < 8; ++co) bias[co] = __ldg(g.b[layer - 1] + 8 * half + co);
       for (int j = 0; j < TILES; ++j) {
-        float a[C];
+        float a[8];
         activations(j, bias, a);
-        const int r = 10 + 16 * j + 4 * warp + lane / 8, z = lane % 8;  // row m = 32 warp + lane
+        const int r = 10 + 16 * j + 4 * quad + lane / 8, z = lane % 8;  // row m = 32 quad + lane
         const int xp = r / 10, yp = r % 10;
         if (yp >= 1 && yp <= 8) {
-          uint32_t pk[8];
+          uint32_t pk[4];
 #pragma unroll
-          for (int i = 0; i < 8; ++i)
+          for (int i = 0; i < 4; ++i)
             pk[i] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16(a[2 * i])) |
                     ((uint32_t)__bfloat16_as_ushort(__float2bfloat16(a[2 * i + 1])) << 16);
           int cx[2], cy[2], cz[2];
           const int nx = copies(xp - 1, cx), ny = copies(yp - 1, cy), nz = copies(z, cz);
           for (int ix = 0; ix < nx; ++ix)
             for (int iy = 0; iy < ny; ++iy)
-              for (int iz = 0; iz < nz; ++iz) {
-                const int o = entry_off(cx[ix], cy[iy], cz[iz]);
-                *reinterpret_cast<uint4*>(dst + o) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                *reinterpret_cast<uint4*>(dst + GRID_BYTES + o) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-              }
+              for (int iz = 0; iz < nz; ++iz)
+                *reinterpret_cast<uint4*>(dst + half * GRID_BYTES + entry_off(cx[ix], cy[iy], cz[iz])) =
+                    make_uint4(pk[0], pk[1], pk[2], pk[3]);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -314,7 +340,7 @@ __global__ void __launch_bounds__(THREADS, 1) cv_forward_tc_kernel(Args g) {
         commit(bars + 2);
       }
       pending[2] = 1;
-      ok = wait_commit(2);
+      ok = wait_bar(2);
       if (!ok) break;
     }
     if (!ok) break;
@@ -322,26 +348,26 @@ __global__ void __launch_bounds__(THREADS, 1) cv_forward_tc_kernel(Args g) {
     if (tid < 16) pool[tid] = 0.0f;
     __syncthreads();
     {
-      float bias[C], sum[C];
+      float bias[8], sum[8];
 #pragma unroll
-      for (int co = 0; co < C; ++co) {
-        bias[co] = __ldg(g.b[2] + co);
+      for (int co = 0; co < 8; ++co) {
+        bias[co] = __ldg(g.b[2] + 8 * half + co);
         sum[co] = 0.0f;
       }
       for (int j = 0; j < TILES; ++j) {
-        float a[C];
+        float a[8];
         activations(j, bias, a);
-        const int r = 10 + 16 * j + 4 * warp + lane / 8;
+        const int r = 10 + 16 * j + 4 * quad + lane / 8;
         const int yp = r % 10;
         const bool valid = yp >= 1 && yp <= 8;
 #pragma unroll
-        for (int co = 0; co < C; ++co) sum[co] += valid ? a[co] : 0.0f;
+        for (int co = 0; co < 8; ++co) sum[co] += valid ? a[co] : 0.0f;
       }
 #pragma unroll
-      for (int co = 0; co < C; ++co) {
+      for (int co = 0; co < 8; ++co) {
         float v = sum[co];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) atomicAdd(pool + co, v);
+        if (lane == 0) atomicAdd(pool + 8 * half + co, v);
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -359,8 +385,8 @@ __global__ void __launch_bounds__(THREADS, 1) cv_forward_tc_kernel(Args g) {
     }
     __syncthreads();
   }
-  // ---- leave: no MMA may still be in flight (bounded drains), then free TMEM
-  for (int i = 0; i < 3; ++i)
+  // ---- leave: no MMA or bulk copy may still be in flight (bounded drains), then free TMEM
+  for (int i = 0; i < 5; ++i)
     if (pending[i]) bar_wait(bars + i, ph[i], g.err);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -385,6 +411,8 @@ extern "C" nrcps_status nrcps_cv_forward_tc(nrcps_context* ctx, const void* dev_
   NRCPS_REQUIRE(ctx, H > 0 && H <= cvtc::MAX_H && T > 0 && T <= cvtc::MAX_T && B >= 0 && dev_x && dev_W && dev_bias &&
                          dev_hw && dev_hb && dev_ow && dev_ob && dev_y,
                 "nrcps_cv_forward_tc: bad arguments");
+  NRCPS_REQUIRE(ctx, reinterpret_cast<uintptr_t>(dev_x) % 16 == 0,
+                "nrcps_cv_forward_tc: the features must start on a 16-byte boundary (bulk copies)");
   if (B == 0) return NRCPS_OK;
   cvtc::Args a{};
   a.x = reinterpret_cast<const __nv_bfloat16*>(dev_x);

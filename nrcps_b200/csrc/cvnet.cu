@@ -369,7 +369,7 @@ static size_t conv_fwd_smem(int Cin, int GS, int Cout) { return 2 * ((size_t)Cin
 extern "C" nrcps_status nrcps_cv_coarse_z2(nrcps_context* ctx, const uint32_t* dev_bits, uint64_t bit0, int L, int T,
                                            int G, int B, void* dev_x) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, dev_bits && dev_x && L > 0 && G > 0 && L % G == 0 && T > 0 && B >= 0,
+  NRCPS_REQUIRE(ctx, ((dev_bits && dev_x) || B == 0) && L > 0 && G > 0 && L % G == 0 && T > 0 && B >= 0,
                 "nrcps_cv_coarse_z2: bad arguments (G must divide L)");
   const long total = (long)B * T * G * G * G;
   if (total == 0) return NRCPS_OK;
@@ -390,7 +390,7 @@ extern "C" nrcps_status nrcps_cv_coarse_z2(nrcps_context* ctx, const uint32_t* d
 extern "C" nrcps_status nrcps_cv_sample_z2_features(nrcps_context* ctx, uint64_t seed, uint64_t first, int L, int T,
                                                     int G, int B, void* dev_x) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, dev_x && L > 0 && G > 0 && L % G == 0 && T > 0 && B >= 0,
+  NRCPS_REQUIRE(ctx, (dev_x || B == 0) && L > 0 && G > 0 && L % G == 0 && T > 0 && B >= 0,
                 "nrcps_cv_sample_z2_features: bad arguments (G must divide L)");
   const int f = L / G;
   const long total = (long)B * T * G * G * G;

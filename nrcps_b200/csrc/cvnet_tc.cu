@@ -408,8 +408,8 @@ extern "C" nrcps_status nrcps_cv_forward_tc(nrcps_context* ctx, const void* dev_
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
   NRCPS_REQUIRE(ctx, G == cvtc::G && Cin > 0 && Cin % 16 == 0 && Cin <= cvtc::MAX_CIN,
                 "nrcps_cv_forward_tc: needs G = 8 and Cin a multiple of 16 up to 64");
-  NRCPS_REQUIRE(ctx, H > 0 && H <= cvtc::MAX_H && T > 0 && T <= cvtc::MAX_T && B >= 0 && dev_x && dev_W && dev_bias &&
-                         dev_hw && dev_hb && dev_ow && dev_ob && dev_y,
+  NRCPS_REQUIRE(ctx, H > 0 && H <= cvtc::MAX_H && T > 0 && T <= cvtc::MAX_T && B >= 0 && ((dev_x && dev_y) || B == 0) &&
+                         dev_W && dev_bias && dev_hw && dev_hb && dev_ow && dev_ob,
                 "nrcps_cv_forward_tc: bad arguments");
   NRCPS_REQUIRE(ctx, reinterpret_cast<uintptr_t>(dev_x) % 16 == 0,
                 "nrcps_cv_forward_tc: the features must start on a 16-byte boundary (bulk copies)");

@@ -102,7 +102,8 @@ using namespace nrcps;
 extern "C" nrcps_status nrcps_accumulate(nrcps_context* ctx, const double* dev_dets, int n_conf, int T, int nmeas,
                                          int mode, int n_cumulants, double* dev_corr, double* dev_z) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, dev_dets && dev_corr && n_conf >= 0 && T > 0 && nmeas > 0 && (mode == 0 || mode == 1),
+  NRCPS_REQUIRE(ctx, (dev_dets || n_conf == 0) && dev_corr && n_conf >= 0 && T > 0 && nmeas > 0 &&
+                         (mode == 0 || mode == 1),
                 "nrcps_accumulate: bad arguments");
   NRCPS_REQUIRE(ctx, n_cumulants >= 0 && n_cumulants <= 8 && (n_cumulants == 0 || dev_z),
                 "nrcps_accumulate: 0 <= n_cumulants <= 8 (z required when > 0)");

@@ -566,8 +566,9 @@ using namespace nrcps;
 extern "C" nrcps_status nrcps_overlap(nrcps_context* ctx, const double* dev_src, int ns, const void* dev_psi, int nt,
                                       int nconf, long vol, nrcps_precision prec, double* dev_S) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, dev_src && dev_psi && dev_S && ns >= 0 && nt >= 0 && nconf >= 0 && vol > 0,
-                "nrcps_overlap: bad arguments");
+  NRCPS_REQUIRE(ctx, ns >= 0 && nt >= 0 && nconf >= 0 && vol > 0, "nrcps_overlap: bad arguments");
+  if ((long)ns * nt * nconf == 0) return NRCPS_OK;  // empty batch: nothing to read or write
+  NRCPS_REQUIRE(ctx, dev_src && dev_psi && dev_S, "nrcps_overlap: null pointer");
   if (prec == NRCPS_F32 && ctx->overlap_tc && ns > 0 && nt > 0 && nconf > 0 && ((uintptr_t)dev_psi & 15) == 0 &&
       overlap_tc_supported(vol, ns, nt, nconf)) {
     const size_t need = overlap_tc_split_bytes(ns, vol);
@@ -590,8 +591,9 @@ extern "C" nrcps_status nrcps_overlap(nrcps_context* ctx, const double* dev_src,
 extern "C" nrcps_status nrcps_overlap_planewave(nrcps_context* ctx, const int* dev_index, int ns, const void* dev_psi,
                                                 int nt, int nconf, long vol, nrcps_precision prec, double* dev_S) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, dev_index && dev_psi && dev_S && ns >= 0 && nt >= 0 && nconf >= 0 && vol > 0,
-                "nrcps_overlap_planewave: bad arguments");
+  NRCPS_REQUIRE(ctx, ns >= 0 && nt >= 0 && nconf >= 0 && vol > 0, "nrcps_overlap_planewave: bad arguments");
+  if ((long)ns * nt * nconf == 0) return NRCPS_OK;
+  NRCPS_REQUIRE(ctx, dev_index && dev_psi && dev_S, "nrcps_overlap_planewave: null pointer");
   return gather_impl(ctx, dev_index, ns, dev_psi, nt, nconf, vol, prec, dev_S);
 }
 
@@ -599,8 +601,9 @@ extern "C" nrcps_status nrcps_pair_matrix(nrcps_context* ctx, const void* dev_ps
                                           int nconf, long vol, const double* dev_w, const int* dev_opposite,
                                           nrcps_precision prec, double* dev_phi) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_w && dev_opposite && dev_phi && n >= 0 && nconf >= 0 && vol > 0,
-                "nrcps_pair_matrix: bad arguments");
+  NRCPS_REQUIRE(ctx, n >= 0 && nconf >= 0 && vol > 0, "nrcps_pair_matrix: bad arguments");
+  if ((long)n * nconf == 0) return NRCPS_OK;
+  NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_w && dev_opposite && dev_phi, "nrcps_pair_matrix: null pointer");
   return pair_impl(ctx, dev_psi1, dev_psi2, n, nconf, vol, dev_w, dev_opposite, prec, dev_phi);
 }
 
@@ -609,11 +612,11 @@ extern "C" nrcps_status nrcps_shifted_pair_matrix(nrcps_context* ctx, const void
                                                   const double* dev_wl, const int* dev_opposite,
                                                   nrcps_precision prec, double* dev_phi) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_shift && dev_wl && dev_opposite && dev_phi && n >= 0 &&
-                         nconf >= 0 && vol > 0 && nterms > 0,
-                "nrcps_shifted_pair_matrix: bad arguments");
+  NRCPS_REQUIRE(ctx, n >= 0 && nconf >= 0 && vol > 0 && nterms > 0, "nrcps_shifted_pair_matrix: bad arguments");
   const long blocks = (long)nconf * n * n;
   if (blocks == 0) return NRCPS_OK;
+  NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_shift && dev_wl && dev_opposite && dev_phi,
+                "nrcps_shifted_pair_matrix: null pointer");
   if (prec == NRCPS_F64)
     shifted_pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(dev_psi1, dev_psi2, n, vol, nterms,
                                                                           dev_shift, dev_wl, dev_opposite, dev_phi);
@@ -650,8 +653,9 @@ extern "C" nrcps_status nrcps_pair_matrix_ptrs(nrcps_context* ctx, const double*
 extern "C" nrcps_status nrcps_slater_dets(nrcps_context* ctx, const double* dev_S, const double* dev_psi1, int N,
                                           int nconf, int mode, int log_det, double* dev_out) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, dev_S && dev_out && N > 0 && nconf >= 0 && (mode == 0 || (mode == 1 && dev_psi1)),
-                "nrcps_slater_dets: bad arguments");
+  NRCPS_REQUIRE(ctx, N > 0 && nconf >= 0 && (mode == 0 || mode == 1), "nrcps_slater_dets: bad arguments");
+  if (nconf == 0) return NRCPS_OK;
+  NRCPS_REQUIRE(ctx, dev_S && dev_out && (mode == 0 || dev_psi1), "nrcps_slater_dets: null pointer");
   const int nmeas = mode ? 2 * N : N;
   return slater_dets_dispatch(ctx, dev_S, dev_psi1, N, nconf, mode, log_det, dev_out, 2L * nmeas, 0, nullptr);
 }

@@ -230,7 +230,8 @@ using namespace nrcps;
 extern "C" nrcps_status nrcps_fft3d(nrcps_context* ctx, void* data, int batch, const int dims[3],
                                     nrcps_precision prec, int sign) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, data && dims && batch >= 0 && (sign == 1 || sign == -1), "nrcps_fft3d: bad arguments");
+  NRCPS_REQUIRE(ctx, (data || batch == 0) && dims && batch >= 0 && (sign == 1 || sign == -1),
+                "nrcps_fft3d: bad arguments");
   NRCPS_TRY(check_dims(ctx, dims));
   if (batch == 0) return NRCPS_OK;
   return fft3d_any(ctx, data, batch, dims, prec, sign);
@@ -239,7 +240,7 @@ extern "C" nrcps_status nrcps_fft3d(nrcps_context* ctx, void* data, int batch, c
 extern "C" nrcps_status nrcps_kinetic_evolve(nrcps_context* ctx, void* psi, int batch, long vol,
                                              const double* dev_xi, nrcps_precision prec) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, psi && dev_xi && batch >= 0 && vol > 0, "nrcps_kinetic_evolve: bad arguments");
+  NRCPS_REQUIRE(ctx, (psi || batch == 0) && dev_xi && batch >= 0 && vol > 0, "nrcps_kinetic_evolve: bad arguments");
   long n = vol * batch;
   if (n == 0) return NRCPS_OK;
   unsigned grid = grid_for(n, 256, (long)ctx->sm_count * 8);
@@ -252,7 +253,7 @@ extern "C" nrcps_status nrcps_kinetic_evolve(nrcps_context* ctx, void* psi, int 
 extern "C" nrcps_status nrcps_potential_evolve(nrcps_context* ctx, void* psi, int batch, const int dims[3],
                                                const double* dev_pot, nrcps_precision prec) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, psi && dev_pot && dims && batch >= 0, "nrcps_potential_evolve: bad arguments");
+  NRCPS_REQUIRE(ctx, (psi || batch == 0) && dev_pot && dims && batch >= 0, "nrcps_potential_evolve: bad arguments");
   NRCPS_TRY(check_dims(ctx, dims));
   long vol = vol_of(dims), n = vol * batch;
   if (n == 0) return NRCPS_OK;
@@ -268,7 +269,7 @@ extern "C" nrcps_status nrcps_potential_evolve(nrcps_context* ctx, void* psi, in
 extern "C" nrcps_status nrcps_interaction_evolve(nrcps_context* ctx, void* psi, int batch, const int dims[3],
                                                  const double* dev_fld, nrcps_precision prec) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, psi && dev_fld && dims && batch >= 0, "nrcps_interaction_evolve: bad arguments");
+  NRCPS_REQUIRE(ctx, (psi || batch == 0) && dev_fld && dims && batch >= 0, "nrcps_interaction_evolve: bad arguments");
   NRCPS_TRY(check_dims(ctx, dims));
   long vol = vol_of(dims), n = vol * batch;
   if (n == 0) return NRCPS_OK;
@@ -376,7 +377,7 @@ extern "C" nrcps_status nrcps_propagate(nrcps_context* ctx, void* psi, int batch
                                        const double* dev_kin, const nrcps_position_factor* w,
                                        nrcps_precision prec) {
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
-  NRCPS_REQUIRE(ctx, psi && dims && dev_kin && w && w->dev_field && batch > 0 && nconf >= 0,
+  NRCPS_REQUIRE(ctx, (psi || nconf == 0) && dims && dev_kin && w && w->dev_field && batch > 0 && nconf >= 0,
                 "nrcps_propagate: bad arguments");
   NRCPS_REQUIRE(ctx, w->field_mode >= 0 && w->field_mode <= 2, "nrcps_propagate: bad field_mode");
   NRCPS_TRY(check_dims(ctx, dims));

@@ -943,8 +943,10 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   if (cs != cudaStreamCaptureStatusNone) return NRCPS_OK;  // keep the default
   const long V = (long)L * L * L;
   const size_t esz = prec == NRCPS_F64 ? 16 : 8;
-  long norb = (long)(512L * 1024 * 1024 / (V * esz));  // ~512 MB: larger than L2
-  if (norb > 4096) norb = 4096;
+  // ~2 GB (16x L2), up to 8192 orbitals: at 2048 orbitals the ranking of the
+  // L=32 variants differed from the one at production batch sizes
+  long norb = (long)(2048L * 1024 * 1024 / (V * esz));
+  if (norb > 8192) norb = 8192;
   if (norb < 8) norb = 8;
   void* psi = nullptr;
   void* kin = nullptr;

@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--split", type=int, default=-1, help="fused kernel lane split: -1 autotuned, 0, 1")
     ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 peer access, 1 split, 2 bulk staged, 3 bulk L2, 4-6 packed 0/2/3, 7/8 peer access L2, 9/10 kinds 6/3 with k(p) in shared memory")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU path measurement")
-    ap.add_argument("--qr", type=int, default=-1, help="re-orthonormalise every k slices (-1: 32 for f32, 0 for f64)")
+    ap.add_argument("--qr", type=int, default=-1, help="re-orthonormalise every k slices (-1: 8 for f32, 0 for f64)")
     ap.add_argument("--workload", default="batched", choices=["batched", "uneven", "cv"],
                     help="batched: the L=32 ensemble (default); uneven: 512 jobs of random (L, N, T) in one launch; "
                          "cv: the learned control variate against the plain estimator")
@@ -68,11 +68,11 @@ def parse():
 
 
 def qr_period(a):
-    # FP32 orbitals are re-orthonormalised every 32 slices: at L=32, T=64, N=19 the
-    # FP32-vs-FP64 error of C_n(tau) is 1.2e-6 (QR every 8), 1.9e-6 (16),
-    # 1.5e-6 (32) and 1.7e-6 (never), all far inside 1e-5, while every QR costs
-    # one read and one read + write of the orbitals
-    return a.qr if a.qr >= 0 else (32 if a.precision == "f32" else 0)
+    # FP32 orbitals are re-orthonormalised every 8 slices, as the batched L=32
+    # workload prescribes (--qr changes it: at L=32, T=64, N=19 the FP32-vs-FP64
+    # error of C_n(tau) is 1.2e-6 every 8, 1.9e-6 every 16, 1.5e-6 every 32 and
+    # 1.7e-6 never)
+    return a.qr if a.qr >= 0 else (8 if a.precision == "f32" else 0)
 
 
 def workload(a, n_orb):

@@ -208,7 +208,7 @@ __global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double
 // all N orbitals of a configuration in registers (N <= 64), arithmetic in R
 // (FP32 orbitals: Rinv rounded to FP32, see chol_inv_kernel).
 template <typename R, int NMAX>
-__global__ void __launch_bounds__(128) apply_rinv_kernel(void* __restrict__ psi, int N, long vol, int nconf,
+__global__ void __launch_bounds__(256) apply_rinv_kernel(void* __restrict__ psi, int N, long vol, int nconf,
                                                           const double* __restrict__ Rinv) {
   extern __shared__ double rs_raw[];  // 2 N^2 values of R of this block's configuration
   R* rs = reinterpret_cast<R*>(rs_raw);
@@ -217,18 +217,20 @@ __global__ void __launch_bounds__(128) apply_rinv_kernel(void* __restrict__ psi,
   const long c = blockIdx.x / blocks_per_conf;
   if (c >= nconf) return;
   const long p = (blockIdx.x % blocks_per_conf) * sites_per_block + threadIdx.x;
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) rs[e] = (R)Rinv[2L * c * N * N + e];
-  __syncthreads();
-  if (p >= vol) return;
-  cplx<R>* base = reinterpret_cast<cplx<R>*>(psi) + (size_t)c * N * vol + p;
+  const bool live = p < vol;
+  cplx<R>* base = reinterpret_cast<cplx<R>*>(psi) + (size_t)c * N * vol + (live ? p : 0);
+  // the orbital loads go out first; their latency covers the fill of R below
   R xr[NMAX], xi[NMAX];
 #pragma unroll
   for (int i = 0; i < NMAX; ++i)
-    if (i < N) {
+    if (i < N && live) {
       cplx<R> v = base[(size_t)i * vol];
       xr[i] = v.re;
       xi[i] = v.im;
     }
+  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) rs[e] = (R)Rinv[2L * c * N * N + e];
+  __syncthreads();
+  if (!live) return;
 #pragma unroll
   for (int t = NMAX - 1; t >= 0; --t) {
     if (t >= N) continue;
@@ -262,12 +264,12 @@ __global__ void rescale_dets_kernel(double* dets, const double* logR, int N, int
 template <int NMAX>
 static nrcps_status launch_apply(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
                                  const double* Rinv) {
-  const long bpc = (vol + 127) / 128;
+  const long bpc = (vol + 255) / 256;
   const size_t sh = sizeof(double) * 2 * N * N;
   if (prec == NRCPS_F64)
-    apply_rinv_kernel<double, NMAX><<<(unsigned)(bpc * nconf), 128, sh, ctx->stream>>>(psi, N, vol, nconf, Rinv);
+    apply_rinv_kernel<double, NMAX><<<(unsigned)(bpc * nconf), 256, sh, ctx->stream>>>(psi, N, vol, nconf, Rinv);
   else
-    apply_rinv_kernel<float, NMAX><<<(unsigned)(bpc * nconf), 128, sh, ctx->stream>>>(psi, N, vol, nconf, Rinv);
+    apply_rinv_kernel<float, NMAX><<<(unsigned)(bpc * nconf), 256, sh, ctx->stream>>>(psi, N, vol, nconf, Rinv);
   ctx->launches++;
   return check_launch(ctx, "apply_rinv_kernel");
 }

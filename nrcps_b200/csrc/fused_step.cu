@@ -930,6 +930,29 @@ bool fused_supported(nrcps_precision prec, const int d[3]) {
 
 // Times every cluster size for (prec, L) on a scratch batch and records the
 // fastest.  Runs outside graph capture (it allocates and synchronises).
+// Scratch orbitals for the autotuner: values of order one that vary from
+// word to word (all-zero buffers move through the memory system differently
+// from real orbitals), k(p) = 1 and a half-filled Z2 field.
+__global__ void autotune_fill_kernel(uint32_t* words, long n_words, int fp64) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_words; i += (long)gridDim.x * blockDim.x) {
+    uint32_t h = (uint32_t)i * 0x9E3779B1u;
+    h ^= h >> 15;
+    h *= 0x85EBCA77u;
+    h ^= h >> 13;
+    // FP32: a float in [0.5, 1) with random mantissa and sign; FP64: keep the
+    // high word of each double in [0.5, 1) the same way, the low word random
+    if (!fp64 || (i & 1)) words[i] = 0x3F000000u | (h & 0x807FFFFFu);
+    else words[i] = h;
+  }
+}
+
+__global__ void autotune_unit_kin_kernel(void* kin, long V, int fp64) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V; i += (long)gridDim.x * blockDim.x) {
+    if (fp64) reinterpret_cast<double*>(kin)[i] = 1.0;
+    else reinterpret_cast<float2*>(kin)[i] = make_float2(1.0f, 0.0f);
+  }
+}
+
 nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster) {
   init_choices();
   int dev = ctx->device & 15;
@@ -960,9 +983,14 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
     if (kin) cudaFree(kin);
     return NRCPS_OK;  // keep the default choice
   }
-  cudaMemsetAsync(psi, 0, esz * V * norb, ctx->stream);
-  cudaMemsetAsync(kin, 0, esz * V, ctx->stream);
-  cudaMemsetAsync(bits, 0, (size_t)(V / 32 + 1) * 4, ctx->stream);
+  {
+    const long n_words = (long)(esz / 4) * V * norb;
+    autotune_fill_kernel<<<grid_for(n_words, 256, (long)ctx->sm_count * 8), 256, 0, ctx->stream>>>(
+        reinterpret_cast<uint32_t*>(psi), n_words, prec == NRCPS_F64 ? 1 : 0);
+  }
+  autotune_unit_kin_kernel<<<grid_for(V, 256, (long)ctx->sm_count * 8), 256, 0, ctx->stream>>>(
+      kin, V, prec == NRCPS_F64 ? 1 : 0);
+  cudaMemsetAsync(bits, 0x5A, (size_t)(V / 32 + 1) * 4, ctx->stream);
   FusedArgs f{};
   f.psi = psi;
   f.n_orb_total = norb;
@@ -971,10 +999,12 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   f.kin_d = (const double*)kin;
   f.field_mode = 1;
   f.field = bits;
-  f.a = 0.5;
+  // a = 0 with k = 1: the step preserves the norm, so the ~100 timing
+  // launches on the same buffer keep the values of order one
+  f.a = 0.0;
   f.vol = (double)V;
-  f.w_plus = 1.5 / V;
-  f.w_minus = 0.5 / V;
+  f.w_plus = 1.0 / V;
+  f.w_minus = 1.0 / V;
   f.err = ctx->dev_err;
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);

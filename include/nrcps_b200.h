@@ -408,6 +408,17 @@ nrcps_status nrcps_branch_create(nrcps_context *ctx, const nrcps_branch_params *
 nrcps_status nrcps_branch_run(nrcps_branch *branch, double *dev_corr);
 nrcps_status nrcps_branch_destroy(nrcps_branch *branch);
 
+/* CholeskyQR of every configuration's orbital block, in place:
+ * Psi = Q R (G = Psi^H Psi accumulated in FP64, Cholesky and R^-1 in FP64,
+ * Psi <- Psi R^-1), dev_logR[c][i] += log R_ii (FP32 orbitals: -log of the
+ * FP32-rounded (R^-1)_ii that was applied).  The reference's only
+ * stabilisation is a norm rescale (Propagator::Normalize,
+ * src/alg/propagator.C:78-135); the ensemble runners call this every
+ * qr_period slices.  dev_psi [nconf][N][vol]; dev_work: 2 nconf N^2 doubles
+ * of scratch; N <= 64. */
+nrcps_status nrcps_reorthonormalise(nrcps_context *ctx, void *dev_psi, int N, long vol, int nconf,
+                                    nrcps_precision prec, double *dev_work, double *dev_logR);
+
 /* ------------------------------------------- learned control variate
  * Kernels of the control-variate network (no counterpart in the reference;
  * nrcps_b200/cv.py drives them): a 3-layer 3x3x3 periodic convolution net

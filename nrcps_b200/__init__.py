@@ -10,7 +10,7 @@ this package only binds it.  Build with ``python -m nrcps_b200.build``.
 """
 from ._capi import NrcpsError, lib  # noqa: F401
 from .api import (  # noqa: F401
-    Batch, BatchJob, Branching, Context, GeneralizedTwoBody, Ensemble, EnsembleJob, accumulate, jackknife, Fourier, Interaction, Kinetic, Lattice, OneBody, Potential, Propagator,
+    Batch, BatchJob, Branching, Context, GeneralizedTwoBody, Ensemble, EnsembleJob, accumulate, jackknife, reorthonormalise, Fourier, Interaction, Kinetic, Lattice, OneBody, Potential, Propagator,
     Random, SlaterDet, TwoBody, cutoff_sq, default_context, dispersion_table, draw_fields, draw_z2_bits,
     interaction_table, kinetic_table, momenta, overlap, propagate, overlap_planewave, potential_table, rng_seed_state,
     rng_skip, sho_source, slater_dets, two_body_tables, uniforms,

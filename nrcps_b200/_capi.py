@@ -122,6 +122,7 @@ SIGNATURES = {
     "nrcps_branch_destroy": ([_P], _I),
     "nrcps_cv_coarse_z2": ([_P, _P, _U64, _I, _I, _I, _I, _P], _I),
     "nrcps_cv_sample_z2_features": ([_P, _U64, _U64, _I, _I, _I, _I, _P], _I),
+    "nrcps_reorthonormalise": ([_P, _P, _I, ctypes.c_long, _I, _I, _P, _P], _I),
     "nrcps_cv_forward_tc": ([_P, _P, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _I, _P], _I),
     "nrcps_cv_conv_forward": ([_P, _P, _I, _I, _I, _I, _P, _P, _P, _P], _I),
     "nrcps_cv_conv_backward": ([_P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P], _I),

@@ -474,6 +474,24 @@ def slater_dets(S: torch.Tensor, psi1: Optional[torch.Tensor] = None, mode: int 
     return out
 
 
+def reorthonormalise(psi: torch.Tensor, logR: Optional[torch.Tensor] = None,
+                     ctx: Optional[Context] = None) -> torch.Tensor:
+    """CholeskyQR in place of psi [nconf, N, V] (complex64 or complex128):
+    psi <- psi R^-1; returns logR [nconf, N] (FP64) with log R_ii added."""
+    ctx = ctx or default_context()
+    nconf, N = psi.shape[0], psi.shape[1]
+    vol = psi[0, 0].numel()
+    if not psi.is_contiguous():
+        raise ValueError("reorthonormalise works in place on a contiguous tensor")
+    if logR is None:
+        logR = torch.zeros((nconf, N), dtype=torch.float64, device=ctx.device)
+    work = torch.empty((nconf, N, N, 2), dtype=torch.float64, device=ctx.device)
+    prec = C.F64 if psi.dtype == torch.complex128 else C.F32
+    ctx.check(lib().nrcps_reorthonormalise(ctx.handle, _ptr(psi), N, vol, nconf, prec, _ptr(work), _ptr(logR)),
+              "reorthonormalise")
+    return logR
+
+
 def accumulate(dets: torch.Tensor, mode: str = "slater", n_cumulants: int = 0, ctx: Optional[Context] = None):
     """Block sums of the production drivers on the device (FP64):
     corr [nmeas, T] complex = sum_c |det|^2 (mode 'slater', main.C:208-211) or

@@ -207,8 +207,9 @@ __global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double
 // Register-blocked variant for FP32 orbitals and N <= 20: thread (pair, g)
 // accumulates one 4 x 4 block (rows 4 bi.., columns 4 bj.., bi <= bj) of G
 // over the sites g, g + NG, .. of every tile -- 8 shared-memory loads per 64
-// FMAs instead of 4 per 16 -- and the NG = 16 site groups of a pair (16
-// adjacent lanes of one warp) are summed by shuffles in FP64 at the end.
+// FMAs instead of 4 per 16 -- in FP32 over 32 sites (4 tiles), then in FP64;
+// the NG = 16 site groups of a pair (16 adjacent lanes of one warp) are
+// summed by shuffles in FP64 at the end.
 // Tile rows N .. 19 are zero, so partial blocks need no special case.
 constexpr int G4_ROWS = 20;  // 5 row blocks of 4
 constexpr int G4_NG = 16;    // site groups per block pair
@@ -241,12 +242,17 @@ __global__ void __launch_bounds__(256) gram4_kernel(const void* __restrict__ psi
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
+  // FP32 partial sums over 4 tiles (32 sites per thread), then FP64
   double acc[32];
+  float s[32];
 #pragma unroll
-  for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+  for (int k = 0; k < 32; ++k) {
+    acc[k] = 0.0;
+    s[k] = 0.f;
+  }
   fill(0, tiles);
-  int buf = 0;
-  for (long p0 = 0; p0 < vol; p0 += GT, buf ^= 1) {
+  int buf = 0, ntile = 0;
+  for (long p0 = 0; p0 < vol; p0 += GT, buf ^= 1, ++ntile) {
     const float2* tile = tiles + buf * TS;
     __syncthreads();  // every thread is done with the tile the next copies overwrite
     if (p0 + GT < vol) fill(p0 + GT, tiles + (buf ^ 1) * TS);
@@ -254,9 +260,6 @@ __global__ void __launch_bounds__(256) gram4_kernel(const void* __restrict__ psi
     asm volatile("cp.async.wait_group 1;" ::: "memory");
     __syncthreads();
     if (active) {
-      float s[32];
-#pragma unroll
-      for (int k = 0; k < 32; ++k) s[k] = 0.f;
       for (int q = g; q < GT; q += G4_NG) {
         float2 a[4], b[4];
 #pragma unroll
@@ -272,8 +275,13 @@ __global__ void __launch_bounds__(256) gram4_kernel(const void* __restrict__ psi
             s[2 * (4 * u + v) + 1] += a[u].x * b[v].y - a[u].y * b[v].x;
           }
       }
+      if ((ntile & 3) == 3 || p0 + GT >= vol) {
 #pragma unroll
-      for (int k = 0; k < 32; ++k) acc[k] += (double)s[k];
+        for (int k = 0; k < 32; ++k) {
+          acc[k] += (double)s[k];
+          s[k] = 0.f;
+        }
+      }
     }
   }
   // sum the 16 site groups of a pair (adjacent lanes) and write the upper triangle

@@ -5,6 +5,7 @@ context's stream, after warm-up), one JSON line per measurement.
     python -m nrcps_b200.kernel_bench overlap --L 32 --ns 19 --nconf 1024 [--tc 1|0]
     python -m nrcps_b200.kernel_bench dets    --N 19 --nconf 4096
     python -m nrcps_b200.kernel_bench cv      --T 64 --batch 256
+    python -m nrcps_b200.kernel_bench qr      --L 32 --N 19 --nconf 1024 [--precision f32]
 
 step:    one transfer-matrix step (nrcps_propagate, Z2 field, a = 0.5) over
          `orbitals` orbitals in batches of 19; GB/s counts one read and one
@@ -16,6 +17,9 @@ dets:    determinants of all N leading minors of nconf FP64 matrices.
 cv:      one training step (forward, backward, Adam) and one inference pass
          of the control-variate network on random inputs; TFLOP/s counts the
          conv multiply-adds (2 flops each; backward twice the forward).
+qr:      one CholeskyQR re-orthonormalisation (nrcps_reorthonormalise) of
+         nconf configurations of N orbitals; GB/s counts the algorithmic
+         three passes over the orbitals (Gram read, apply read + write).
 """
 from __future__ import annotations
 
@@ -28,7 +32,7 @@ import torch
 
 from . import _capi as C
 from ._capi import lib
-from .api import Context, draw_z2_bits, kinetic_table, overlap, slater_dets
+from .api import Context, draw_z2_bits, kinetic_table, overlap, reorthonormalise, slater_dets
 
 
 def _time(fn, reps: int, warmup: int = 2) -> float:
@@ -134,9 +138,20 @@ def bench_cv(ctx: Context, T: int, batch: int, reps: int) -> dict:
             "coarse_ms": round(ms_coarse, 4), "coarse_GBs": round(nbits / 8 / ms_coarse / 1e6, 1)}
 
 
+def bench_qr(ctx: Context, L: int, N: int, nconf: int, precision: str, reps: int) -> dict:
+    dt = torch.complex64 if precision == "f32" else torch.complex128
+    g = torch.Generator(device=ctx.device).manual_seed(11)
+    psi = torch.randn((nconf, N, L ** 3), dtype=dt, device=ctx.device, generator=g)
+    logR = torch.zeros((nconf, N), dtype=torch.float64, device=ctx.device)
+    ms = _time(lambda: reorthonormalise(psi, logR, ctx), reps)
+    nbytes = 3 * psi.numel() * psi.element_size()
+    return {"kernel": "qr", "L": L, "N": N, "nconf": nconf, "precision": precision, "ms": round(ms, 4),
+            "GBps": round(nbytes / ms / 1e6, 1)}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["step", "overlap", "dets", "cv"])
+    ap.add_argument("what", choices=["step", "overlap", "dets", "cv", "qr"])
     ap.add_argument("--L", type=int, default=32)
     ap.add_argument("--orbitals", type=int, default=19456)
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
@@ -157,6 +172,8 @@ def main(argv=None) -> int:
         r = bench_overlap(ctx, a.L, a.ns, a.nconf, a.tc, a.reps)
     elif a.what == "cv":
         r = bench_cv(ctx, a.T, a.batch, a.reps)
+    elif a.what == "qr":
+        r = bench_qr(ctx, a.L, a.N, a.nconf, a.precision, a.reps)
     else:
         r = bench_dets(ctx, a.N, a.nconf, a.reps)
     print(json.dumps(r), flush=True)

@@ -207,13 +207,14 @@ __global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double
 // Register-blocked variant for FP32 orbitals and N <= 20: thread (pair, g)
 // accumulates one 4 x 4 block (rows 4 bi.., columns 4 bj.., bi <= bj) of G
 // over the sites g, g + NG, .. of every tile -- 8 shared-memory loads per 64
-// FMAs instead of 4 per 16 -- in FP32 over 32 sites (4 tiles), then in FP64;
+// FMAs instead of 4 per 16, as packed FP32x2 FMAs -- in FP32 over 32 sites
+// (4 tiles), then in FP64;
 // the NG = 16 site groups of a pair (16 adjacent lanes of one warp) are
 // summed by shuffles in FP64 at the end.
 // Tile rows N .. 19 are zero, so partial blocks need no special case.
 constexpr int G4_ROWS = 20;  // 5 row blocks of 4
 constexpr int G4_NG = 16;    // site groups per block pair
-__global__ void __launch_bounds__(256) gram4_kernel(const void* __restrict__ psi, int N, long vol,
+__global__ void __launch_bounds__(256, 2) gram4_kernel(const void* __restrict__ psi, int N, long vol,
                                                   double* __restrict__ G) {
   extern __shared__ __align__(16) unsigned char gsm[];
   float2* tiles = reinterpret_cast<float2*>(gsm);  // [2][G4_ROWS][GT + 1]
@@ -244,12 +245,11 @@ __global__ void __launch_bounds__(256) gram4_kernel(const void* __restrict__ psi
   };
   // FP32 partial sums over 4 tiles (32 sites per thread), then FP64
   double acc[32];
-  float s[32];
+  float2 s[16];  // (re, im) of the 4 x 4 block, FP32 over 4 tiles
 #pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    acc[k] = 0.0;
-    s[k] = 0.f;
-  }
+  for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s[k] = make_float2(0.f, 0.f);
   fill(0, tiles);
   int buf = 0, ntile = 0;
   for (long p0 = 0; p0 < vol; p0 += GT, buf ^= 1, ++ntile) {
@@ -260,26 +260,34 @@ __global__ void __launch_bounds__(256) gram4_kernel(const void* __restrict__ psi
     asm volatile("cp.async.wait_group 1;" ::: "memory");
     __syncthreads();
     if (active) {
-      for (int q = g; q < GT; q += G4_NG) {
-        float2 a[4], b[4];
+      const float2* ta = tile + 4 * bi * (GT + 1) + g;
+      const float2* tb = tile + 4 * bj * (GT + 1) + g;
+#pragma unroll
+      for (int k = 0; k < GT / G4_NG; ++k) {
+        float2 a[4], b[4], bn[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          a[u] = tile[(4 * bi + u) * (GT + 1) + q];
-          b[u] = tile[(4 * bj + u) * (GT + 1) + q];
+          a[u] = ta[u * (GT + 1) + G4_NG * k];
+          b[u] = tb[u * (GT + 1) + G4_NG * k];
+          bn[u] = make_float2(b[u].y, -b[u].x);
         }
+        // conj(a_u) b_v = (a.x b.x + a.y b.y, a.x b.y - a.y b.x): two packed FMAs
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 4; ++u) {
+          const float2 ax = make_float2(a[u].x, a[u].x), ay = make_float2(a[u].y, a[u].y);
 #pragma unroll
-          for (int v = 0; v < 4; ++v) {  // conj(a_u) b_v
-            s[2 * (4 * u + v)] += a[u].x * b[v].x + a[u].y * b[v].y;
-            s[2 * (4 * u + v) + 1] += a[u].x * b[v].y - a[u].y * b[v].x;
+          for (int v = 0; v < 4; ++v) {
+            s[4 * u + v] = __ffma2_rn(ax, b[v], s[4 * u + v]);
+            s[4 * u + v] = __ffma2_rn(ay, bn[v], s[4 * u + v]);
           }
+        }
       }
       if ((ntile & 3) == 3 || p0 + GT >= vol) {
 #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          acc[k] += (double)s[k];
-          s[k] = 0.f;
+        for (int k = 0; k < 16; ++k) {
+          acc[2 * k] += (double)s[k].x;
+          acc[2 * k + 1] += (double)s[k].y;
+          s[k] = make_float2(0.f, 0.f);
         }
       }
     }

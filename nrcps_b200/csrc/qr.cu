@@ -313,7 +313,9 @@ __global__ void __launch_bounds__(256, 2) gram4_kernel(const void* __restrict__ 
 template <typename R, int NMAX>
 __global__ void __launch_bounds__(256) apply_rinv_kernel(void* __restrict__ psi, int N, long vol, int nconf,
                                                           const double* __restrict__ Rinv) {
-  extern __shared__ double rs_raw[];  // 2 N^2 values of R of this block's configuration
+  // R^-1 of this block's configuration: 2 N^2 values in R (FP64), or for FP32
+  // N^2 float4 (re, re, im, im) entries that feed packed FMAs
+  extern __shared__ __align__(16) double rs_raw[];
   R* rs = reinterpret_cast<R*>(rs_raw);
   const long sites_per_block = blockDim.x;
   const long blocks_per_conf = (vol + sites_per_block - 1) / sites_per_block;
@@ -331,20 +333,45 @@ __global__ void __launch_bounds__(256) apply_rinv_kernel(void* __restrict__ psi,
       xr[i] = v.re;
       xi[i] = v.im;
     }
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) rs[e] = (R)Rinv[2L * c * N * N + e];
-  __syncthreads();
-  if (!live) return;
-#pragma unroll
-  for (int t = NMAX - 1; t >= 0; --t) {
-    if (t >= N) continue;
-    R sr = 0, si = 0;
-#pragma unroll
-    for (int i = 0; i <= t; ++i) {
-      const R ar = rs[2 * (i * N + t)], ai = rs[2 * (i * N + t) + 1];
-      sr += xr[i] * ar - xi[i] * ai;
-      si += xr[i] * ai + xi[i] * ar;
+  if constexpr (sizeof(R) == 4) {
+    // x r = (xr ar - xi ai, xr ai + xi ar): with X = (xr, xi) the packed sums
+    // s = sum X (ar, ar) and u = sum X (ai, ai) give re = s.x - u.y, im = s.y + u.x
+    float4* r4 = reinterpret_cast<float4*>(rs_raw);
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+      const float ar = (float)Rinv[2L * (c * N * N + e)], ai = (float)Rinv[2L * (c * N * N + e) + 1];
+      r4[e] = make_float4(ar, ar, ai, ai);
     }
-    base[(size_t)t * vol] = cplx<R>{(R)sr, (R)si};
+    __syncthreads();
+    if (!live) return;
+#pragma unroll
+    for (int t = NMAX - 1; t >= 0; --t) {
+      if (t >= N) continue;
+      float2 sa = make_float2(0.f, 0.f), ua = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int i = 0; i <= t; ++i) {
+        const float4 r = r4[i * N + t];
+        const float2 x = make_float2(xr[i], xi[i]);
+        sa = __ffma2_rn(x, make_float2(r.x, r.y), sa);
+        ua = __ffma2_rn(x, make_float2(r.z, r.w), ua);
+      }
+      base[(size_t)t * vol] = cplx<R>{sa.x - ua.y, sa.y + ua.x};
+    }
+  } else {
+    for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) rs[e] = (R)Rinv[2L * c * N * N + e];
+    __syncthreads();
+    if (!live) return;
+#pragma unroll
+    for (int t = NMAX - 1; t >= 0; --t) {
+      if (t >= N) continue;
+      R sr = 0, si = 0;
+#pragma unroll
+      for (int i = 0; i <= t; ++i) {
+        const R ar = rs[2 * (i * N + t)], ai = rs[2 * (i * N + t) + 1];
+        sr += xr[i] * ar - xi[i] * ai;
+        si += xr[i] * ai + xi[i] * ar;
+      }
+      base[(size_t)t * vol] = cplx<R>{(R)sr, (R)si};
+    }
   }
 }
 

@@ -51,19 +51,18 @@ __host__ __device__ __forceinline__ cplx<R> cmul(cplx<R> a, cplx<R> b) {
   return cplx<R>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
 
-// x * (hi + lo) for a real factor carried as two floats in FP32.  The
-// product p = x*hi is split error-free (e = fma(x, hi, -p) is exact) and the
-// remainder e + x*lo is added before the single final rounding, so the
-// result is the correctly rounded x*(hi + lo).  A plain x*k with k rounded to
-// one float -- or fma(x, lo, x*hi), which rounds x*hi first and so loses lo
-// -- scales a mode by the same wrong factor every step: a deterministic drift
-// of ~1e-8 per application that reaches ~5e-6 in |det|^2 after 32 steps.
+// x * (hi + lo) for a real factor carried as two floats in FP32:
+// fma(x, hi, x*lo) adds the small product before the single rounding of the
+// sum.  Rounding x*lo first costs at most 2^-24 |x lo| <= 2^-48 |x hi|, so
+// the result is the correctly rounded x*(hi + lo) but for sums within 2^-48
+// of a rounding boundary.  A plain x*k with k rounded to one float -- or
+// fma(x, lo, x*hi), which rounds x*hi first and so loses lo -- scales a mode
+// by the same wrong factor every step: a deterministic drift of ~1e-8 per
+// application that reaches ~5e-6 in |det|^2 after 32 steps.
 template <typename R>
 __host__ __device__ __forceinline__ R mul2(R x, R hi, R lo) {
   if constexpr (sizeof(R) == 4) {
-    float p = x * hi;
-    float e = fmaf(x, hi, -p);
-    return p + fmaf(x, lo, e);
+    return fmaf(x, hi, x * lo);
   } else {
     return x * hi;
   }

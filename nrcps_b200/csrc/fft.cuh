@@ -143,6 +143,18 @@ __device__ __forceinline__ cplx<R> twiddle(cplx<R> x) {
     if constexpr (qs == 1) return cplx<R>{-x.im, x.re};
     else if constexpr (qs == 2) return cplx<R>{-x.re, -x.im};
     else return cplx<R>{x.im, -x.re};
+  } else if constexpr (sizeof(R) == 4 && (8 * k) % N == 0) {
+    // an odd multiple of pi/4: |cos| = |sin| = m, so
+    // x w = m (cs x.re - ss x.im) + i m (ss x.re + cs x.im) with the signs
+    // cs, ss of cos and sin: two adds and two products by m = hi + lo
+    constexpr CS w = unit_root(k, N);
+    constexpr double sd = SIGN > 0 ? w.s : -w.s;
+    constexpr double m = w.c > 0 ? w.c : -w.c;
+    constexpr float mh = (float)m, ml = (float)(m - (double)(float)m);
+    constexpr float cs = w.c > 0 ? 1.f : -1.f, ss = sd > 0 ? 1.f : -1.f;
+    const float a = cs * x.re - ss * x.im;
+    const float b = ss * x.re + cs * x.im;
+    return cplx<R>{fmaf(a, mh, a * ml), fmaf(b, mh, b * ml)};
   } else {
     if constexpr (sizeof(R) == 4) {
       // The root carried as an unevaluated float pair hi + lo (exact to
@@ -425,15 +437,11 @@ __device__ __forceinline__ void dft(cplx<R>* x) {
   else Dft<N, SIGN, R>::run(x);
 }
 
-// x * (hi + lo) on both components at once, correctly rounded as mul2:
-// q = -x hi (exact negation of the rounded product), e = x hi + q exactly,
-// result = (x lo + e) - q with one rounding each.
+// x * (hi + lo) on both components at once, as mul2: fma(x, hi, x lo).
 __device__ __forceinline__ cplx<float> scale2_packed(cplx<float> x, float hi, float lo) {
   const float2 v = make_float2(x.re, x.im);
-  const float2 q = __fmul2_rn(v, make_float2(-hi, -hi));
-  const float2 e = __ffma2_rn(v, make_float2(hi, hi), q);
-  const float2 g = __ffma2_rn(v, make_float2(lo, lo), e);
-  const float2 r = __ffma2_rn(q, make_float2(-1.f, -1.f), g);
+  const float2 g = __fmul2_rn(v, make_float2(lo, lo));
+  const float2 r = __ffma2_rn(v, make_float2(hi, hi), g);
   return cplx<float>{r.x, r.y};
 }
 

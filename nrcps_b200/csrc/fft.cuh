@@ -304,6 +304,19 @@ __device__ __forceinline__ cpk ptwiddle(cpk x) {
     if constexpr (qs == 1) return cpk{psub(z, x.im), x.re};
     else if constexpr (qs == 2) return cpk{psub(z, x.re), psub(z, x.im)};
     else return cpk{x.im, psub(z, x.re)};
+  } else if constexpr ((8 * k) % N == 0) {
+    // odd multiple of pi/4 as in twiddle() above, with the sign cs of the
+    // cosine folded into m: re = (cs m)(x.re - cs ss x.im), im = (cs m)(x.im + cs ss x.re)
+    constexpr CS w = unit_root(k, N);
+    constexpr double sd = SIGN > 0 ? w.s : -w.s;
+    constexpr double cm = w.c;  // cs m
+    constexpr float mh = (float)cm, ml = (float)(cm - (double)(float)cm);
+    constexpr float t = (w.c > 0) == (sd > 0) ? 1.f : -1.f;  // cs ss
+    const float2 a = __ffma2_rn(x.im, make_float2(-t, -t), x.re);
+    const float2 b = __ffma2_rn(x.re, make_float2(t, t), x.im);
+    const float2 u = __ffma2_rn(a, make_float2(mh, mh), __fmul2_rn(a, make_float2(ml, ml)));
+    const float2 v = __ffma2_rn(b, make_float2(mh, mh), __fmul2_rn(b, make_float2(ml, ml)));
+    return cpk{u, v};
   } else {
     // hi + lo root as in twiddle() above
     constexpr CS w = unit_root(k, N);

@@ -103,6 +103,18 @@ __device__ __forceinline__ cplx<R> scale_w(cplx<R> x, R hi, R lo) {
   else return scale2<R>(x, hi, lo);
 }
 
+// x * w for a weight that one float holds exactly (lo = 0): the same value
+// as scale_w(x, w, 0), in one product per component
+template <typename R, bool PK>
+__device__ __forceinline__ cplx<R> scale_w1(cplx<R> x, R w) {
+  if constexpr (PK && sizeof(R) == 4) {
+    const float2 r = __fmul2_rn(make_float2(x.re, x.im), make_float2(w, w));
+    return cplx<R>{r.x, r.y};
+  } else {
+    return cplx<R>{x.re * w, x.im * w};
+  }
+}
+
 template <typename R, int L, int C>
 struct FusedShape {
   static constexpr int S = L / C;             // x (or y) planes per CTA
@@ -204,6 +216,9 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
+  // (1 +- a)/V held exactly by one float (a = 0.5 with V a power of two):
+  // one product per component instead of the hi + lo product
+  const bool w_exact = wp_lo == (R)0 && wm_lo == (R)0;
 
   if (STAGED && tid == 0) mbar_init(bar);
   __syncthreads();
@@ -286,10 +301,18 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
         const uint64_t k0 = kb + (uint64_t)site0;
         const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
         const int bit = (int)(k0 & 31);
+        if (w_exact) {
 #pragma unroll
-        for (int xx = 0; xx < L; ++xx) {
-          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
-          x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+            x[xx] = scale_w1<R, PK>(x[xx], up ? wp_hi : wm_hi);
+          }
+        } else {
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+            x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          }
         }
       } else {
 #pragma unroll
@@ -382,6 +405,9 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
+  // (1 +- a)/V held exactly by one float (a = 0.5 with V a power of two):
+  // one product per component instead of the hi + lo product
+  const bool w_exact = wp_lo == (R)0 && wm_lo == (R)0;
 
   if (tid == 0) mbar_init(bar);
   __syncthreads();
@@ -447,11 +473,20 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
         const uint64_t k0 = kb + (uint64_t)site0;
         const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
         const int bit = (int)(k0 & 31);
+        if (w_exact) {
 #pragma unroll
-        for (int k = 0; k < H; ++k) {
-          const int xx = h * H + k;
-          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
-          v[k] = scale2<R>(v[k], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          for (int k = 0; k < H; ++k) {
+            const int xx = h * H + k;
+            const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+            v[k] = scale_w1<R, false>(v[k], up ? wp_hi : wm_hi);
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < H; ++k) {
+            const int xx = h * H + k;
+            const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+            v[k] = scale2<R>(v[k], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          }
         }
       } else {
 #pragma unroll
@@ -629,6 +664,9 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
+  // (1 +- a)/V held exactly by one float (a = 0.5 with V a power of two):
+  // one product per component instead of the hi + lo product
+  const bool w_exact = wp_lo == (R)0 && wm_lo == (R)0;
 
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar_hbm)) : "memory");
@@ -720,10 +758,18 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
         const uint64_t k0 = kb + (uint64_t)site0;
         const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
         const int bit = (int)(k0 & 31);
+        if (w_exact) {
 #pragma unroll
-        for (int xx = 0; xx < L; ++xx) {
-          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
-          x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+            x[xx] = scale_w1<R, PK>(x[xx], up ? wp_hi : wm_hi);
+          }
+        } else {
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+            x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          }
         }
       } else {
 #pragma unroll

@@ -47,6 +47,7 @@ struct FusedArgs {
   const uint64_t* conf_base;  // optional per-configuration offsets (replace conf * conf_stride)
   double a;
   double vol;
+  double inv_vol;          // 1 / vol (a product per site instead of a division)
   double w_plus, w_minus;  // (1 + a)/V and (1 - a)/V for Z2 fields
   int* err;                // device flag: 1 = a bounded wait timed out
 };
@@ -62,8 +63,8 @@ __device__ __forceinline__ cplx<R> apply_w_general(const FusedArgs& f, uint64_t 
     wi = 0.0;
   } else if (f.field_mode == 2) {
     double2 phi = __ldg(reinterpret_cast<const double2*>(f.field) + k);
-    wr = (1.0 + f.a * phi.x) / f.vol;
-    wi = (f.a * phi.y) / f.vol;
+    wr = (1.0 + f.a * phi.x) * f.inv_vol;
+    wi = (f.a * phi.y) * f.inv_vol;
   } else {
     double2 v = __ldg(reinterpret_cast<const double2*>(f.field) + k);
     wr = v.x;
@@ -1049,6 +1050,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   // launches on the same buffer keep the values of order one
   f.a = 0.0;
   f.vol = (double)V;
+  f.inv_vol = 1.0 / (double)V;
   f.w_plus = 1.0 / V;
   f.w_minus = 1.0 / V;
   f.err = ctx->dev_err;
@@ -1123,6 +1125,7 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   f.conf_base = w->dev_conf_base;
   f.a = w->a;
   f.vol = (double)d[0] * d[1] * d[2];
+  f.inv_vol = 1.0 / f.vol;
   f.w_plus = (1.0 + f.a) / f.vol;
   f.w_minus = (1.0 - f.a) / f.vol;
   f.err = ctx->dev_err;

@@ -77,6 +77,7 @@ __device__ __forceinline__ cplx<R> apply_w_general(const FusedArgs& f, uint64_t 
   }
   R rh, rl, ih, il;
   split<R>(wr, rh, rl);
+  if (wi == 0.0) return scale2<R>(x, rh, rl);  // real weight (Z2, Gaussian, potential): the same value, half the work
   split<R>(wi, ih, il);
   // (x.re + i x.im)(wr + i wi) with each real product taken correctly rounded
   cplx<R> y;

@@ -511,6 +511,21 @@ def test_qr_fp32_against_fp64(golden, ctx):
     assert rel_err(d64[:2], g["dets"]) < FP64_REL
 
 
+@pytest.mark.parametrize("L,T,ef,n_conf", [(24, 64, 0.08, 16), (48, 32, 0.02, 4)])
+def test_fp32_correlators_other_extents(ctx, L, T, ef, n_conf):
+    """The same FP32-vs-FP64 bound at the extents whose register DFTs use
+    radix-3 stages (24 = 8 x 3, 48 = 16 x 3), N = 19, QR every 8 slices."""
+    idx, _, _ = nb.momenta((L, L, L), "PERFECT", 1.0, ef, 2.0)
+    assert len(idx) == 19
+    out = {}
+    for prec, qr in (("f32", 8), ("f64", 0)):
+        job = nb.EnsembleJob(L=L, T=T, n_conf=n_conf, seed=11, precision=prec, fermi_energy=ef, qr_period=qr)
+        ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
+        out[prec] = (np.abs(ens.run(0).cpu().numpy()) ** 2).mean(0)
+        ens.close()
+    assert rel_err(out["f32"], out["f64"]) < FP32_REL
+
+
 def test_fp32_correlators_at_the_batched_config_shape(ctx):
     """L=32, T=64, N=19 plane waves, Z2 a=0.5, seed 7: FP32 propagation with
     re-orthonormalisation every 8 slices against the FP64 mode (itself held to

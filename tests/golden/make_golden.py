@@ -3,14 +3,18 @@
 Run here (where the reference tree and its CPU build exist), never on a GPU
 box:
 
-    make -C oracle/ref_build REF=/root/reference
-    python tests/golden/make_golden.py --ref /root/reference
+    make -C oracle/ref_build REF=<reference tree>
+    python tests/golden/make_golden.py --ref <reference tree> [--only GROUP]
 
 Sources of truth:
   * ranlx_kat.npz      -- Luscher's published ranlxs/ranlxd sequences, parsed
                           from the reference's own test (tests/ranlx/main.C).
   * ludcmp_kat.json    -- the reference's 10x10 Hilbert LU test
                           (tests/ludcmp_test/main.C) as printed by its binary.
+  * batch_large.npz    -- the oracle's batch runner (o_run_batch) at the
+                          uneven workload's largest shapes; the reference has
+                          no batch driver, and the oracle is pinned to it by
+                          the ensemble fixtures.
   * everything else    -- outputs of the reference's CPU path compiled from
                           its unchanged sources (oracle/_ref/nrcps_ref, see
                           oracle/ref_build/ref_driver.cc).
@@ -94,6 +98,17 @@ def fields(tmp: str) -> dict:
     return out
 
 
+# Keys passed to the reference binary that name a path of the generating
+# machine; they are left out of the stored arguments.
+_LOCAL_KEYS = ("sho_dir", "out")
+
+# Above this many source entries only every SOURCE_STRIDE-th entry of the
+# sources is stored (sources_sample); the tests rebuild the full sources with
+# the library's own builders and check them against the sample.
+SOURCE_FULL_MAX = 1 << 16
+SOURCE_STRIDE = 61
+
+
 def ensemble(tmp: str, name: str, **kv) -> dict:
     d = os.path.join(tmp, name)
     os.makedirs(d, exist_ok=True)
@@ -102,11 +117,16 @@ def ensemble(tmp: str, name: str, **kv) -> dict:
     L, T = int(kv["L"]), int(kv["T"])
     N = info["N"]
     nmeas = 2 * N if kv.get("mode") == "slater2" else N
+    sources = np.fromfile(os.path.join(d, "sources.bin"), dtype=np.complex128).reshape(N, L ** 3)
     res = {
         "dets": np.fromfile(os.path.join(d, "dets.bin"), dtype=np.complex128).reshape(-1, T, nmeas),
-        "sources": np.fromfile(os.path.join(d, "sources.bin"), dtype=np.complex128).reshape(N, L ** 3),
-        "args": json.dumps(kv),
+        "args": json.dumps({k: v for k, v in kv.items() if k not in _LOCAL_KEYS}),
     }
+    if sources.size <= SOURCE_FULL_MAX:
+        res["sources"] = sources
+    else:
+        res["sources_sample"] = sources[:, ::SOURCE_STRIDE].copy()
+        res["sources_stride"] = np.int64(SOURCE_STRIDE)
     if os.path.exists(os.path.join(d, "momenta.txt")):
         res["momenta"] = np.loadtxt(os.path.join(d, "momenta.txt"), dtype=np.int64).reshape(-1, 4)
     if os.path.exists(os.path.join(d, "props.bin")):
@@ -188,50 +208,144 @@ def ohpair_cases(tmp: str) -> dict:
     return out
 
 
+def result_files(tmp: str, name: str, sho: dict, **kv) -> dict:
+    """The drivers' own result files for a small run: the reference's
+    accumulation and Fprintf rows (one row per block of `unload`
+    configurations), next to the raw determinants they were made from."""
+    d = os.path.join(tmp, name)
+    os.makedirs(d, exist_ok=True)
+    if kv.get("sources") == "sho":
+        write_sho_dir(sho, os.path.join(d, "sho"))
+        kv["sho_dir"] = os.path.join(d, "sho")
+    res = ensemble(tmp, name, results=d, **kv)
+    texts = {}
+    for fn in sorted(os.listdir(d)):
+        if fn.startswith("slater.") or (fn.startswith("z") and "." in fn):
+            texts[fn] = open(os.path.join(d, fn)).read()
+    res["result_files"] = json.dumps(texts)
+    res["args"] = json.dumps({k: v for k, v in json.loads(str(res["args"])).items() if k != "results"})
+    return res
+
+
+def write_sho_dir(sho: dict, shodir: str) -> None:
+    os.makedirs(shodir, exist_ok=True)
+    for n, lines in sho.items():
+        with open(os.path.join(shodir, f"source.{n}"), "w") as f:
+            for l in lines:
+                f.write(f"{l[0]} {l[1]} {l[2]} {l[3]!r} {l[4]!r}\n")
+
+
+# The uneven-batch workload's largest and middle shapes (L, T, n_conf, N) with
+# E_F between closed shells; N = 7, 19, 33 are the shells |n|^2 <= 1, 2, 4.
+BATCH_LARGE_JOBS = [(48, 128, 1, 33), (24, 64, 1, 19), (16, 32, 2, 7)]
+_SHELL = {7: 1.5, 19: 2.5, 33: 4.5}
+
+
+def batch_large() -> dict:
+    """Uneven-batch jobs at the workload's largest shapes through the oracle's
+    batch runner (o_run_batch, Gaussian fields a = 0.3, RANLXS2 seed 99).  The
+    oracle is pinned to the reference on the ensemble fixtures; the reference
+    itself has no batch driver."""
+    import sys
+    sys.path.insert(0, REPO)
+    from oracle import oracle as O
+    jobs, meta = [], []
+    for L, T, nc, N in BATCH_LARGE_JOBS:
+        ef = 0.5 * (2 * np.pi / L) ** 2 * _SHELL[N]
+        idx, _, _ = O.momenta((L,) * 3, "PERFECT", 1.0, ef, (2 * O.PI) ** 2)
+        assert len(idx) == N
+        jobs.append((L, T, nc, list(idx)))
+        meta.append([L, T, nc, N])
+    outs = O.run_batch(jobs, "RANLXS2", 99, "GAUSS", 0.3)
+    res = {f"dets{i}": o for i, o in enumerate(outs)}
+    res["jobs"] = np.array(meta, dtype=np.int64)
+    res["fermi_energies"] = np.array([0.5 * (2 * np.pi / L) ** 2 * _SHELL[N] for L, _, _, N in BATCH_LARGE_JOBS])
+    res["args"] = json.dumps({"rng": "RANLXS2", "seed": 99, "field": "GAUSS", "a": 0.3, "kin_dt": 0.5,
+                              "cutoff": 2.0})
+    return res
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", default="", help="regenerate one fixture only (ohpair)")
+    ap.add_argument("--ref", default=os.environ.get("NRCPS_REFERENCE", ""),
+                    help="the reference tree (or set NRCPS_REFERENCE)")
+    ap.add_argument("--only", default="",
+                    help="regenerate one group only: ohpair, small, config2, trapped48, results, batch_large")
     a = ap.parse_args()
-    if not os.path.exists(REF_BIN) or not os.path.exists(os.path.join(REPO, "oracle", "_ref", "ohpair_dump")):
+    need_ref = a.only != "batch_large"
+    if need_ref and not a.ref:
+        ap.error("--ref (or NRCPS_REFERENCE) names the reference tree")
+    if need_ref and (not os.path.exists(REF_BIN) or
+                     not os.path.exists(os.path.join(REPO, "oracle", "_ref", "ohpair_dump"))):
         subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "oracle", "ref_build"), f"REF={a.ref}"])
-    if a.only == "ohpair" or not a.only:
+    if a.only in ("", "ohpair"):
         with tempfile.TemporaryDirectory() as tmp:
             np.savez_compressed(os.path.join(HERE, "ohpair.npz"), **ohpair_cases(tmp))
-        if a.only:
-            return
-    np.savez_compressed(os.path.join(HERE, "ranlx_kat.npz"), **parse_ranlx_kat(a.ref))
-    json.dump(parse_ludcmp_kat(a.ref), open(os.path.join(HERE, "ludcmp_kat.json"), "w"), indent=1)
-    sho = sho_coefficients(a.ref)
-    json.dump(sho, open(os.path.join(HERE, "sho_coefficients.json"), "w"))
-    with tempfile.TemporaryDirectory() as tmp:
-        np.savez_compressed(os.path.join(HERE, "rng_streams.npz"), **rng_streams(tmp))
-        np.savez_compressed(os.path.join(HERE, "fields.npz"), **fields(tmp))
-        np.savez_compressed(os.path.join(HERE, "lu_cases.npz"), **lu_cases(tmp))
-        # config 1 of the benchmark: L=16, T=32, N=7 (E_F=0.1), Z2 a=0.5, seed 1234
-        np.savez_compressed(os.path.join(HERE, "ensemble_config1.npz"), **ensemble(
-            tmp, "c1", L=16, T=32, ef=0.1, seed=1234, rng="RANLXS2", field="ZTWO",
-            couplings="0.019894367886486918", cutoff=2.0, configs=2, dump_fields=3))
-        # small lattice, p-dependent interaction (3 couplings), ranlxd, props dumped
-        np.savez_compressed(os.path.join(HERE, "ensemble_multicoupling.npz"), **ensemble(
-            tmp, "mc", L=8, T=8, ef=0.35, seed=5, rng="RANLXD1", field="ZTWO",
-            couplings="0.02,0.004,0.001", cutoff=0.99999, configs=2, dump_props=4))
-        # Gaussian field, a=0.3
-        np.savez_compressed(os.path.join(HERE, "ensemble_gauss.npz"), **ensemble(
-            tmp, "g", L=8, T=8, ef=0.35, seed=99, rng="RANLXS2", field="GAUSS",
-            couplings=repr(0.09 / (4 * np.pi)), cutoff=2.0, configs=2))
-        # trapped, SHO sources, pair sink (production/slater_det2_trapped shape)
-        shodir = os.path.join(tmp, "sho")
-        os.makedirs(shodir)
-        for n, lines in sho.items():
-            with open(os.path.join(shodir, f"source.{n}"), "w") as f:
-                for l in lines:
-                    f.write(f"{l[0]} {l[1]} {l[2]} {l[3]!r} {l[4]!r}\n")
-        np.savez_compressed(os.path.join(HERE, "ensemble_trapped.npz"), **ensemble(
-            tmp, "tr", L=8, T=6, sources="sho", N=4, sho_dir=shodir, lambda1=2.0, lambda2=2.0,
-            lambda3=2.0, mode="slater2", potential=1, kappa=0.005, ptype="EXP", wavefunc="TGND",
-            tb_disp="STANDARD", tb_lambda=0.176776695, seed=31, rng="RANLXS2", field="ZTWO",
-            couplings="0.019894367886486918", cutoff=0.99999, configs=2, dump_props=3))
+    sho = sho_coefficients(a.ref) if need_ref else None
+    if a.only in ("", "small"):
+        np.savez_compressed(os.path.join(HERE, "ranlx_kat.npz"), **parse_ranlx_kat(a.ref))
+        json.dump(parse_ludcmp_kat(a.ref), open(os.path.join(HERE, "ludcmp_kat.json"), "w"), indent=1)
+        json.dump(sho, open(os.path.join(HERE, "sho_coefficients.json"), "w"))
+        with tempfile.TemporaryDirectory() as tmp:
+            np.savez_compressed(os.path.join(HERE, "rng_streams.npz"), **rng_streams(tmp))
+            np.savez_compressed(os.path.join(HERE, "fields.npz"), **fields(tmp))
+            np.savez_compressed(os.path.join(HERE, "lu_cases.npz"), **lu_cases(tmp))
+            # config 1 of the benchmark: L=16, T=32, N=7 (E_F=0.1), Z2 a=0.5, seed 1234
+            np.savez_compressed(os.path.join(HERE, "ensemble_config1.npz"), **ensemble(
+                tmp, "c1", L=16, T=32, ef=0.1, seed=1234, rng="RANLXS2", field="ZTWO",
+                couplings="0.019894367886486918", cutoff=2.0, configs=2, dump_fields=3))
+            # small lattice, p-dependent interaction (3 couplings), ranlxd, props dumped
+            np.savez_compressed(os.path.join(HERE, "ensemble_multicoupling.npz"), **ensemble(
+                tmp, "mc", L=8, T=8, ef=0.35, seed=5, rng="RANLXD1", field="ZTWO",
+                couplings="0.02,0.004,0.001", cutoff=0.99999, configs=2, dump_props=4))
+            # Gaussian field, a=0.3
+            np.savez_compressed(os.path.join(HERE, "ensemble_gauss.npz"), **ensemble(
+                tmp, "g", L=8, T=8, ef=0.35, seed=99, rng="RANLXS2", field="GAUSS",
+                couplings=repr(0.09 / (4 * np.pi)), cutoff=2.0, configs=2))
+            # trapped, SHO sources, pair sink (production/slater_det2_trapped shape)
+            shodir = os.path.join(tmp, "sho")
+            write_sho_dir(sho, shodir)
+            np.savez_compressed(os.path.join(HERE, "ensemble_trapped.npz"), **ensemble(
+                tmp, "tr", L=8, T=6, sources="sho", N=4, sho_dir=shodir, lambda1=2.0, lambda2=2.0,
+                lambda3=2.0, mode="slater2", potential=1, kappa=0.005, ptype="EXP", wavefunc="TGND",
+                tb_disp="STANDARD", tb_lambda=0.176776695, seed=31, rng="RANLXS2", field="ZTWO",
+                couplings="0.019894367886486918", cutoff=0.99999, configs=2, dump_props=3))
+    if a.only in ("", "config2"):
+        # the batched workload's shape: L=32, T=64, N=19 (E_F=0.045), Z2 a=0.5,
+        # RANLXS2 seed 7 (production/slater_det/main.C:185-220); 2 configurations
+        with tempfile.TemporaryDirectory() as tmp:
+            np.savez_compressed(os.path.join(HERE, "ensemble_config2.npz"), **ensemble(
+                tmp, "c2", L=32, T=64, ef=0.045, seed=7, rng="RANLXS2", field="ZTWO",
+                couplings="0.019894367886486918", cutoff=2.0, configs=2))
+    if a.only in ("", "trapped48"):
+        # the trapped few-body workload's shape: L=48, T=128, SHO N=10 from
+        # production/slater_det2_trapped/sources/source.{0..9} with that
+        # production's lambda = 4 (args/one_body.arg), [K,V,I,V,K] with a
+        # harmonic EXP trap kappa = 0.005, TGND pair sink, Z2 a=0.5, RANLXS2
+        # seed 31 (production/slater_det2_trapped/main-no_cum.C:90-128,185-210)
+        with tempfile.TemporaryDirectory() as tmp:
+            shodir = os.path.join(tmp, "sho")
+            write_sho_dir(sho, shodir)
+            np.savez_compressed(os.path.join(HERE, "ensemble_trapped48.npz"), **ensemble(
+                tmp, "t48", L=48, T=128, sources="sho", N=10, sho_dir=shodir, lambda1=4.0, lambda2=4.0,
+                lambda3=4.0, mode="slater2", potential=1, kappa=0.005, ptype="EXP", wavefunc="TGND",
+                tb_disp="STANDARD", tb_lambda=0.176776695, seed=31, rng="RANLXS2", field="ZTWO",
+                couplings="0.019894367886486918", cutoff=2.0, configs=2))
+    if a.only in ("", "results"):
+        # results/slater.<m> of production/slater_det/main.C (|det|^2 rows) and
+        # results/slater.<m> + z<k>.<m> of production/slater_det2_trapped/main-cum.C
+        # (det rows, Nc = 6 log-det cumulants), 6 configurations in blocks of 2
+        with tempfile.TemporaryDirectory() as tmp:
+            np.savez_compressed(os.path.join(HERE, "results_slater.npz"), **result_files(
+                tmp, "rs", sho, L=8, T=6, ef=0.35, seed=5, rng="RANLXS2", field="ZTWO",
+                couplings="0.019894367886486918", cutoff=2.0, configs=6, unload=2))
+            np.savez_compressed(os.path.join(HERE, "results_trapped_cum.npz"), **result_files(
+                tmp, "rc", sho, L=8, T=6, sources="sho", N=4, lambda1=2.0, lambda2=2.0, lambda3=2.0,
+                mode="slater2", potential=1, kappa=0.005, ptype="EXP", wavefunc="TGND", tb_disp="STANDARD",
+                tb_lambda=0.176776695, seed=31, rng="RANLXS2", field="ZTWO", couplings="0.019894367886486918",
+                cutoff=0.99999, configs=6, unload=2, cumulants=6))
+    if a.only in ("", "batch_large"):
+        np.savez_compressed(os.path.join(HERE, "batch_large.npz"), **batch_large())
     print("golden fixtures written to", HERE)
 
 

@@ -92,3 +92,26 @@ def test_device_batch_uneven_shapes_fp32_vs_fp64():
         b.close()
     for a, r in zip(out["f32"], out["f64"]):
         assert _rel(a, r) < 1e-5
+
+
+@pytest.mark.gpu
+def test_device_batch_fp64_at_the_largest_uneven_shapes(golden):
+    """The uneven workload's largest shapes -- one L=48, N=33, T=128 job, one
+    L=24, N=19, T=64 job and two L=16, N=7, T=32 configurations, Gaussian
+    fields a=0.3 from RANLXS2 seed 99 -- as one device batch in FP64 against
+    the oracle's batch runner (tests/golden/batch_large.npz), 1e-12."""
+    import json
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    g = golden("batch_large.npz")
+    args = json.loads(str(g["args"]))
+    jobs = [nb.BatchJob(L=int(L), T=int(T), n_conf=int(c), fermi_energy=float(ef))
+            for (L, T, c, _), ef in zip(g["jobs"], g["fermi_energies"])]
+    b = nb.Batch(jobs, seed=int(args["seed"]), field=args["field"], a=float(args["a"]), precision="f64", ctx=ctx)
+    assert b.n_orb == [int(n) for n in g["jobs"][:, 3]]
+    got = [d.cpu().numpy() for d in b.run()]
+    b.close()
+    for i, d in enumerate(got):
+        ref = g[f"dets{i}"]
+        assert d.shape == ref.shape
+        assert _rel(d, ref) < FP64_REL, (i, _rel(d, ref))

@@ -61,6 +61,24 @@ def test_momenta_and_sources_bit_exact(golden):
         assert np.array_equal(nb.sho_source((8, 8, 8), (2.0, 2.0, 2.0), sho[str(n)]), t["sources"][n])
 
 
+def test_headline_and_trapped_shape_tables_bit_exact(golden):
+    """The batched workload's 19 plane waves at L=32 (E_F = 0.045) and the
+    trapped workload's 10 SHO sources at L=48 (lambda = 4) against the
+    reference's own (the momenta list and every 61st source entry)."""
+    g = golden("ensemble_config2.npz")
+    idx, _, par = nb.momenta((32, 32, 32), "PERFECT", 1.0, 0.045, 2.0)
+    mom = g["momenta"]
+    assert len(idx) == 19
+    assert np.array_equal(idx, mom[:, 2] + 32 * (mom[:, 1] + 32 * mom[:, 0]))
+    assert np.array_equal(par, mom[:, 3])
+    t = golden("ensemble_trapped48.npz")
+    sho = json.load(open(os.path.join(GOLDEN, "sho_coefficients.json")))
+    stride = int(t["sources_stride"])
+    for n in range(t["sources_sample"].shape[0]):
+        got = nb.sho_source((48, 48, 48), (4.0, 4.0, 4.0), sho[str(n)])
+        assert np.array_equal(got[::stride], t["sources_sample"][n]), n
+
+
 def test_momenta_errors():
     with pytest.raises(nb.NrcpsError):
         nb.momenta((16, 16, 16), "PERFECT", 1.0, -1.0, 2.0)  # nothing below the Fermi level

@@ -167,6 +167,28 @@ def test_ensemble_bit_exact(golden, name):
     assert np.array_equal(dets, g["dets"])
 
 
+@pytest.mark.parametrize("name,slices", [("ensemble_config2.npz", 8), ("ensemble_trapped48.npz", 6)])
+def test_ensemble_prefix_bit_exact_at_workload_shapes(golden, name, slices):
+    """The first slices of configuration 0 at the batched workload's shape
+    (L=32, N=19) and at the trapped workload's (L=48, SHO N=10, [K,V,I,V,K],
+    pair sink) against the reference's run of the full extent: the first
+    slices of configuration 0 do not depend on T."""
+    g = golden(name)
+    args = json.loads(str(g["args"]))
+    job = _job_from_args(args)
+    job.T, job.configs = slices, 1
+    if "momenta" in g.files and args.get("sources", "mom") == "mom":
+        idx, _, _ = O.momenta(job.dims, "PERFECT", 1.0, float(args["ef"]), job.cutoff_sq)
+        src = O.plane_wave_sources(job.dims, idx)
+    else:
+        sho = json.load(open(os.path.join(GOLDEN, "sho_coefficients.json")))
+        lam = (float(args["lambda1"]), float(args["lambda2"]), float(args["lambda3"]))
+        src = np.stack([O.sho_source(job.dims, lam, sho[str(n)]) for n in range(int(args["N"]))])
+        assert np.array_equal(src[:, ::int(g["sources_stride"])], g["sources_sample"])
+    dets = O.run_ensemble(job, src)
+    assert np.array_equal(dets[0], g["dets"][0, :slices])
+
+
 def test_propagation_steps_match_reference_props(golden):
     """Per-step orbitals of config 0 against Propagator::Run's dumps."""
     g = golden("ensemble_multicoupling.npz")

@@ -26,12 +26,14 @@ __global__ void accumulate_kernel(const double* __restrict__ dets, int n_conf, i
   for (int k = 0; k < 8; ++k) zs[k] = 0.0;
   for (int c = 0; c < n_conf; ++c) {
     const double2 d = reinterpret_cast<const double2*>(dets)[((long)c * T + t) * nmeas + m];
+    // explicitly rounded products and sums (no fused multiply-add): the
+    // reference's arithmetic to the bit
     if (mode == 0) {
-      // tmp * conj(tmp) (main.C:210)
-      cr += d.x * d.x + d.y * d.y;
+      // tmp * conj(tmp) (main.C:210): real part re*re + im*im
+      cr = __dadd_rn(cr, __dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)));
     } else {
-      cr += d.x;
-      ci += d.y;
+      cr = __dadd_rn(cr, d.x);
+      ci = __dadd_rn(ci, d.y);
     }
     if (nc > 0) {
       const double l = log(hypot(d.x, d.y));  // cum[0] = log(abs(slat)) (main-cum.C:221)
@@ -39,8 +41,8 @@ __global__ void accumulate_kernel(const double* __restrict__ dets, int n_conf, i
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         if (k < nc) {
-          zs[k] += p;
-          p *= l;  // cum[nc] = cum[0] * cum[nc-1]
+          zs[k] = __dadd_rn(zs[k], p);
+          p = __dmul_rn(p, l);  // cum[nc] = cum[0] * cum[nc-1]
         }
       }
     }

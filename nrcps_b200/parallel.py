@@ -31,17 +31,50 @@ def rank_seed(seed: int, rank: int) -> int:
 
 
 def accumulate(dets, mode: str = "slater"):
-    """Sum over configurations of |det|^2 (mode 'slater') or det ('slater2').
+    """Sum over configurations of |det|^2 (mode 'slater') or det ('slater2'),
+    configuration after configuration as the drivers' `corr[n][t] += ...`
+    (|det|^2 as re*re + im*im, the real part of tmp*conj(tmp)), so that the
+    sums -- and the result rows printed from them -- are the reference's to
+    the bit.
 
-    dets: [n_conf, T, nmeas] complex (numpy or torch); returns [nmeas, T] complex128.
-    """
-    if isinstance(dets, torch.Tensor):
-        d = dets.to(torch.complex128)
-        s = (d.real ** 2 + d.imag ** 2).sum(0).to(torch.complex128) if mode == "slater" else d.sum(0)
-        return s.transpose(0, 1).contiguous()
+    dets: [n_conf, T, nmeas] complex (numpy or torch); returns [nmeas, T]
+    complex128 (a device tensor through the library's kernel for CUDA
+    tensors, the same type as the input otherwise)."""
+    if isinstance(dets, torch.Tensor) and dets.is_cuda:
+        from .api import accumulate as device_accumulate
+        corr, _ = device_accumulate(dets, mode, 0)
+        return corr
+    as_torch = isinstance(dets, torch.Tensor)
+    d = np.asarray(dets.numpy() if as_torch else dets, dtype=np.complex128)
+    s = np.zeros(d.shape[1:], dtype=np.complex128)
+    for c in range(d.shape[0]):
+        if mode == "slater":
+            s.real += d[c].real * d[c].real + d[c].imag * d[c].imag
+        else:
+            s += d[c]
+    out = np.ascontiguousarray(s.T)
+    return torch.from_numpy(out) if as_torch else out
+
+
+def cumulant_sums(dets, n_cumulants: int):
+    """The log-det moments of production/slater_det2_trapped/main-cum.C:219-233
+    on the host: cum[0] = log(abs(det)), cum[k] = cum[0] cum[k-1],
+    z[k][m][t] += cum[k], configuration after configuration, with the C
+    library's log and hypot (math.log, abs of a Python complex) as the
+    reference's.  dets [n_conf, T, nmeas] -> z [n_cumulants, nmeas, T]."""
+    import math
     d = np.asarray(dets, dtype=np.complex128)
-    s = (np.abs(d) ** 2).sum(0).astype(np.complex128) if mode == "slater" else d.sum(0)
-    return np.ascontiguousarray(s.T)
+    n_conf, T, nmeas = d.shape
+    z = np.zeros((n_cumulants, nmeas, T))
+    for c in range(n_conf):
+        for t in range(T):
+            for m in range(nmeas):
+                c0 = math.log(abs(complex(d[c, t, m])))
+                p = c0
+                for k in range(n_cumulants):
+                    z[k, m, t] += p
+                    p = c0 * p
+    return z
 
 
 def global_sum(corr: torch.Tensor, group=None) -> torch.Tensor:

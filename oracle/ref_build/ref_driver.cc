@@ -10,7 +10,12 @@
 //   ensemble  -- the loop of production/slater_det/main.C:185-220 (mode=slater)
 //                or production/slater_det2_trapped/main-no_cum.C:185-210
 //                (mode=slater2); writes every per-configuration determinant
-//                det S_n(tau) before any accumulation.
+//                det S_n(tau) before any accumulation, and with
+//                results=<dir> also the drivers' own result files
+//                <dir>/slater.<m> (and <dir>/z<k>.<m> for cumulants=<Nc>),
+//                a row per block of unload=<k> configurations, accumulated
+//                and printed as production/slater_det/main.C:208-247 and
+//                production/slater_det2_trapped/main-cum.C:219-270 do.
 //   rng       -- Random::Uniform stream (src/random/random.C:100-103).
 //   gauss     -- Random::Gauss stream (src/random/random.C:105-116).
 //   field     -- Lattice::Refresh slices (src/alg/lattice.C:60-109).
@@ -49,6 +54,7 @@ using namespace std;
 #include "slater_det.h"
 #include "slater_det2.h"
 #include "sysfunc.h"
+#include "sysio.h"
 #include "two_body.h"
 #include "uniform_deviates.h"
 #include "verbose.h"
@@ -368,6 +374,27 @@ int run_ensemble(const KV& kv, bool timed_only) {
   vector<complex<double> > row(nmeas);
   vector<complex<double> > smat((size_t)N * N), psi1((size_t)N * N);
 
+  // The drivers' block accumulators and result files (Comms::Size() is 1
+  // here, so GlobalSum is the identity and block_size = unload_period).
+  const string results = get(kv, "results", "");
+  const int unload = (int)getl(kv, "unload", 1);
+  const int Nc = (int)getl(kv, "cumulants", 0);
+  vector<FILE*> rfile, zfile;
+  vector<complex<Float> > corr((size_t)nmeas * T, complex<Float>(0.0, 0.0));
+  vector<complex<Float> > zacc((size_t)(Nc > 0 ? Nc : 1) * nmeas * T, complex<Float>(0.0, 0.0));
+  vector<complex<Float> > cum(Nc > 0 ? Nc : 1);
+  if (!timed_only && !results.empty()) {
+    char f_name[512];
+    for (int m = 0; m < nmeas; ++m) {
+      snprintf(f_name, sizeof f_name, "%s/slater.%d", results.c_str(), m + 1);
+      rfile.push_back(Fopen(IO_TYPE_ROOT, f_name, "a"));
+      for (int nc = 0; nc < Nc; ++nc) {
+        snprintf(f_name, sizeof f_name, "%s/z%d.%d", results.c_str(), nc + 1, m + 1);
+        zfile.push_back(Fopen(IO_TYPE_ROOT, f_name, "a"));  // zfile[m * Nc + nc]
+      }
+    }
+  }
+
   for (int j = 0; j < configs; ++j) {
     for (int n = 0; n < N; ++n) propagator.Set(one_bodies[n]->Get(), n);
     for (int t = 0; t < T; ++t) {
@@ -395,6 +422,18 @@ int run_ensemble(const KV& kv, bool timed_only) {
         for (int n = 0; n < N; ++n) row[n] = minor_det(smat, N, n + 1, -1, -1, 0);
       }
       if (fd) fwrite(&row[0], sizeof(complex<double>), nmeas, fd);
+      if (!rfile.empty()) {
+        for (int m = 0; m < nmeas; ++m) {
+          complex<Float> slat = row[m];
+          // main.C:209-210 (|det|^2 as tmp * conj(tmp)); main-no_cum.C:205-207 (det)
+          corr[(size_t)m * T + t] += (mode == "slater2") ? slat : slat * conj(slat);
+          if (Nc > 0) {  // main-cum.C:220-224
+            cum[0] = log(abs(slat));
+            for (int nc = 1; nc < Nc; ++nc) cum[nc] = cum[0] * cum[nc - 1];
+            for (int nc = 0; nc < Nc; ++nc) zacc[((size_t)nc * nmeas + m) * T + t] += cum[nc];
+          }
+        }
+      }
       if (ff && slices_done < dump_fields) {
         write_vec(ff, lattice.Get(), 2 * vol);
       }
@@ -406,7 +445,27 @@ int run_ensemble(const KV& kv, bool timed_only) {
     }
     if (max_slices > 0 && slices_done >= max_slices) break;
     if (timed_only && now_s() - t0 > budget) break;
+    if (!rfile.empty() && (j + 1) % unload == 0) {
+      // main.C:225-247 / main-cum.C:256-270 with Comms::Size() = 1
+      Float block_size = Comms::Size() * unload;
+      for (int m = 0; m < nmeas; ++m) {
+        for (int t = 0; t < T; ++t) {
+          complex<Float>& c = corr[(size_t)m * T + t];
+          Fprintf(rfile[m], "%.*e %.*e ", PREC, c.real() / block_size, PREC, c.imag() / block_size);
+          c = 0.0;
+          for (int nc = 0; nc < Nc; ++nc) {
+            complex<Float>& zz = zacc[((size_t)nc * nmeas + m) * T + t];
+            Fprintf(zfile[(size_t)m * Nc + nc], "%.*e ", PREC, zz.real() / block_size);
+            zz = 0.0;
+          }
+        }
+        Fprintf(rfile[m], "\n");
+        for (int nc = 0; nc < Nc; ++nc) Fprintf(zfile[(size_t)m * Nc + nc], "\n");
+      }
+    }
   }
+  for (size_t i = 0; i < rfile.size(); ++i) Fclose(rfile[i]);
+  for (size_t i = 0; i < zfile.size(); ++i) Fclose(zfile[i]);
   double el = now_s() - t0;
   if (fd) fclose(fd);
   if (ff) fclose(ff);

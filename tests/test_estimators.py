@@ -5,6 +5,8 @@ vectorised numpy form, and the result-file rows.  GPU: the device kernels
 (nrcps_accumulate, nrcps_jackknife) against the oracle and a direct numpy
 jackknife.
 """
+import json
+
 import numpy as np
 import pytest
 
@@ -76,3 +78,61 @@ def test_device_jackknife_matches_numpy():
     rmu, rerr, rem, ree = _np_jackknife(x, 17, True)
     for a, b in ((mu, rmu), (err, rerr), (em, rem), (ee, ree)):
         assert np.allclose(a.cpu().numpy(), b, rtol=1e-10, atol=0)
+
+
+# ------------------------------------------------------------ result files
+def _blocks(g):
+    args = json.loads(str(g["args"]))
+    return g["dets"], int(args["unload"]), int(args.get("cumulants", 0)), args.get("mode", "slater")
+
+
+@pytest.mark.parametrize("name", ["results_slater.npz", "results_trapped_cum.npz"])
+def test_result_rows_byte_identical_to_the_reference_files(golden, name):
+    """results/slater.<m> (and z<k>.<m>) as written by the reference's own
+    accumulation and Fprintf (production/slater_det/main.C:208-247,
+    production/slater_det2_trapped/main-cum.C:219-270), from the same raw
+    determinants: parallel.accumulate / cumulant_sums + block_rows reproduce
+    every file byte for byte."""
+    g = golden(name)
+    dets, unload, nc, mode = _blocks(g)
+    files = json.loads(str(g["result_files"]))
+    nmeas = dets.shape[2]
+    got = {f"slater.{m + 1}": "" for m in range(nmeas)}
+    got.update({f"z{k + 1}.{m + 1}": "" for k in range(nc) for m in range(nmeas)})
+    for b in range(dets.shape[0] // unload):
+        blk = dets[b * unload:(b + 1) * unload]
+        for m, row in enumerate(parallel.block_rows(parallel.accumulate(blk, mode), 1, unload)):
+            got[f"slater.{m + 1}"] += row + "\n"
+        if nc:
+            for k, rows in enumerate(parallel.block_rows_cumulants(parallel.cumulant_sums(blk, nc), 1, unload)):
+                for m, row in enumerate(rows):
+                    got[f"z{k + 1}.{m + 1}"] += row + "\n"
+    assert sorted(got) == sorted(files)
+    for fn in files:
+        assert got[fn] == files[fn], fn
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["results_slater.npz", "results_trapped_cum.npz"])
+def test_device_accumulate_result_rows(golden, name):
+    """The device accumulator (nrcps_accumulate) on the reference's raw
+    determinants: the slater.<m> rows byte for byte; the cumulant rows, whose
+    log and hypot are CUDA's (within an ulp or two of the C library's), within
+    1e-14 relative value for value."""
+    import torch
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    g = golden(name)
+    dets, unload, nc, mode = _blocks(g)
+    files = json.loads(str(g["result_files"]))
+    for b in range(dets.shape[0] // unload):
+        blk = torch.from_numpy(np.ascontiguousarray(dets[b * unload:(b + 1) * unload])).to(ctx.device)
+        corr, z = nb.accumulate(blk, mode, nc, ctx)
+        for m, row in enumerate(parallel.block_rows(corr, 1, unload)):
+            assert row == files[f"slater.{m + 1}"].splitlines()[b], (m, b)
+        if nc:
+            for k, rows in enumerate(parallel.block_rows_cumulants(z, 1, unload)):
+                for m, row in enumerate(rows):
+                    want = np.array(files[f"z{k + 1}.{m + 1}"].splitlines()[b].split(), dtype=float)
+                    got = np.array(row.split(), dtype=float)
+                    assert np.allclose(got, want, rtol=1e-14, atol=0), (k, m, b)

@@ -20,6 +20,9 @@
 //   gauss     -- Random::Gauss stream (src/random/random.C:105-116).
 //   field     -- Lattice::Refresh slices (src/alg/lattice.C:60-109).
 //   lu        -- ludcmp + det on matrices read from a file (src/utils/ludcmp.C).
+//   branch    -- the multilevel branching recursion of
+//                production/two_body-branched/main.C:23-80 over the current
+//                classes (see run_branch).
 //   bench     -- the ensemble loop timed with clock_gettime, for the CPU baseline.
 //
 // Built twice: against the reference's CPU units (nrcps_ref) and, as
@@ -542,9 +545,116 @@ int run_lu(const KV& kv) {
 
 }  // namespace
 
+// ---------------------------------------------------------------- branch
+// The multilevel branching driver of production/two_body-branched/main.C:23-80
+// (MultiLevel), written against the reference's current classes: that file
+// still calls Propagator::SetSource, Get() and Interaction3, which its headers
+// no longer declare, so it does not compile.  The recursion is kept as is;
+// Set(psi, 0) and Get(0) stand for SetSource(psi) and Get() of a
+// one-orbital Propagator, and the Hamiltonians are [K, I, K] (one coupling).
+struct Branch {
+  int branches, steps, levels;
+  Propagator *prop1, *prop2;
+  TwoBody* two_body;
+  Lattice* lattice;
+  vector<Hamiltonian*> hamiltonians;
+  vector<complex<Float> >* corr;
+};
+
+void multi_level(Branch& b, int level) {
+  if (level <= 0) return;
+  const int vol = GJP.Vol();
+  Float* p1 = b.prop1->Get(0);
+  Float* p2 = b.prop2->Get(0);
+  vector<Float> source1(p1, p1 + 2 * vol), source2(p2, p2 + 2 * vol);
+  const Float norm = pow((Float)b.branches, (Float)(b.levels - level + 1));
+  for (int i = 0; i < b.branches; ++i) {
+    b.prop1->Set(&source1[0], 0);
+    b.prop2->Set(&source2[0], 0);
+    for (int s = 0; s < b.steps; ++s) {
+      const int t = GJP.Tsites() - (level - 1) * b.steps - (b.steps - s);
+      (*b.corr)[t] += (b.two_body->Run(p1, p2) / norm);
+      for (size_t p = 0; p < b.hamiltonians.size(); ++p) b.hamiltonians[p]->Initialize();
+      b.prop1->Run(b.hamiltonians);
+      b.prop2->Run(b.hamiltonians);
+      b.lattice->Refresh();
+    }
+    multi_level(b, level - 1);
+  }
+}
+
+// Keys: L, levels, branches, steps, trees, seed, rng, field, couplings,
+// cutoff, p1 / p2 (momentum of each plane-wave source, "n1,n2,n3"),
+// wavefunc, tb_disp, tb_lambda, out (corr[T] complex doubles, summed over
+// the trees).
+int run_branch(const KV& kv) {
+  KV g = kv;
+  const int levels = (int)getl(kv, "levels", 3), steps = (int)getl(kv, "steps", 2);
+  char tbuf[32];
+  snprintf(tbuf, sizeof tbuf, "%d", levels * steps);
+  g["T"] = tbuf;
+  init_geometry(g);
+  Comms::Initialize();
+  RandomArg random_arg;
+  make_random_arg(kv, &random_arg);
+  Random rng(random_arg);
+  LatticeArg lattice_arg;
+  lattice_arg.field_type = field_type_of(get(kv, "field", "ZTWO"));
+  Lattice lattice(lattice_arg, &rng);
+  InteractionArg interaction_arg;
+  interaction_arg.mass = 1.0;
+  interaction_arg.interaction_type = INTERACTION_TYPE_ONEMINUSXIINVSQ;
+  interaction_arg.couplings = parse_list(get(kv, "couplings", "0.019894367886486918"));
+  interaction_arg.num_couplings = interaction_arg.couplings.size();
+  KineticArg kinetic_arg;
+  kinetic_arg.dispersion_type = DISPERSION_TYPE_PERFECT;
+  kinetic_arg.mass = 1.0;
+  Interaction interaction(&lattice, interaction_arg, 1.0);
+  Kinetic kinetic(kinetic_arg, 0.5);
+  OneBodyArg one_body_arg;
+  one_body_arg.source_type = SOURCE_TYPE_MOM;
+  OneBody source1(one_body_arg), source2(one_body_arg);
+  vector<double> m1 = parse_list(get(kv, "p1", "0,0,0")), m2 = parse_list(get(kv, "p2", "0,0,0"));
+  source1.Set((int)m1[0], (int)m1[1], (int)m1[2]);
+  source2.Set((int)m2[0], (int)m2[1], (int)m2[2]);
+  TwoBodyArg tb;
+  tb.wavefunc_type = wavefunc_type_of(get(kv, "wavefunc", "TGND"));
+  tb.dispersion_type1 = disp_type_of(get(kv, "tb_disp", "STANDARD"));
+  tb.dispersion_type2 = tb.dispersion_type1;
+  tb.mass1 = tb.mass2 = 1.0;
+  tb.lambda = getd(kv, "tb_lambda", 0.176776695);
+  TwoBody two_body(tb);
+  PropagatorArg prop_arg;
+  prop_arg.n_fermions = 1;
+  Propagator prop1(prop_arg), prop2(prop_arg);
+  vector<complex<Float> > corr(GJP.Tsites(), complex<Float>(0.0, 0.0));
+  Branch b;
+  b.branches = (int)getl(kv, "branches", 2);
+  b.steps = steps;
+  b.levels = levels;
+  b.prop1 = &prop1;
+  b.prop2 = &prop2;
+  b.two_body = &two_body;
+  b.lattice = &lattice;
+  b.hamiltonians.push_back(&kinetic);
+  b.hamiltonians.push_back(&interaction);
+  b.hamiltonians.push_back(&kinetic);
+  b.corr = &corr;
+  const int trees = (int)getl(kv, "trees", 1);
+  for (int r = 0; r < trees; ++r) {
+    prop1.Set(source1.Get(), 0);
+    prop2.Set(source2.Get(), 0);
+    multi_level(b, levels);
+  }
+  FILE* f = open_out(get(kv, "out", "branch.bin"));
+  fwrite(&corr[0], sizeof(complex<Float>), corr.size(), f);
+  fclose(f);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc < 2) {
-    fprintf(stderr, "usage: %s ensemble|bench|rng|gauss|field|lu key=value...\n", argv[0]);
+    fprintf(stderr, "usage: %s ensemble|bench|rng|gauss|field|lu|branch key=value...\n", argv[0]);
     return 2;
   }
   quiet();
@@ -556,6 +666,7 @@ int main(int argc, char** argv) {
   if (cmd == "gauss") return run_rng(kv, true);
   if (cmd == "field") return run_field(kv);
   if (cmd == "lu") return run_lu(kv);
+  if (cmd == "branch") return run_branch(kv);
   fprintf(stderr, "unknown command %s\n", cmd.c_str());
   return 2;
 }

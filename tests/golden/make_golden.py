@@ -227,6 +227,28 @@ def result_files(tmp: str, name: str, sho: dict, **kv) -> dict:
     return res
 
 
+# Multilevel branching trees (production/two_body-branched/main.C:23-80 over
+# the current classes, oracle/ref_build/ref_driver.cc run_branch): L, levels,
+# branches, steps, trees, field, seed; plane-wave sources at p = 0, TGND sink.
+BRANCH_CASES = [(8, 3, 2, 2, 2, "ZTWO", 11), (8, 2, 3, 3, 2, "GAUSS", 11), (4, 4, 2, 1, 2, "ZTWO", 11),
+                (8, 10, 2, 2, 1, "ZTWO", 7)]
+
+
+def branching_cases(tmp: str) -> dict:
+    out = {}
+    for k, (L, levels, branches, steps, trees, field, seed) in enumerate(BRANCH_CASES):
+        fn = os.path.join(tmp, f"br{k}.bin")
+        run_ref("branch", f"L={L}", f"levels={levels}", f"branches={branches}", f"steps={steps}",
+                f"trees={trees}", f"field={field}", f"seed={seed}", "rng=RANLXS2",
+                "couplings=0.019894367886486918", "cutoff=2.0", f"out={fn}")
+        out[f"c{k}_params"] = np.array([L, levels, branches, steps, trees, seed], dtype=np.int64)
+        out[f"c{k}_field"] = np.array(field)
+        out[f"c{k}_corr"] = np.fromfile(fn, dtype=np.complex128)
+    out["cases"] = np.int64(len(BRANCH_CASES))
+    out["couplings"] = np.array([0.019894367886486918])
+    return out
+
+
 def write_sho_dir(sho: dict, shodir: str) -> None:
     os.makedirs(shodir, exist_ok=True)
     for n, lines in sho.items():
@@ -270,7 +292,8 @@ def main() -> None:
     ap.add_argument("--ref", default=os.environ.get("NRCPS_REFERENCE", ""),
                     help="the reference tree (or set NRCPS_REFERENCE)")
     ap.add_argument("--only", default="",
-                    help="regenerate one group only: ohpair, small, config2, trapped48, results, batch_large")
+                    help="regenerate one group only: ohpair, small, config2, trapped48, results, branching, "
+                         "batch_large")
     a = ap.parse_args()
     need_ref = a.only != "batch_large"
     if need_ref and not a.ref:
@@ -344,6 +367,9 @@ def main() -> None:
                 mode="slater2", potential=1, kappa=0.005, ptype="EXP", wavefunc="TGND", tb_disp="STANDARD",
                 tb_lambda=0.176776695, seed=31, rng="RANLXS2", field="ZTWO", couplings="0.019894367886486918",
                 cutoff=0.99999, configs=6, unload=2, cumulants=6))
+    if a.only in ("", "branching"):
+        with tempfile.TemporaryDirectory() as tmp:
+            np.savez_compressed(os.path.join(HERE, "branching.npz"), **branching_cases(tmp))
     if a.only in ("", "batch_large"):
         np.savez_compressed(os.path.join(HERE, "batch_large.npz"), **batch_large())
     print("golden fixtures written to", HERE)

@@ -1,5 +1,7 @@
 """The multilevel branching driver (production/two_body-branched/main.C:23-80)
-breadth first on the device against the oracle's depth-first restatement.
+breadth first on the device against the reference's own recursion over its
+current classes (tests/golden/branching.npz, written by the reference build)
+and the oracle's depth-first restatement.
 
 Tolerances: FP64 1e-12 of each slice's value; FP32 1e-5 against FP64.
 """
@@ -56,3 +58,46 @@ def test_device_branching_fp32_vs_fp64():
         out[prec] = br.run().cpu().numpy()
         br.close()
     assert np.max(np.abs(out["f32"] - out["f64"]) / np.abs(out["f64"])) < 1e-5
+
+
+def _golden_case(g, k):
+    L, levels, branches, steps, trees, seed = (int(v) for v in g[f"c{k}_params"])
+    return L, levels, branches, steps, trees, seed, str(g[f"c{k}_field"])
+
+
+def _local_a(L, couplings):
+    """The one-coupling Interaction's (1 + a phi)/V: a = c(p) V."""
+    return float(O.interaction_table((L,) * 3, 1.0, list(couplings), 1.0, (2 * O.PI) ** 2)[0] * L ** 3)
+
+
+def test_oracle_branching_matches_reference_trees(golden):
+    """The oracle's restatement against the reference's recursion (plane
+    waves at p = 0, TGND sink), every slice to 1e-13."""
+    g = golden("branching.npz")
+    for k in range(int(g["cases"])):
+        L, levels, branches, steps, trees, seed, field = _golden_case(g, k)
+        if levels > 4:
+            continue  # the deep tree runs on the device only
+        src = _sources(L)
+        wf, opp = O.two_body_tables((L,) * 3, "TGND", "STANDARD", 1.0, 0.176776695, (2.0 * O.PI) ** 2)
+        got = O.run_branching(L, levels, branches, steps, trees, "RANLXS2", seed, field,
+                              _local_a(L, g["couplings"]), src, wf, opp)
+        ref = g[f"c{k}_corr"]
+        assert np.max(np.abs(got - ref) / np.abs(ref)) < 1e-13, k
+
+
+@pytest.mark.gpu
+def test_device_branching_fp64_matches_reference_trees(golden):
+    """The device tree walk in FP64 against the reference's recursion,
+    including a 10-level binary tree (1024 leaves), to 1e-12 per slice."""
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    g = golden("branching.npz")
+    for k in range(int(g["cases"])):
+        L, levels, branches, steps, trees, seed, field = _golden_case(g, k)
+        br = nb.Branching(L, levels, branches, steps, _sources(L), seed=seed, field=field,
+                          a=_local_a(L, g["couplings"]), precision="f64", ctx=ctx)
+        got = sum(br.run().cpu().numpy() for _ in range(trees))
+        br.close()
+        ref = g[f"c{k}_corr"]
+        assert np.max(np.abs(got - ref) / np.abs(ref)) < 1e-12, k

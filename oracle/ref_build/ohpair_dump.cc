@@ -44,7 +44,7 @@ int main(int argc, char** argv) {
   const string wf = arg(argc, argv, "wf", "TGND");
   const double lambda = atof(arg(argc, argv, "lambda", "0.25").c_str());
   unsigned long long state = strtoull(arg(argc, argv, "seed", "3").c_str(), nullptr, 10) * 2654435761ull + 1;
-  const string out = arg(argc, argv, "out", "/tmp/ohpair.bin");
+  const string out = arg(argc, argv, "out", "ohpair.bin");
 
   DoArg d;
   d.t_sites = 4;

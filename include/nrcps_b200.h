@@ -106,7 +106,15 @@ const char *nrcps_version(void);
  *                      CUDA-core kernel with FP64 accumulation;
  *   "lu.warp"          1 (default): leading-minor determinants with one warp
  *                      per minor in shared memory (N <= 64); 0: one thread
- *                      per minor with global scratch. */
+ *                      per minor with global scratch;
+ *   "fused.wait_ns"    time limit of every mbarrier wait in the fused step,
+ *                      in nanoseconds (default 2e9, minimum 1000).  A wait
+ *                      that runs out sets the context's time-out flag and
+ *                      its whole cluster leaves the orbital loop; the next
+ *                      nrcps_synchronize returns NRCPS_ERR_TIMEOUT;
+ *   "fused.stall_test" 1: the first wait of one CTA of the next fused steps
+ *                      is made on an mbarrier nothing arrives on, so that it
+ *                      runs out (a test of the time-out path); 0 (default). */
 nrcps_status nrcps_set_option(nrcps_context *ctx, const char *name, long value);
 /* Times every fused-kernel variant (cluster size, lane split) for (prec, L)
  * on this device and keeps the fastest for later calls; *cluster receives

@@ -113,6 +113,11 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
   } else if (n == "fused.kind") {
     if (value < -1 || value > 10) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
     ctx->fused_kind = (int)value;
+  } else if (n == "fused.wait_ns") {
+    if (value < 1000) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.wait_ns below 1000 ns");
+    ctx->fused_wait_ns = (unsigned long long)value;
+  } else if (n == "fused.stall_test") {
+    ctx->fused_stall_test = value != 0;
   } else if (n == "lu.warp") {
     ctx->lu_warp = value != 0;
   } else if (n == "overlap.tc") {

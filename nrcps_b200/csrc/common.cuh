@@ -102,8 +102,15 @@ struct Context {
   // TF32 hi / lo split of the sources for nrcps_overlap's tensor-core path (grown on demand)
   void* tc_split = nullptr;
   size_t tc_split_bytes = 0;
-  // FP32 copy of a kinetic table for nrcps_propagate(F32).
   int* dev_err = nullptr;  // device flag set by kernels whose bounded waits time out
+  // Time limit of every mbarrier wait in the fused step (nanoseconds of the
+  // GPU's global timer; the legitimate waits take microseconds).
+  unsigned long long fused_wait_ns = 2000000000ull;
+  // Time-out test: the first wait of one CTA of the fused step is on an
+  // mbarrier nothing arrives on, so that it runs out (nrcps_synchronize then
+  // reports NRCPS_ERR_TIMEOUT and the context stays usable).
+  int fused_stall_test = 0;
+  // FP32 copy of a kinetic table for nrcps_propagate(F32).
   float2* kin_f32 = nullptr;  // (hi, lo) split of the last table
   long kin_f32_len = 0;
 };

@@ -50,6 +50,8 @@ struct FusedArgs {
   double inv_vol;          // 1 / vol (a product per site instead of a division)
   double w_plus, w_minus;  // (1 + a)/V and (1 - a)/V for Z2 fields
   int* err;                // device flag: 1 = a bounded wait timed out
+  unsigned long long wait_ns;  // time limit of every mbarrier wait (%globaltimer nanoseconds)
+  int stall_test;          // 1: the first wait of CTA 0 of cluster 0 is on an mbarrier nothing arrives on
 };
 
 // x * w for the position-space factor of site `site` (general modes).
@@ -127,7 +129,8 @@ struct FusedShape {
   static constexpr int WORK = C * REGION;     // padded working copy of the slab
   static constexpr int STAGE = S * L * L;     // unpadded slab, landing zone of the bulk copy
   static constexpr int THREADS = S * L;       // one pencil per thread per pass
-  static constexpr size_t SMEM = sizeof(cplx<R>) * (size_t)(STAGE + WORK) + 16;  // + mbarrier
+  // + the slab's mbarrier, the time-out test's idle mbarrier and the cluster's abort word
+  static constexpr size_t SMEM = sizeof(cplx<R>) * (size_t)(STAGE + WORK) + 32;
   static constexpr int CTAS_PER_SM = (int)(228 * 1024 / (SMEM + 1024)) > 4 ? 4 : (int)(228 * 1024 / (SMEM + 1024));
   static constexpr int MIN_BLOCKS = CTAS_PER_SM < 1 ? 1 : CTAS_PER_SM;
   static_assert(L % C == 0, "cluster size must divide L");
@@ -153,23 +156,69 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                : "memory");
 }
 
+// One poll of an mbarrier phase; ACQ_CLUSTER: acquire at cluster scope (the
+// awaited bytes were written by other CTAs of the cluster).
+template <bool ACQ_CLUSTER = false>
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
+  if constexpr (ACQ_CLUSTER)
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+  else
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
   return ok != 0;
 }
 
-// Bounded wait: gives up after ~2^24 polls (seconds), records the timeout
-// in *err and returns false; the kernel then finishes without hanging.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
-  for (int i = 0; i < (1 << 24); ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  if (err) atomicExch(err, 1);
-  return false;
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for a phase: true once it completed; false when the cluster's
+// abort word (this CTA's copy, written by whichever CTA gave up first) is
+// raised, or when f.wait_ns of wall time passed -- then the timeout is
+// recorded in *f.err.  A false return is acted on by the caller: the whole
+// cluster leaves its orbital loop (see the abort paths of the kernels).
+// abort_word = nullptr: the final wait of an abort path (only the time limit).
+template <bool ACQ_CLUSTER = false>
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, const FusedArgs& f,
+                                                  const volatile int* abort_word) {
+  if (mbar_try_wait<ACQ_CLUSTER>(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait<ACQ_CLUSTER>(bar, parity)) return true;
+    if (abort_word && *abort_word) return false;
+    if (global_ns() - t0 > f.wait_ns) {
+      if (f.err) atomicExch(f.err, 1);
+      return false;
+    }
+  }
+}
+
+// Raises the abort word of every CTA of the cluster (C = 1: this CTA's).
+template <int C>
+__device__ __forceinline__ void raise_abort(cg::cluster_group& cluster, int* abort_word) {
+#pragma unroll
+  for (int r = 0; r < C; ++r) {
+    volatile int* w = C > 1 ? cluster.map_shared_rank(abort_word, r) : abort_word;
+    *w = 1;
+  }
+  __threadfence_block();
+}
+
+// The time-out test's stand-in for a stuck copy: the first wait of CTA 0 of
+// cluster 0 is on `idle`, an initialised mbarrier nothing ever arrives on.
+__device__ __forceinline__ bool stall_here(const FusedArgs& f, long cluster_id, int rank, bool first) {
+  return f.stall_test && first && cluster_id == 0 && rank == 0;
 }
 
 // Prefetch of a global range into L2 by the bulk copy engine (no completion).
@@ -185,7 +234,7 @@ template <typename R, int L, int C, bool STAGED>
 struct PullShape {
   using Base = FusedShape<R, L, C>;
   static constexpr int THREADS = Base::THREADS;
-  static constexpr size_t SMEM = STAGED ? Base::SMEM : sizeof(cplx<R>) * (size_t)Base::WORK + 16;
+  static constexpr size_t SMEM = STAGED ? Base::SMEM : sizeof(cplx<R>) * (size_t)Base::WORK + 32;
   static constexpr int FIT = (int)(228 * 1024 / (SMEM + 1024));
   static constexpr int MIN_BLOCKS = STAGED ? Base::MIN_BLOCKS : (FIT > 4 ? 4 : (FIT < 1 ? 1 : FIT));
 };
@@ -201,6 +250,8 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
   cplx<R>* stage = reinterpret_cast<cplx<R>*>(smem_raw);
   cplx<R>* sm = stage + (STAGED ? Sh::STAGE : 0);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Sh::WORK);
+  uint64_t* idle = bar + 1;                              // the time-out test's mbarrier
+  int* abort_word = reinterpret_cast<int*>(bar + 2);     // raised by the first CTA that gives up
 
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
@@ -222,13 +273,27 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
   // one product per component instead of the hi + lo product
   const bool w_exact = wp_lo == (R)0 && wm_lo == (R)0;
 
-  if (STAGED && tid == 0) mbar_init(bar);
-  __syncthreads();
+  if (tid == 0) {
+    *reinterpret_cast<volatile int*>(abort_word) = 0;
+    if constexpr (STAGED) {
+      mbar_init(bar);
+      mbar_init(idle);
+    }
+  }
+  // every CTA's abort word is set up before any peer can raise it
+  if constexpr (C > 1) cluster.sync();
+  else __syncthreads();
   uint32_t parity = 0;
+  bool outstanding = false;  // a slab copy on `bar` (phase `parity`) that nobody has waited for
+  bool aborted = false;
   long orb = cluster_id;
-  if (tid == 0 && orb < f.n_orb_total) {
-    if constexpr (STAGED) bulk_load(stage, slab(orb), STAGE_BYTES, bar);
-    else prefetch_l2(slab(orb), STAGE_BYTES);
+  if (orb < f.n_orb_total) {
+    if constexpr (STAGED) {
+      if (tid == 0) bulk_load(stage, slab(orb), STAGE_BYTES, bar);
+      outstanding = true;
+    } else if (tid == 0) {
+      prefetch_l2(slab(orb), STAGE_BYTES);
+    }
   }
 
   for (; orb < f.n_orb_total; orb += n_clusters) {
@@ -236,9 +301,10 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
     const uint64_t kb = f.off0 + (f.conf_base ? __ldg(f.conf_base + conf) : (uint64_t)conf * f.conf_stride);  // field offset of this configuration
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> x[L];
+    bool ok = true;
     if constexpr (STAGED) {
-      mbar_wait_bounded(bar, parity, f.err);
-      parity ^= 1u;
+      ok = stall_here(f, cluster_id, c, orb == cluster_id) ? mbar_wait_bounded(idle, 0u, f, abort_word)
+                                                           : mbar_wait_bounded(bar, parity, f, abort_word);
     } else if (tid == 0 && orb + n_clusters < f.n_orb_total) {
       prefetch_l2(slab(orb + n_clusters), STAGE_BYTES);
     }
@@ -268,11 +334,22 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
 #pragma unroll
       for (int y = 0; y < L; ++y) sm[off(y / S, xl, y % S, z)] = x[y];
     }
-    __syncthreads();
-    // the staging buffer is free: prefetch this cluster's next orbital
-    if (STAGED && tid == 0 && orb + n_clusters < f.n_orb_total) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      bulk_load(stage, slab(orb + n_clusters), STAGE_BYTES, bar);
+    if constexpr (STAGED) {
+      if (__syncthreads_or(!ok)) {
+        // the slab copy timed out (or a peer gave up): no further copy on
+        // `bar`; the whole cluster leaves after the next cluster barrier
+        if (tid == 0) raise_abort<C>(cluster, abort_word);
+      } else {
+        parity ^= 1u;
+        outstanding = orb + n_clusters < f.n_orb_total;
+        // the staging buffer is free: prefetch this cluster's next orbital
+        if (tid == 0 && outstanding) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          bulk_load(stage, slab(orb + n_clusters), STAGE_BYTES, bar);
+        }
+      }
+    } else {
+      __syncthreads();
     }
     // ---- 2. forward DFT along z in place: thread -> (xl, y)
     {
@@ -290,6 +367,15 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
     // touches only region c of its peers, so the accesses are disjoint).
     if constexpr (C > 1) cluster.sync();
     else __syncthreads();
+    if constexpr (STAGED) {
+      // an abort word is raised only before this barrier (after the slab
+      // wait) and read only between it and the next one: every CTA of the
+      // cluster takes the same decision
+      if (*reinterpret_cast<volatile int*>(abort_word)) {
+        aborted = true;
+        break;
+      }
+    }
     {
       cplx<R>* base[C];
 #pragma unroll
@@ -357,6 +443,11 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
     // working-copy elements it read in step 5, and peers touch this CTA's
     // shared memory only between the barriers of step 3: no barrier needed.
   }
+  if constexpr (STAGED) {
+    // leaving early: the slab copy this CTA started last lands before its
+    // shared memory goes away (bounded like every other wait)
+    if (aborted && outstanding && tid == 0) mbar_wait_bounded(bar, parity, f, nullptr);
+  }
   // keep shared memory alive until every CTA of the cluster is done with it
   if constexpr (C > 1) cluster.sync();
 }
@@ -389,6 +480,8 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
   cplx<R>* stage = reinterpret_cast<cplx<R>*>(smem_raw);
   cplx<R>* sm = stage + Sh::STAGE;
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Sh::WORK);
+  uint64_t* idle = bar + 1;                           // the time-out test's mbarrier
+  int* abort_word = reinterpret_cast<int*>(bar + 2);  // raised by the first CTA that gives up
 
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
@@ -411,19 +504,30 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
   // one product per component instead of the hi + lo product
   const bool w_exact = wp_lo == (R)0 && wm_lo == (R)0;
 
-  if (tid == 0) mbar_init(bar);
-  __syncthreads();
+  if (tid == 0) {
+    *reinterpret_cast<volatile int*>(abort_word) = 0;
+    mbar_init(bar);
+    mbar_init(idle);
+  }
+  // every CTA's abort word is set up before any peer can raise it
+  if constexpr (C > 1) cluster.sync();
+  else __syncthreads();
   uint32_t parity = 0;
+  bool outstanding = false;  // a slab copy on `bar` (phase `parity`) that nobody has waited for
+  bool aborted = false;
   long orb = cluster_id;
-  if (tid == 0 && orb < f.n_orb_total) bulk_load(stage, slab(orb), STAGE_BYTES, bar);
+  if (orb < f.n_orb_total) {
+    if (tid == 0) bulk_load(stage, slab(orb), STAGE_BYTES, bar);
+    outstanding = true;
+  }
 
   for (; orb < f.n_orb_total; orb += n_clusters) {
     const long conf = orb / f.batch;
     const uint64_t kb = f.off0 + (f.conf_base ? __ldg(f.conf_base + conf) : (uint64_t)conf * f.conf_stride);
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> v[H];
-    mbar_wait_bounded(bar, parity, f.err);
-    parity ^= 1u;
+    const bool ok = stall_here(f, cluster_id, c, orb == cluster_id) ? mbar_wait_bounded(idle, 0u, f, abort_word)
+                                                                    : mbar_wait_bounded(bar, parity, f, abort_word);
     // ---- 1. k(p), forward DFT along y from the staged slab: pencil (xl, z)
     {
       const int z = p % L, xl = p / L;
@@ -440,10 +544,17 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
         sm[off(y / S, xl, y % S, z)] = v[k];
       }
     }
-    __syncthreads();
-    if (tid == 0 && orb + n_clusters < f.n_orb_total) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      bulk_load(stage, slab(orb + n_clusters), STAGE_BYTES, bar);
+    if (__syncthreads_or(!ok)) {
+      // the slab copy timed out (or a peer gave up): no further copy on
+      // `bar`; the whole cluster leaves after the next cluster barrier
+      if (tid == 0) raise_abort<C>(cluster, abort_word);
+    } else {
+      parity ^= 1u;
+      outstanding = orb + n_clusters < f.n_orb_total;
+      if (tid == 0 && outstanding) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        bulk_load(stage, slab(orb + n_clusters), STAGE_BYTES, bar);
+      }
     }
     // ---- 2. forward DFT along z in place: pencil (xl, y)
     {
@@ -458,6 +569,11 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
     }
     if constexpr (C > 1) cluster.sync();
     else __syncthreads();
+    // raised only before this barrier, read only before the next: one decision per cluster
+    if (*reinterpret_cast<volatile int*>(abort_word)) {
+      aborted = true;
+      break;
+    }
     // ---- 3. x: forward DFT, times w, backward DFT through DSMEM: pencil (yl, z)
     {
       cplx<R>* base[C];
@@ -540,6 +656,8 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
     // pair must be done reading first
     __syncwarp();
   }
+  // leaving early: the slab copy this CTA started last lands first (bounded)
+  if (aborted && outstanding && tid == 0) mbar_wait_bounded(bar, parity, f, nullptr);
   if constexpr (C > 1) cluster.sync();
 }
 
@@ -553,24 +671,6 @@ __device__ __forceinline__ uint32_t mapa_u32(uint32_t addr, uint32_t rank) {
 __device__ __forceinline__ void expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-
-// Bounded wait with cluster-scope acquire: the awaited bytes were written
-// by other CTAs of the cluster.
-__device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_t parity, int* err) {
-  for (int i = 0; i < (1 << 24); ++i) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  if (err) atomicExch(err, 1);
-  return false;
-}
-
 
 // ------------------------------------------------ bulk-copy exchange variant
 // Same passes, but both exchanges move whole padded regions with the bulk
@@ -637,6 +737,8 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
   uint64_t* bar_hbm = reinterpret_cast<uint64_t*>(smem_raw);
   uint64_t* bar_recv = bar_hbm + 1;
   uint64_t* bar_work = bar_hbm + 2;
+  uint64_t* idle = bar_hbm + 3;                           // the time-out test's mbarrier
+  int* abort_word = reinterpret_cast<int*>(bar_hbm + 4);  // raised by the first CTA that gives up
   cplx<R>* stage = reinterpret_cast<cplx<R>*>(smem_raw + 128);
   cplx<R>* work = stage + (STAGED ? Sh::STAGE : 0);
   cplx<R>* recv = work + Sh::WORK;
@@ -671,29 +773,49 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
   const bool w_exact = wp_lo == (R)0 && wm_lo == (R)0;
 
   if (tid == 0) {
+    *reinterpret_cast<volatile int*>(abort_word) = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar_hbm)) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar_recv)) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar_work)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(idle)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if constexpr (KSM)
     for (int i = tid; i < Sh::STAGE; i += Bs::THREADS) kin_s[i] = __ldg(f.kin_f + (size_t)c * Sh::STAGE + i);
-  cluster.sync();  // every CTA's mbarriers are initialised before any copy targets them
+  cluster.sync();  // every CTA's mbarriers and abort word are set up before any copy or abort targets them
   uint32_t parity = 0;
+  // phases this CTA expects bytes on and has not yet seen complete (all
+  // three barriers advance one phase per orbital, so `parity` is theirs)
+  bool hbm_out = false, recv_out = false, work_out = false;
+  uint32_t hbm_phase = 0;  // phase of the outstanding HBM slab copy
+  bool aborted = false;
+  const volatile int* abort_flag = abort_word;
   long orb = cluster_id;
-  if (tid == 0 && orb < f.n_orb_total) {
-    if constexpr (STAGED) bulk_load(stage, slab(orb), Bs::STAGE_BYTES, bar_hbm);
-    else prefetch_l2(slab(orb), Bs::STAGE_BYTES);
+  if (orb < f.n_orb_total) {
+    if constexpr (STAGED) {
+      if (tid == 0) bulk_load(stage, slab(orb), Bs::STAGE_BYTES, bar_hbm);
+      hbm_out = true;
+    } else if (tid == 0) {
+      prefetch_l2(slab(orb), Bs::STAGE_BYTES);
+    }
   }
+  // A CTA that gives up (a wait timed out, or it found the abort word
+  // raised) raises every peer's abort word and leaves the loop at its next
+  // block barrier, before it issues another copy; its peers' waits see the
+  // word and they follow.  Every wait is bounded, so every CTA reaches the
+  // exit.
 
   for (; orb < f.n_orb_total; orb += n_clusters) {
     const long conf = orb / f.batch;
     const uint64_t kb = f.off0 + (f.conf_base ? __ldg(f.conf_base + conf) : (uint64_t)conf * f.conf_stride);
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> x[L];
+    const bool first = orb == cluster_id;
+    bool ok = true;
     if constexpr (STAGED) {
-      mbar_wait_bounded(bar_hbm, parity, f.err);
+      ok = stall_here(f, cluster_id, c, first) ? mbar_wait_bounded(idle, 0u, f, abort_word)
+                                               : mbar_wait_bounded(bar_hbm, parity, f, abort_word);
     } else if (tid == 0 && orb + n_clusters < f.n_orb_total) {
       prefetch_l2(slab(orb + n_clusters), Bs::STAGE_BYTES);
     }
@@ -723,9 +845,14 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
 #pragma unroll
       for (int y = 0; y < L; ++y) work[off(y / S, xl, y % S, z)] = x[y];
     }
-    __syncthreads();
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
     if constexpr (STAGED) {
-      if (tid == 0 && orb + n_clusters < f.n_orb_total) {
+      hbm_out = orb + n_clusters < f.n_orb_total;  // the next slab, on the barrier's next phase
+      hbm_phase = parity ^ 1u;
+      if (tid == 0 && hbm_out) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         bulk_load(stage, slab(orb + n_clusters), Bs::STAGE_BYTES, bar_hbm);
       }
@@ -741,14 +868,19 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
       for (int j = 0; j < L; ++j) row[j] = x[j];
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> bulk copy reads
-    __syncthreads();
+    if (__syncthreads_or(*abort_flag != 0)) {  // a peer gave up: send nothing more
+      aborted = true;
+      break;
+    }
     if (tid < C) {
       const uint32_t dst = mapa_u32(smem_u32(recv + c * REGION), (uint32_t)tid);
       const uint32_t bar = mapa_u32(smem_u32(bar_recv), (uint32_t)tid);
       bulk_to_peer(dst, work + tid * REGION, Bs::REGION_BYTES, bar);
     }
     if (tid == 0) expect_tx(bar_recv, Bs::XBYTES);
-    mbar_wait_cluster_bounded(bar_recv, parity, f.err);
+    recv_out = true;
+    ok = (!STAGED && stall_here(f, cluster_id, c, first)) ? mbar_wait_bounded(idle, 0u, f, abort_word)
+                                                          : mbar_wait_bounded<true>(bar_recv, parity, f, abort_word);
     // ---- 3. x: forward DFT, times w, backward DFT on the pencils of y-slab c, in recv
     {
       const int z = tid % L, yl = tid / L;
@@ -782,15 +914,19 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
       for (int xx = 0; xx < L; ++xx) recv[off(xx / S, xx % S, yl, z)] = x[xx];
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
+    if (__syncthreads_or(!ok || *abort_flag != 0)) {
+      aborted = true;
+      break;
+    }
+    recv_out = false;
     if (tid < C) {
       const uint32_t dst = mapa_u32(smem_u32(work + c * REGION), (uint32_t)tid);
       const uint32_t bar = mapa_u32(smem_u32(bar_work), (uint32_t)tid);
       bulk_to_peer(dst, recv + tid * REGION, Bs::REGION_BYTES, bar);
     }
     if (tid == 0) expect_tx(bar_work, Bs::XBYTES);
-    mbar_wait_cluster_bounded(bar_work, parity, f.err);
-    parity ^= 1u;
+    work_out = true;
+    ok = mbar_wait_bounded<true>(bar_work, parity, f, abort_word);
     // ---- 4. backward DFT along z in place
     {
       const int y = tid % L, xl = tid / L;
@@ -801,7 +937,12 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
 #pragma unroll
       for (int j = 0; j < L; ++j) row[j] = x[j];
     }
-    __syncthreads();
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+    work_out = false;
+    parity ^= 1u;
     // ---- 5. backward DFT along y, times k(p), streaming stores
     {
       const int z = tid % L, xl = tid / L;
@@ -821,6 +962,20 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
     // Pass 1 of the next orbital writes, per thread, the work elements this
     // thread read in pass 5; no copy reads work between pass 4 and the next
     // pass 2 (all copies out of work completed before this CTA's recv filled).
+  }
+  if (aborted) {
+    if (tid == 0) {
+      raise_abort<C>(cluster, abort_word);
+      // Copies into this CTA whose bytes it announced either land or time
+      // out here; then a short grace period for the copies its peers issued
+      // just before they saw the abort word (each lands within microseconds).
+      if (hbm_out) mbar_wait_bounded(bar_hbm, hbm_phase, f, nullptr);
+      if (recv_out) mbar_wait_bounded<true>(bar_recv, parity, f, nullptr);
+      if (work_out) mbar_wait_bounded<true>(bar_work, parity, f, nullptr);
+      const unsigned long long t0 = global_ns();
+      while (global_ns() - t0 < 20000ull) __nanosleep(1000);
+    }
+    __syncthreads();
   }
   cluster.sync();  // no CTA leaves while a copy may still target it
 }
@@ -1055,6 +1210,8 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   f.w_plus = 1.0 / V;
   f.w_minus = 1.0 / V;
   f.err = ctx->dev_err;
+  f.wait_ns = ctx->fused_wait_ns;
+  f.stall_test = 0;
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -1130,6 +1287,8 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   f.w_plus = (1.0 + f.a) / f.vol;
   f.w_minus = (1.0 - f.a) / f.vol;
   f.err = ctx->dev_err;
+  f.wait_ns = ctx->fused_wait_ns;
+  f.stall_test = ctx->fused_stall_test;
   if (f.n_orb_total == 0) return NRCPS_OK;
   init_choices();
   const int L = d[0];

@@ -230,21 +230,80 @@ def _job_from_golden(args, precision):
     return j
 
 
+def _golden_sources(g, args, dims):
+    """The fixture's dense sources; fixtures too large to hold them store every
+    k-th entry, and the sources are rebuilt by the library's OneBody::Set
+    (nrcps_sho_source) and checked against that sample."""
+    if "sources" in g.files:
+        return g["sources"]
+    sho = json.load(open(os.path.join(GOLDEN, "sho_coefficients.json")))
+    lam = (float(args["lambda1"]), float(args["lambda2"]), float(args["lambda3"]))
+    src = np.stack([nb.sho_source(dims, lam, sho[str(n)]) for n in range(int(args["N"]))])
+    assert np.array_equal(src[:, ::int(g["sources_stride"])], g["sources_sample"])
+    return src
+
+
+def _ensemble_from_golden(g, args, job, ctx):
+    if "momenta" in g.files and args.get("sources", "mom") == "mom":
+        idx, _, _ = nb.momenta(job.dims, "PERFECT", 1.0, float(args["ef"]), job.cutoff)
+        return nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
+    return nb.Ensemble(job, sources=_golden_sources(g, args, job.dims), ctx=ctx)
+
+
+def per_tau_rel_err(got, ref):
+    """max over configurations and minors of |got - ref| / |ref|, per slice."""
+    got, ref = np.asarray(got), np.asarray(ref)
+    e = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
+    return e.reshape(-1, e.shape[-2], e.shape[-1]).max(axis=(0, 2))
+
+
+# config 1 (L=16, N=7, T=32), small lattices with several couplings, Gaussian
+# fields and the trapped form, and the reference's own runs at the batched
+# workload's shape (L=32, N=19, T=64, 2 configurations) and at the trapped
+# workload's (L=48, T=128, SHO N=10, [K,V,I,V,K], pair sink, 2 configurations)
 @pytest.mark.parametrize("name", ["ensemble_config1.npz", "ensemble_multicoupling.npz", "ensemble_gauss.npz",
-                                  "ensemble_trapped.npz"])
+                                  "ensemble_trapped.npz", "ensemble_config2.npz", "ensemble_trapped48.npz"])
 def test_ensemble_fp64_matches_reference(golden, ctx, name):
     g = golden(name)
     args = json.loads(str(g["args"]))
     job = _job_from_golden(args, "f64")
-    if "momenta" in g.files and args.get("sources", "mom") == "mom":
-        idx, _, _ = nb.momenta(job.dims, "PERFECT", 1.0, float(args["ef"]), job.cutoff)
-        ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
-    else:
-        ens = nb.Ensemble(job, sources=g["sources"], ctx=ctx)
+    ens = _ensemble_from_golden(g, args, job, ctx)
     dets = ens.run(0).cpu().numpy()
+    ens.close()
     ref = g["dets"]
     assert dets.shape == ref.shape
-    assert rel_err(dets, ref) < FP64_REL
+    err = per_tau_rel_err(dets, ref)
+    print(f"{name}: FP64 vs reference, max rel err per tau: " + " ".join(f"{v:.1e}" for v in err))
+    assert err.max() < FP64_REL, err.max()
+
+
+def test_trapped_workload_fp32_vs_fp64_full_shape(golden, ctx):
+    """The trapped workload at its own shape and size: L=48, T=128, SHO N=10,
+    [K,V,I,V,K] with kappa = 0.005, pair sink, Z2 a=0.5, RANLXS2 seed 31,
+    1024 configurations.  FP32 propagation (dense FP32 overlap on the tensor
+    cores) against the FP64 mode -- which the fixture test above holds to the
+    reference -- on the same fields: the correlators
+    C_m(tau) = <det S2_m(tau)> (production/slater_det2_trapped/main-no_cum.C:205-207)
+    within 1e-5 relative at every tau."""
+    g = golden("ensemble_trapped48.npz")
+    args = json.loads(str(g["args"]))
+    out = {}
+    for prec in ("f32", "f64"):
+        job = _job_from_golden(args, prec)
+        job.n_conf = 1024
+        ens = _ensemble_from_golden(g, args, job, ctx)
+        d = ens.run(0)
+        out[prec] = d.mean(0).cpu().numpy()  # [T, 2N]
+        scale = d.abs().mean(0).cpu().numpy()
+        ens.close()
+        del d
+    c32, c64 = out["f32"], out["f64"]
+    err = np.max(np.abs(c32 - c64) / np.abs(c64), axis=1)
+    err_scale = np.max(np.abs(c32 - c64) / scale, axis=1)
+    print("trapped L=48 T=128 1024 conf: FP32 vs FP64, max rel err of C(tau) per tau: " +
+          " ".join(f"{v:.1e}" for v in err))
+    print("  relative to <|det|>: " + " ".join(f"{v:.1e}" for v in err_scale))
+    assert err.max() < FP32_REL, err.max()
 
 
 def test_ensemble_fp32_config1(golden, ctx):
@@ -476,6 +535,50 @@ def test_synchronize_reports_no_timeout(ctx):
     psi, kinv, bits = _random_step_inputs(ctx, 32, 2, 2, "f32")
     nb.propagate(psi, 2, kinv, bits, 0.5, ctx=ctx)
     ctx.synchronize()  # raises NrcpsError(TIMEOUT) if a bounded wait gave up
+
+
+# every fused kernel with mbarrier waits: peer access with a staged slab (0,
+# also as a one-CTA cluster), lane split (1), bulk exchange staged (2) and via
+# L2 (3)
+_WAITING_VARIANTS = [(0, "f32", 32, 8), (0, "f32", 16, 1), (1, "f32", 32, 8), (2, "f32", 32, 8), (3, "f32", 32, 8),
+                     (3, "f64", 32, 16)]
+
+
+@pytest.mark.parametrize("kind,precision,L,cluster", _WAITING_VARIANTS)
+def test_fused_wait_time_out_is_reported_and_context_survives(ctx, kind, precision, L, cluster):
+    """A wait that runs out: the first wait of CTA 0 of cluster 0 is made on
+    an mbarrier nothing arrives on (a stand-in for a copy that never lands),
+    with a 2 ms limit.  Its cluster leaves the orbital loop together, the
+    launch ends in milliseconds, nrcps_synchronize reports TIMEOUT, and the
+    next step on the same context is bit-identical to a clean run."""
+    import time
+    psi, kinv, bits = _random_step_inputs(ctx, L, 3, 5, precision, seed=8)
+    try:
+        ctx.set_option("fused.kind", kind)
+        ctx.set_option("fused.cluster", cluster)
+        ref = psi.clone()
+        nb.propagate(ref, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.synchronize()
+        ctx.set_option("fused.wait_ns", 2_000_000)
+        ctx.set_option("fused.stall_test", 1)
+        bad = psi.clone()
+        t0 = time.perf_counter()
+        nb.propagate(bad, 5, kinv, bits, 0.5, ctx=ctx)
+        with pytest.raises(nb.NrcpsError) as err:
+            ctx.synchronize()
+        assert err.value.status == 7  # NRCPS_ERR_TIMEOUT
+        assert time.perf_counter() - t0 < 5.0
+        ctx.set_option("fused.stall_test", 0)
+        ctx.set_option("fused.wait_ns", 2_000_000_000)
+        again = psi.clone()
+        nb.propagate(again, 5, kinv, bits, 0.5, ctx=ctx)
+        ctx.synchronize()
+        assert torch.equal(again, ref)
+    finally:
+        ctx.set_option("fused.stall_test", 0)
+        ctx.set_option("fused.wait_ns", 2_000_000_000)
+        ctx.set_option("fused.cluster", 0)
+        ctx.set_option("fused.kind", -1)
 
 
 # ------------------------------------------------ re-orthonormalisation

@@ -100,6 +100,9 @@ const char *nrcps_version(void);
  *                      of staged in shared memory (four CTAs per SM);
  *                      9, 10: kinds 6, 3 with the CTA's slab of the
  *                      kinetic table resident in shared memory (FP32);
+ *                      11, 12: kinds 7, 8 with the x pass written back by
+ *                      st.async onto the owner CTA's mbarrier (one cluster
+ *                      barrier per orbital);
  *   "overlap.tc"       1 (default): dense-source overlaps of FP32 orbitals
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the
@@ -120,6 +123,12 @@ nrcps_status nrcps_set_option(nrcps_context *ctx, const char *name, long value);
  * on this device and keeps the fastest for later calls; *cluster receives
  * its cluster size, negated for the lane-split variants (may be NULL). */
 nrcps_status nrcps_autotune(nrcps_context *ctx, nrcps_precision prec, int L, int *cluster);
+/* The fused-kernel variant that nrcps_propagate uses for (prec, L^3) on this
+ * context's device under its current options (no counterpart in the
+ * reference; it names the kernel behind a measurement): *kind (0..12, see
+ * "fused.kind") and *cluster (CTAs per cluster); both -1 when no fused
+ * variant serves the shape.  Tunes nothing. */
+nrcps_status nrcps_fused_choice(nrcps_context *ctx, nrcps_precision prec, int L, int *kind, int *cluster);
 
 /* ----------------------------------------------------- host-side tables
  * Replace the reference's host constructors' table builds so that callers

@@ -81,6 +81,7 @@ SIGNATURES = {
     "nrcps_version": ([], ctypes.c_char_p),
     "nrcps_set_option": ([_P, ctypes.c_char_p, _L], _I),
     "nrcps_autotune": ([_P, _I, _I, _IP], _I),
+    "nrcps_fused_choice": ([_P, _I, _I, _IP, _IP], _I),
     "nrcps_dispersion_table": ([_IP, _I, _D, _I, _D, _DP], _I),
     "nrcps_kinetic_table": ([_IP, _I, _D, _D, _D, _DP], _I),
     "nrcps_interaction_table": ([_IP, _D, _I, _DP, _I, _D, _D, _DP], _I),

@@ -70,7 +70,7 @@ class Context:
 
     def set_option(self, name: str, value: int) -> None:
         """nrcps_set_option: "propagate.fused" (1/0), "fused.cluster" (0 = autotuned),
-        "fused.split" (-1 = autotuned, 0, 1), "fused.kind" (-1 = autotuned, 0..10)."""
+        "fused.split" (-1 = autotuned, 0, 1), "fused.kind" (-1 = autotuned, 0..12)."""
         self.check(lib().nrcps_set_option(self.handle, name.encode(), int(value)), "set_option")
 
     def autotune(self, precision: str, L: int) -> int:
@@ -78,6 +78,13 @@ class Context:
         c = ctypes.c_int()
         self.check(lib().nrcps_autotune(self.handle, _prec(precision), L, ctypes.byref(c)), "autotune")
         return c.value
+
+    def fused_choice(self, precision: str, L: int):
+        """(kind, cluster) of the fused kernel nrcps_propagate runs for (precision, L^3); (-1, -1) if none."""
+        k, c = ctypes.c_int(), ctypes.c_int()
+        self.check(lib().nrcps_fused_choice(self.handle, _prec(precision), L, ctypes.byref(k), ctypes.byref(c)),
+                   "fused_choice")
+        return k.value, c.value
 
     def close(self) -> None:
         if self.handle:

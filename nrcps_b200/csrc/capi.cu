@@ -97,6 +97,7 @@ extern "C" nrcps_status nrcps_set_stream(nrcps_context* ctx, void* stream) {
 
 namespace nrcps {
 nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster);
+nrcps_status fused_choice(nrcps_context* ctx, nrcps_precision prec, int L, int* kind, int* cluster);
 }
 
 extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, long value) {
@@ -111,7 +112,7 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
     if (value < -1 || value > 1) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.split out of range");
     ctx->fused_split = (int)value;
   } else if (n == "fused.kind") {
-    if (value < -1 || value > 10) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
+    if (value < -1 || value > 12) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
     ctx->fused_kind = (int)value;
   } else if (n == "fused.wait_ns") {
     if (value < 1000) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.wait_ns below 1000 ns");
@@ -132,6 +133,12 @@ extern "C" nrcps_status nrcps_autotune(nrcps_context* ctx, nrcps_precision prec,
   if (!ctx || L <= 0 || L >= 64) return NRCPS_ERR_INVALID_ARGUMENT;
   if (cluster) *cluster = 0;
   return fused_autotune(ctx, prec, L, cluster);
+}
+
+extern "C" nrcps_status nrcps_fused_choice(nrcps_context* ctx, nrcps_precision prec, int L, int* kind, int* cluster) {
+  if (!ctx || !kind || !cluster || L <= 0) return NRCPS_ERR_INVALID_ARGUMENT;
+  if (prec != NRCPS_F32 && prec != NRCPS_F64) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "bad precision");
+  return fused_choice(ctx, prec, L, kind, cluster);
 }
 
 // Waits for the context's stream, then reports a timed-out bounded wait in

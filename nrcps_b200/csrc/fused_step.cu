@@ -980,21 +980,270 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
   cluster.sync();  // no CTA leaves while a copy may still target it
 }
 
+// ------------------------------------------------ asynchronous write-back variant
+// The x pass reads its pencils from the peers' shared memory as kind 7 does,
+// but stores the results back with st.async, each store completing on the
+// owner CTA's mbarrier (complete_tx).  A CTA starts its inverse z pass as
+// soon as every write-back into its slab has landed, so the second cluster
+// barrier of the step goes away, and with it that barrier's cluster-wide
+// release, which orders every outstanding memory operation of the thread,
+// the HBM stores of the previous orbital included.  The one remaining
+// cluster barrier (after pass 2) orders shared memory only: since its last
+// crossing the CTA has written nothing but its own shared memory (the
+// write-backs are tracked by the receivers' mbarriers), so its release is
+// restricted to shared::cta.  The slab is prefetched into L2 (as kind 7).
+// Addresses into the peers' shared memory are 32-bit shared::cluster ones
+// (mapa), which also keeps the pass-3 pointers out of 64-bit registers.
+//
+// Reuse without further signals: a peer reads and writes back region c of
+// this CTA only between the cluster barrier and the completion of this
+// CTA's mbarrier phase (it reads before it writes back, and the phase needs
+// all of its write-backs); this CTA touches that region again only after
+// the phase completed.
+__device__ __forceinline__ void cluster_barrier_shared_release() {
+  asm volatile("fence.release.sync_restrict::shared::cta.cluster;" ::: "memory");
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+  asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
+}
+
+template <typename R>
+__device__ __forceinline__ cplx<R> ld_cluster(uint32_t addr) {
+  cplx<R> v;
+  if constexpr (sizeof(R) == 4)
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.re), "=f"(v.im) : "r"(addr) : "memory");
+  else
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.re), "=d"(v.im) : "r"(addr) : "memory");
+  return v;
+}
+
+template <typename R>
+__device__ __forceinline__ void st_async(uint32_t addr, cplx<R> v, uint32_t bar) {
+  if constexpr (sizeof(R) == 4)
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(addr),
+                 "f"(v.re), "f"(v.im), "r"(bar)
+                 : "memory");
+  else
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(addr),
+                 "d"(v.re), "d"(v.im), "r"(bar)
+                 : "memory");
+}
+
+template <typename R, int L, int C, bool PK = false>
+__global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<R, L, C, false>::MIN_BLOCKS)
+    fused_step_async_kernel(FusedArgs f) {
+  using Sh = FusedShape<R, L, C>;
+  static_assert(C > 1, "the write-back goes to cluster peers");
+  constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION;
+  constexpr int V = L * L * L;
+  constexpr uint32_t SLAB_BYTES = (uint32_t)(Sh::STAGE * sizeof(cplx<R>));  // bytes written back into a CTA
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  cplx<R>* sm = reinterpret_cast<cplx<R>*>(smem_raw);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Sh::WORK);  // write-backs into this CTA's slab
+  uint64_t* idle = bar + 1;                                    // the time-out test's mbarrier
+  // This CTA's abort words, by iteration parity: set (in this CTA's own
+  // shared memory only) when a write-back wait of iteration i gave up, read
+  // by every CTA of the cluster after the cluster barrier of iteration i + 1.
+  // A word of parity p is written only between the barriers of iterations
+  // with parity p and p + 1 and read only after the latter: every CTA sees
+  // the same words and leaves at the same barrier.
+  int* abort_words = reinterpret_cast<int*>(bar + 2);
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int c = (int)cluster.block_rank();
+  const long cluster_id = blockIdx.x / C;
+  const long n_clusters = gridDim.x / C;
+  const int tid = threadIdx.x;
+
+  auto off = [](int r, int xl, int yl, int z) { return r * REGION + (xl * S + yl) * LP + z; };
+  auto slab = [&](long orb) {
+    return reinterpret_cast<const cplx<R>*>(f.psi) + (size_t)orb * V + (size_t)c * S * L * L;
+  };
+
+  const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  R wp_hi, wp_lo, wm_hi, wm_lo;
+  split<R>(f.w_plus, wp_hi, wp_lo);
+  split<R>(f.w_minus, wm_hi, wm_lo);
+  const bool w_exact = wp_lo == (R)0 && wm_lo == (R)0;
+
+  if (tid == 0) {
+    reinterpret_cast<volatile int*>(abort_words)[0] = 0;
+    reinterpret_cast<volatile int*>(abort_words)[1] = 0;
+    mbar_init(bar);
+    mbar_init(idle);
+  }
+  cluster.sync();  // mbarriers and abort words are set up before any peer uses them
+  // this CTA's region c and abort words; mapa turns them into every peer's copy
+  const uint32_t my_region = smem_u32(sm + c * REGION);
+  const uint32_t my_words = smem_u32(abort_words);
+  uint32_t parity = 0;       // of this CTA's write-back phase and of the iteration
+  bool outstanding = false;  // a write-back phase of `bar` (parity x_phase) not seen complete
+  uint32_t x_phase = 0;
+  bool aborted = false;
+  long orb = cluster_id;
+  if (tid == 0 && orb < f.n_orb_total) prefetch_l2(slab(orb), SLAB_BYTES);
+
+  for (; orb < f.n_orb_total; orb += n_clusters) {
+    const long conf = orb / f.batch;
+    const uint64_t kb = f.off0 + (f.conf_base ? __ldg(f.conf_base + conf) : (uint64_t)conf * f.conf_stride);
+    cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
+    cplx<R> x[L];
+    if (tid == 0 && orb + n_clusters < f.n_orb_total) prefetch_l2(slab(orb + n_clusters), SLAB_BYTES);
+    // ---- 1. k(p), forward DFT along y from the slab (L2): thread -> (xl, z)
+    {
+      const int z = tid % L, xl = tid / L;
+      const int site0 = (c * S + xl) * L * L + z;
+      const cplx<R>* src = slab(orb);
+#pragma unroll
+      for (int y = 0; y < L; ++y) {
+        cplx<R> v;
+        if constexpr (sizeof(R) == 4) {
+          float2 t = __ldcg(reinterpret_cast<const float2*>(src) + (xl * L + y) * L + z);
+          v = cplx<R>{t.x, t.y};
+        } else {
+          double2 t = __ldcg(reinterpret_cast<const double2*>(src) + (xl * L + y) * L + z);
+          v = cplx<R>{t.x, t.y};
+        }
+        x[y] = apply_kin<R, PK>(f, site0 + y * L, v);
+      }
+      fft::dft<L, -1, R, PK>(x);
+#pragma unroll
+      for (int y = 0; y < L; ++y) sm[off(y / S, xl, y % S, z)] = x[y];
+    }
+    __syncthreads();
+    // ---- 2. forward DFT along z in place: thread -> (xl, y)
+    {
+      const int y = tid % L, xl = tid / L;
+      cplx<R>* row = sm + off(y / S, xl, y % S, 0);
+#pragma unroll
+      for (int j = 0; j < L; ++j) x[j] = row[j];
+      fft::dft<L, -1, R, PK>(x);
+#pragma unroll
+      for (int j = 0; j < L; ++j) row[j] = x[j];
+    }
+    cluster_barrier_shared_release();
+    if (orb != cluster_id) {  // did any CTA give up in the previous iteration?
+      int any = 0;
+#pragma unroll
+      for (int r = 0; r < C; ++r) {
+        int w;
+        asm volatile("ld.shared::cluster.b32 %0, [%1];"
+                     : "=r"(w)
+                     : "r"(mapa_u32(my_words, (uint32_t)r) + 4u * (parity ^ 1u))
+                     : "memory");
+        any |= w;
+      }
+      if (any) {
+        aborted = true;
+        break;
+      }
+    }
+    // ---- 3. x: forward DFT, times w, backward DFT on the pencils of y-slab
+    // c, read from and written back to region c of CTA x/S
+    if (tid == 0) expect_tx(bar, SLAB_BYTES);
+    outstanding = true;
+    x_phase = parity;
+    {
+      const int z = tid % L, yl = tid / L;
+      const int site0 = (c * S + yl) * L + z;  // site of x = 0
+#pragma unroll
+      for (int xx = 0; xx < L; ++xx)
+        x[xx] = ld_cluster<R>(mapa_u32(my_region, (uint32_t)(xx / S)) +
+                              (uint32_t)((((xx % S) * S + yl) * LP + z) * sizeof(cplx<R>)));
+      fft::dft<L, -1, R, PK>(x);
+      if (z2_fast) {
+        const uint64_t k0 = kb + (uint64_t)site0;
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
+        const int bit = (int)(k0 & 31);
+        if (w_exact) {
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+            x[xx] = scale_w1<R, PK>(x[xx], up ? wp_hi : wm_hi);
+          }
+        } else {
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+            x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
+      }
+      fft::dft<L, +1, R, PK>(x);
+      const uint32_t my_bar = smem_u32(bar);
+#pragma unroll
+      for (int xx = 0; xx < L; ++xx) {
+        const uint32_t rank = (uint32_t)(xx / S);
+        st_async<R>(mapa_u32(my_region, rank) + (uint32_t)((((xx % S) * S + yl) * LP + z) * sizeof(cplx<R>)), x[xx],
+                    mapa_u32(my_bar, rank));
+      }
+    }
+    // every peer's write-back into this CTA's slab
+    const bool ok = stall_here(f, cluster_id, c, orb == cluster_id) ? mbar_wait_bounded(idle, 0u, f, nullptr)
+                                                                    : mbar_wait_bounded<true>(bar, parity, f, nullptr);
+    // ---- 4. backward DFT along z in place
+    {
+      const int y = tid % L, xl = tid / L;
+      cplx<R>* row = sm + off(y / S, xl, y % S, 0);
+#pragma unroll
+      for (int j = 0; j < L; ++j) x[j] = row[j];
+      fft::dft<L, +1, R, PK>(x);
+#pragma unroll
+      for (int j = 0; j < L; ++j) row[j] = x[j];
+    }
+    if (__syncthreads_or(!ok)) {
+      // the write-backs did not all land: the cluster leaves at the next
+      // cluster barrier (no further expect_tx on the stuck phase)
+      if (tid == 0) reinterpret_cast<volatile int*>(abort_words)[parity] = 1;
+    } else {
+      outstanding = false;
+    }
+    parity ^= 1u;
+    // ---- 5. backward DFT along y, times k(p), streaming stores
+    {
+      const int z = tid % L, xl = tid / L;
+      const int site0 = (c * S + xl) * L * L + z;
+#pragma unroll
+      for (int y = 0; y < L; ++y) x[y] = sm[off(y / S, xl, y % S, z)];
+      fft::dft<L, +1, R, PK>(x);
+#pragma unroll
+      for (int y = 0; y < L; ++y) {
+        cplx<R> v = apply_kin<R, PK>(f, site0 + y * L, x[y]);
+        if constexpr (sizeof(R) == 4)
+          __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(v.re, v.im));
+        else
+          __stcs(reinterpret_cast<double2*>(gpsi) + site0 + y * L, make_double2(v.re, v.im));
+      }
+    }
+    // pass 1 of the next orbital writes, per thread, the elements this thread
+    // read in pass 5; no peer touches this CTA's shared memory before the
+    // next cluster barrier
+  }
+  // leaving early: write-backs this CTA expected land (or time out) first
+  if (aborted && outstanding && tid == 0) mbar_wait_bounded<true>(bar, x_phase, f, nullptr);
+  cluster.sync();
+}
+
 // KIND 0: one lane per pencil, exchange through peers' shared memory;
 // 1: two lanes per pencil; 2: bulk-copy exchange, staged slab; 3: bulk-copy
 // exchange, slab prefetched into L2; 4, 5, 6: kinds 0, 2, 3 with the packed
 // FP32x2 transforms (FP32 only); 7, 8: kinds 0, 4 with the slab prefetched
 // into L2 instead of staged (four CTAs per SM); 9, 10: kinds 6, 3 with the
-// CTA's slab of the kinetic table resident in shared memory (FP32 only).
+// CTA's slab of the kinetic table resident in shared memory (FP32 only);
+// 11, 12: kinds 7, 8 with the x pass written back by st.async onto the
+// owners' mbarriers (one cluster barrier per orbital).
 template <typename R, int L, int C, int KIND = 0>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
-  static_assert(KIND < 4 || KIND == 7 || sizeof(R) == 4, "packed transforms and the resident k(p) slab are FP32");
+  static_assert(KIND < 4 || KIND == 7 || KIND == 11 || sizeof(R) == 4,
+                "packed transforms and the resident k(p) slab are FP32");
   constexpr int THREADS = KIND == 1 ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
   constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
                           : (KIND == 3 || KIND == 6) ? BulkShape<R, L, C, false>::SMEM
                           : (KIND == 9 || KIND == 10) ? BulkShape<R, L, C, false, true>::SMEM
-                          : (KIND == 7 || KIND == 8) ? PullShape<R, L, C, false>::SMEM
+                          : (KIND == 7 || KIND == 8 || KIND == 11 || KIND == 12) ? PullShape<R, L, C, false>::SMEM
                                                      : Sh::SMEM;
   void (*kern)(FusedArgs);
   if constexpr (KIND == 1) kern = fused_step_split_kernel<R, L, C>;
@@ -1007,6 +1256,8 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   else if constexpr (KIND == 10) kern = fused_step_bulk_kernel<R, L, C, false, false, true>;
   else if constexpr (KIND == 7) kern = fused_step_kernel<R, L, C, false, false>;
   else if constexpr (KIND == 8) kern = fused_step_kernel<R, L, C, true, false>;
+  else if constexpr (KIND == 11) kern = fused_step_async_kernel<R, L, C, false>;
+  else if constexpr (KIND == 12) kern = fused_step_async_kernel<R, L, C, true>;
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");
@@ -1072,6 +1323,7 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 16, 2, 9, launch_fused<float, 16, 2, 9>},
     {NRCPS_F32, 16, 2, 10, launch_fused<float, 16, 2, 10>},
     {NRCPS_F32, 16, 2, 0, launch_fused<float, 16, 2>},
+    {NRCPS_F32, 16, 2, 11, launch_fused<float, 16, 2, 11>},
     {NRCPS_F32, 16, 1, 1, launch_fused<float, 16, 1, 1>},
     {NRCPS_F32, 24, 3, 5, launch_fused<float, 24, 3, 5>},
     {NRCPS_F32, 24, 4, 4, launch_fused<float, 24, 4, 4>},
@@ -1081,8 +1333,12 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 24, 4, 10, launch_fused<float, 24, 4, 10>},
     {NRCPS_F32, 24, 3, 0, launch_fused<float, 24, 3>},
     {NRCPS_F32, 24, 4, 0, launch_fused<float, 24, 4>},
+    {NRCPS_F32, 24, 4, 11, launch_fused<float, 24, 4, 11>},
     {NRCPS_F32, 32, 8, 4, launch_fused<float, 32, 8, 4>},
     {NRCPS_F32, 32, 8, 7, launch_fused<float, 32, 8, 7>},
+    {NRCPS_F32, 32, 8, 11, launch_fused<float, 32, 8, 11>},
+    {NRCPS_F32, 32, 8, 12, launch_fused<float, 32, 8, 12>},
+    {NRCPS_F32, 32, 16, 11, launch_fused<float, 32, 16, 11>},
     {NRCPS_F32, 32, 8, 8, launch_fused<float, 32, 8, 8>},
     {NRCPS_F32, 32, 8, 6, launch_fused<float, 32, 8, 6>},
     {NRCPS_F32, 32, 8, 5, launch_fused<float, 32, 8, 5>},
@@ -1103,8 +1359,10 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F64, 16, 2, 1, launch_fused<double, 16, 2, 1>},
     {NRCPS_F64, 24, 4, 2, launch_fused<double, 24, 4, 2>},
     {NRCPS_F64, 24, 4, 0, launch_fused<double, 24, 4>},
+    {NRCPS_F64, 24, 4, 11, launch_fused<double, 24, 4, 11>},
     {NRCPS_F64, 32, 16, 3, launch_fused<double, 32, 16, 3>},
     {NRCPS_F64, 32, 16, 7, launch_fused<double, 32, 16, 7>},
+    {NRCPS_F64, 32, 16, 11, launch_fused<double, 32, 16, 11>},
     {NRCPS_F64, 32, 16, 0, launch_fused<double, 32, 16>},
     {NRCPS_F64, 32, 8, 0, launch_fused<double, 32, 8>},
     {NRCPS_F64, 32, 16, 2, launch_fused<double, 32, 16, 2>},
@@ -1264,6 +1522,39 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   return NRCPS_OK;
 }
 
+// The variant (index into kVariants) a step of (prec, L) runs under the
+// context's options: the autotuned one, or the first listed, restricted to
+// the forced cluster size / split / kind; -1 if none qualifies.
+static int fused_pick(nrcps_context* ctx, nrcps_precision prec, int L, int cluster) {
+  init_choices();
+  int pick = -1;
+  const int want_split = ctx->fused_split;  // -1: any
+  const int want_kind = ctx->fused_kind;    // -1: any
+  auto admissible = [&](const FusedVariant& v) {
+    return (cluster <= 0 || v.C == cluster) && (want_split < 0 || (v.kind == 1) == (want_split == 1)) &&
+           (want_kind < 0 || v.kind == want_kind);
+  };
+  const int tuned = L < 64 ? g_choice[ctx->device & 15][prec][L] : -1;
+  if (cluster > 0 || want_split >= 0 || want_kind >= 0) {
+    if (tuned >= 0 && admissible(kVariants[tuned])) pick = tuned;
+    for (int i = 0; i < kNumVariants && pick < 0; ++i)
+      if (kVariants[i].prec == prec && kVariants[i].L == L && admissible(kVariants[i])) pick = i;
+  } else {
+    pick = tuned;
+    for (int i = 0; i < kNumVariants && pick < 0; ++i)  // default: the first listed variant
+      if (kVariants[i].prec == prec && kVariants[i].L == L) pick = i;
+  }
+  return pick;
+}
+
+nrcps_status fused_choice(nrcps_context* ctx, nrcps_precision prec, int L, int* kind, int* cluster) {
+  const int d[3] = {L, L, L};
+  const int pick = (ctx->fused_enabled && fused_supported(prec, d)) ? fused_pick(ctx, prec, L, ctx->fused_cluster) : -1;
+  *kind = pick >= 0 ? kVariants[pick].kind : -1;
+  *cluster = pick >= 0 ? kVariants[pick].C : -1;
+  return NRCPS_OK;
+}
+
 // One fused step; `kin_table` is (hi, lo) float pairs for prec F32 and FP64 for F64.
 // cluster = 0 selects the autotuned (or default) cluster size.
 nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const void* kin_table,
@@ -1290,28 +1581,10 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   f.wait_ns = ctx->fused_wait_ns;
   f.stall_test = ctx->fused_stall_test;
   if (f.n_orb_total == 0) return NRCPS_OK;
-  init_choices();
-  const int L = d[0];
-  int pick = -1;
-  const int want_split = ctx->fused_split;  // -1: any
-  const int want_kind = ctx->fused_kind;    // -1: any
-  auto admissible = [&](const FusedVariant& v) {
-    return (cluster <= 0 || v.C == cluster) && (want_split < 0 || (v.kind == 1) == (want_split == 1)) &&
-           (want_kind < 0 || v.kind == want_kind);
-  };
-  if (cluster > 0 || want_split >= 0 || want_kind >= 0) {
-    const int tuned = g_choice[ctx->device & 15][prec][L];
-    if (tuned >= 0 && admissible(kVariants[tuned])) pick = tuned;
-    for (int i = 0; i < kNumVariants && pick < 0; ++i)
-      if (kVariants[i].prec == prec && kVariants[i].L == L && admissible(kVariants[i])) pick = i;
-    if (pick < 0)
-      return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "no fused variant with cluster size %d, split %d, kind %d",
-                       cluster, want_split, want_kind);
-  } else {
-    pick = g_choice[ctx->device & 15][prec][L];
-    for (int i = 0; i < kNumVariants && pick < 0; ++i)  // default: the first listed variant
-      if (kVariants[i].prec == prec && kVariants[i].L == L) pick = i;
-  }
+  const int pick = fused_pick(ctx, prec, d[0], cluster);
+  if (pick < 0)
+    return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "no fused variant with cluster size %d, split %d, kind %d",
+                     cluster, ctx->fused_split, ctx->fused_kind);
   return kVariants[pick].fn(ctx, f, 0);
 }
 

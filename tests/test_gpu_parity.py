@@ -488,13 +488,17 @@ def test_packed_variants_agree(ctx, kind, L, cluster):
         ctx.set_option("fused.kind", -1)
 
 
-@pytest.mark.parametrize("kind,ref_kind,precision,cluster", [(5, 4, "f32", 8), (6, 4, "f32", 8), (8, 4, "f32", 8),
-                                                             (7, 0, "f32", 8), (7, 0, "f64", 16), (9, 4, "f32", 8),
-                                                             (10, 0, "f32", 8)])
-def test_same_arithmetic_variants_are_bit_identical(ctx, kind, ref_kind, precision, cluster):
+@pytest.mark.parametrize("kind,ref_kind,precision,cluster,L", [
+    (5, 4, "f32", 8, 32), (6, 4, "f32", 8, 32), (8, 4, "f32", 8, 32), (7, 0, "f32", 8, 32), (7, 0, "f64", 16, 32),
+    (9, 4, "f32", 8, 32), (10, 0, "f32", 8, 32), (11, 0, "f32", 8, 32), (12, 4, "f32", 8, 32),
+    (11, 0, "f32", 16, 32), (11, 0, "f64", 16, 32), (11, 0, "f32", 2, 16), (11, 0, "f32", 4, 24),
+    (11, 0, "f64", 4, 24)])
+def test_same_arithmetic_variants_are_bit_identical(ctx, kind, ref_kind, precision, cluster, L):
     """Variants that differ only in how the slab reaches shared memory or how
-    the exchange moves it run the same arithmetic: results agree bit for bit."""
-    psi, kinv, bits = _random_step_inputs(ctx, 32, 3, 5, precision, seed=6)
+    the exchange moves it (peer loads and stores, bulk copies, or peer loads
+    with st.async write-backs completing on the owner's mbarrier) run the same
+    arithmetic: results agree bit for bit."""
+    psi, kinv, bits = _random_step_inputs(ctx, L, 3, 5, precision, seed=6)
     try:
         ctx.set_option("fused.cluster", cluster)
         ctx.set_option("fused.kind", ref_kind)
@@ -539,9 +543,9 @@ def test_synchronize_reports_no_timeout(ctx):
 
 # every fused kernel with mbarrier waits: peer access with a staged slab (0,
 # also as a one-CTA cluster), lane split (1), bulk exchange staged (2) and via
-# L2 (3)
+# L2 (3), st.async write-backs (11)
 _WAITING_VARIANTS = [(0, "f32", 32, 8), (0, "f32", 16, 1), (1, "f32", 32, 8), (2, "f32", 32, 8), (3, "f32", 32, 8),
-                     (3, "f64", 32, 16)]
+                     (3, "f64", 32, 16), (11, "f32", 32, 8), (11, "f64", 32, 16)]
 
 
 @pytest.mark.parametrize("kind,precision,L,cluster", _WAITING_VARIANTS)

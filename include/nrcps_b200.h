@@ -304,12 +304,14 @@ nrcps_status nrcps_slater_dets(nrcps_context *ctx, const double *dev_S, const do
  * reference).  For callers that cannot let a library allocate device memory
  * -- a host whose caching pool already owns the device memory, or code
  * measuring between kernels already queued, where an allocation could stall
- * the device -- the working memory comes from one fixed 16 MiB array in the
- * library, which every GPU that loads the library keeps until exit.  Batches
- * needing more (nconf * nmeas * (2N^2 + N) doubles) are rejected with
- * NRCPS_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
- * array's address; make it before any stream capture.  Calls that may run
- * concurrently on the GPU share the array and race: serialise them. */
+ * the device.  N <= 64 runs the warp-per-minor kernel, which needs no memory
+ * beyond the inputs and outputs.  For N > 64 the working memory comes from
+ * one fixed 16 MiB array in the library, which every GPU that loads the
+ * library keeps until exit; batches needing more (nconf * nmeas * (2N^2 + N)
+ * doubles) are rejected with NRCPS_ERR_INVALID_ARGUMENT.  The first N > 64
+ * call on a device looks up the array's address; make it before any stream
+ * capture.  Calls that may run concurrently on the GPU share the array and
+ * race: serialise them.  nconf = 0 is a no-op (null buffers allowed). */
 nrcps_status nrcps_slater_dets_noalloc(nrcps_context *ctx, const double *dev_S, const double *dev_psi1,
                                        int N, int nconf, int mode, int log_det, double *dev_out);
 

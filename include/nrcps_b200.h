@@ -107,6 +107,9 @@ const char *nrcps_version(void);
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the
  *                      CUDA-core kernel with FP64 accumulation;
+ *   "qr.gram_tc"       1 (default): the Gram matrices of the re-orthonormalisation
+ *                      of FP32 orbitals (N <= 32) on the tcgen05 tensor cores
+ *                      (TF32 hi/lo, FP32 accumulation); 0: the CUDA-core kernel;
  *   "lu.warp"          1 (default): leading-minor determinants with one warp
  *                      per minor in shared memory (N <= 64); 0: one thread
  *                      per minor with global scratch;
@@ -355,6 +358,14 @@ nrcps_status nrcps_ensemble_create(nrcps_context *ctx, const nrcps_job *job, con
  * doubles, nmeas = N (mode 0) or 2N (mode 1), raw determinants before any
  * accumulation. */
 nrcps_status nrcps_ensemble_run(nrcps_ensemble *ens, uint64_t first_conf, double *dev_dets);
+/* Replaces the sources of later runs from host memory, the kind given at
+ * creation: sources (N x V complex doubles) for dense sources, pw_index (N
+ * site indices) for plane waves; the other pointer may be NULL.  The copy is
+ * queued on the context's stream ahead of later runs (pinned host memory
+ * keeps it asynchronous).  Every run starts from the current sources, as
+ * the reference's drivers call Propagator::Set(OneBody::Get(), n) for every
+ * configuration (src/alg/propagator.C:47-63, production/slater_det/main.C:196-199). */
+nrcps_status nrcps_ensemble_set_sources(nrcps_ensemble *ens, const double *sources, const int *pw_index);
 nrcps_status nrcps_ensemble_destroy(nrcps_ensemble *ens);
 /* Kernel launches issued by the last run (for launch accounting). */
 nrcps_status nrcps_ensemble_launches(const nrcps_ensemble *ens, long *launches);

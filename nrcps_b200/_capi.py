@@ -109,6 +109,7 @@ SIGNATURES = {
     "nrcps_slater_dets_noalloc": ([_P, _P, _P, _I, _I, _I, _I, _P], _I),
     "nrcps_ensemble_create": ([_P, ctypes.POINTER(Job), _DP, _DP, _DP, _DP, _IP, _DP, _IP, ctypes.POINTER(_P)], _I),
     "nrcps_ensemble_run": ([_P, _U64, _P], _I),
+    "nrcps_ensemble_set_sources": ([_P, _DP, _IP], _I),
     "nrcps_ensemble_destroy": ([_P], _I),
     "nrcps_ensemble_launches": ([_P, _LP], _I),
     "nrcps_accumulate": ([_P, _P, _I, _I, _I, _I, _I, _P, _P], _I),

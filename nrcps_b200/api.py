@@ -804,6 +804,29 @@ class Ensemble:
         self.handle = h
         self.dets = torch.empty((job.n_conf, job.T, self.nmeas), dtype=torch.complex128, device=self.ctx.device)
 
+    def set_sources(self, sources=None, plane_wave_index=None) -> None:
+        """Sources of later runs from host memory (OneBody::Set + Propagator::Set):
+        dense [N, V] complex128 or plane-wave indices [N] int32, the kind given at
+        creation.  Pinned host tensors keep the copy asynchronous."""
+        if plane_wave_index is not None:
+            idx = plane_wave_index
+            if isinstance(idx, torch.Tensor):
+                p = ctypes.cast(idx.data_ptr(), ctypes.POINTER(ctypes.c_int))
+            else:
+                idx = np.ascontiguousarray(np.asarray(idx, dtype=np.int32))
+                p = _ip(idx)
+            self.ctx.check(lib().nrcps_ensemble_set_sources(self.handle, None, p), "ensemble_set_sources")
+            self._src_keep = idx  # the copy may read it after this call returns
+        else:
+            src = sources
+            if isinstance(src, torch.Tensor):
+                p = ctypes.cast(src.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            else:
+                src = np.ascontiguousarray(np.asarray(src, dtype=np.complex128))
+                p = _dp(src.view(np.float64))
+            self.ctx.check(lib().nrcps_ensemble_set_sources(self.handle, p, None), "ensemble_set_sources")
+            self._src_keep = src
+
     def run(self, first_conf: int = 0) -> torch.Tensor:
         """Raw determinants [n_conf, T, nmeas] of configurations first_conf.. (device tensor)."""
         self.ctx.check(lib().nrcps_ensemble_run(self.handle, first_conf, _ptr(self.dets)), "ensemble_run")

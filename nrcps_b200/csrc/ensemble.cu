@@ -360,6 +360,23 @@ extern "C" nrcps_status nrcps_ensemble_run(nrcps_ensemble* e, uint64_t first_con
   return NRCPS_OK;
 }
 
+extern "C" nrcps_status nrcps_ensemble_set_sources(nrcps_ensemble* e, const double* sources, const int* pw_index) {
+  if (!e) return NRCPS_ERR_INVALID_ARGUMENT;
+  nrcps_context* ctx = e->ctx;
+  if (e->pw_index) {
+    NRCPS_REQUIRE(ctx, pw_index, "nrcps_ensemble_set_sources: plane-wave ensemble needs pw_index");
+    for (int n = 0; n < e->N; ++n)
+      NRCPS_REQUIRE(ctx, pw_index[n] >= 0 && pw_index[n] < e->vol, "nrcps_ensemble_set_sources: index out of range");
+    return check_cuda(ctx, cudaMemcpyAsync(e->pw_index, pw_index, sizeof(int) * e->N, cudaMemcpyHostToDevice,
+                                           ctx->stream), "set_sources: copy index");
+  }
+  NRCPS_REQUIRE(ctx, sources, "nrcps_ensemble_set_sources: dense-source ensemble needs sources");
+  NRCPS_TRY(check_cuda(ctx, cudaMemcpyAsync(e->src, sources, 16 * (size_t)e->N * e->vol, cudaMemcpyHostToDevice,
+                                            ctx->stream), "set_sources: copy sources"));
+  if (e->src_split) NRCPS_TRY(overlap_tc_prepare(ctx, e->src, e->N, e->vol, e->src_split));
+  return NRCPS_OK;
+}
+
 extern "C" nrcps_status nrcps_ensemble_launches(const nrcps_ensemble* e, long* launches) {
   if (!e || !launches) return NRCPS_ERR_INVALID_ARGUMENT;
   *launches = e->launches_per_run;

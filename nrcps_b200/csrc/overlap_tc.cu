@@ -424,6 +424,13 @@ static bool make_map(CUtensorMap* m, const void* ptr, long rows, long K, int box
 
 }  // namespace tc
 
+// 2-D FP32 tensor map (rows x K floats, 128-byte swizzle, box 32 floats x
+// box_rows) for the other tcgen05 kernels of the library; false when the
+// driver's encoder is unavailable or rejects the shape.
+bool make_fp32_map_sw128(CUtensorMap* m, const void* ptr, long rows, long K, int box_rows) {
+  return tc::make_map(m, ptr, rows, K, box_rows);
+}
+
 // Shapes the tensor-core path takes: FP32 orbitals, K = 2V a multiple of 32
 // floats, rows addressable as int.
 bool overlap_tc_supported(long vol, int ns, int nt, int nconf) {

@@ -5,7 +5,9 @@ context's stream, after warm-up), one JSON line per measurement.
     python -m nrcps_b200.kernel_bench overlap --L 32 --ns 19 --nconf 1024 [--tc 1|0]
     python -m nrcps_b200.kernel_bench dets    --N 19 --nconf 4096
     python -m nrcps_b200.kernel_bench cv      --T 64 --batch 256
-    python -m nrcps_b200.kernel_bench qr      --L 32 --N 19 --nconf 1024 [--precision f32]
+    python -m nrcps_b200.kernel_bench qr      --L 32 --N 19 --nconf 1024 [--precision f32] [--gram-tc 1|0]
+    python -m nrcps_b200.kernel_bench rng     --L 32 --T 64 --nconf 1024
+    python -m nrcps_b200.kernel_bench pair    --L 48 --N 10 --nconf 1024 [--precision f32]
 
 step:    one transfer-matrix step (nrcps_propagate, Z2 field, a = 0.5) over
          `orbitals` orbitals in batches of 19; GB/s counts one read and one
@@ -20,6 +22,12 @@ cv:      one training step (forward, backward, Adam) and one inference pass
 qr:      one CholeskyQR re-orthonormalisation (nrcps_reorthonormalise) of
          nconf configurations of N orbitals; GB/s counts the algorithmic
          three passes over the orbitals (Gram read, apply read + write).
+rng:     the Z2 field bits of nconf configurations x T slices of L^3 sites
+         from RANLXS2 (nrcps_draw_z2_bits): uniforms per second and the
+         output bits' GB/s.
+pair:    the TwoBody pair matrices phi_st = sum_p w(p) psi_s(p) psi_t(-p) of
+         nconf configurations of N orbitals (nrcps_pair_matrix); GB/s counts
+         one read of the orbitals.
 """
 from __future__ import annotations
 
@@ -149,9 +157,32 @@ def bench_qr(ctx: Context, L: int, N: int, nconf: int, precision: str, reps: int
             "GBps": round(nbytes / ms / 1e6, 1)}
 
 
+def bench_rng(ctx: Context, L: int, T: int, nconf: int, reps: int) -> dict:
+    count = nconf * T * L ** 3
+    ms = _time(lambda: draw_z2_bits("RANLXS2", 7, 0, count, ctx), reps)
+    ctx.synchronize()
+    return {"kernel": "rng", "generator": "RANLXS2", "L": L, "T": T, "nconf": nconf, "uniforms": count,
+            "ms": round(ms, 4), "uniforms_per_s": round(count / ms * 1e3, 1),
+            "out_GBps": round(count / 8 / ms / 1e6, 1)}
+
+
+def bench_pair(ctx: Context, L: int, N: int, nconf: int, precision: str, reps: int) -> dict:
+    from .api import TwoBody
+    dims = (L, L, L)
+    dt = torch.complex64 if precision == "f32" else torch.complex128
+    g = torch.Generator(device=ctx.device).manual_seed(13)
+    psi = torch.randn((nconf, N, L ** 3), dtype=dt, device=ctx.device, generator=g)
+    tb = TwoBody(dims, "TGND", "STANDARD", 1.0, 0.176776695, 2.0, ctx)
+    ms = _time(lambda: tb.run_matrix(psi, psi), reps)
+    ctx.synchronize()
+    return {"kernel": "pair", "L": L, "N": N, "nconf": nconf, "precision": precision, "ms": round(ms, 4),
+            "GBps": round(psi.numel() * psi.element_size() / ms / 1e6, 1)}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["step", "overlap", "dets", "cv", "qr"])
+    ap.add_argument("what", choices=["step", "overlap", "dets", "cv", "qr", "rng", "pair"])
+    ap.add_argument("--gram-tc", type=int, default=1)
     ap.add_argument("--L", type=int, default=32)
     ap.add_argument("--orbitals", type=int, default=19456)
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
@@ -173,7 +204,13 @@ def main(argv=None) -> int:
     elif a.what == "cv":
         r = bench_cv(ctx, a.T, a.batch, a.reps)
     elif a.what == "qr":
+        ctx.set_option("qr.gram_tc", a.gram_tc)
         r = bench_qr(ctx, a.L, a.N, a.nconf, a.precision, a.reps)
+        r["gram_tc"] = a.gram_tc
+    elif a.what == "rng":
+        r = bench_rng(ctx, a.L, a.T, a.nconf, a.reps)
+    elif a.what == "pair":
+        r = bench_pair(ctx, a.L, a.N, a.nconf, a.precision, a.reps)
     else:
         r = bench_dets(ctx, a.N, a.nconf, a.reps)
     print(json.dumps(r), flush=True)

@@ -195,7 +195,7 @@ void make_random_arg(const KV& kv, RandomArg* ra) {
   ra->random_type = random_type_of(get(kv, "rng", "RANLXS2"));
   ra->seed_type = SEED_TYPE_INPUT;
   ra->seed = getl(kv, "seed", 1234);
-  ra->file_stem = get(kv, "rngfile", "/tmp/nrcps_ref_rng_state");
+  ra->file_stem = get(kv, "rngfile", "nrcps_ref_rng_state");
 }
 
 FILE* open_out(const string& path) {

@@ -35,3 +35,35 @@ def test_reorthonormalise_against_numpy(N, L, prec):
         want = np.linalg.slogdet(ref[c].conj() @ ref[c].T)[1]
         got = 2 * logR[c].sum().item()
         assert abs(got - want) <= tol_det * abs(want) + tol_det, c
+
+
+@pytest.mark.parametrize("N,L,nconf", [(19, 32, 5), (10, 48, 2), (32, 16, 4), (1, 8, 9)])
+def test_tensor_core_gram_against_cuda_cores(N, L, nconf):
+    """The Gram matrices on the tcgen05 tensor cores (TF32 hi/lo, the default
+    for FP32 orbitals with N <= 32) against the CUDA-core kernel, through a
+    whole re-orthonormalisation: the same log R_ii to 2e-5 (FP32 sums over
+    2V floats either way) and orthonormal orbitals to the FP32 tolerance of
+    the test above (odd configuration counts leave the last tile half
+    empty)."""
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    V = L ** 3
+    rs = np.random.default_rng(N + L)
+    a = rs.standard_normal((nconf, N, V)) + 1j * rs.standard_normal((nconf, N, V))
+    if N > 1:
+        a[:, 1:] += 0.5 * a[:, :1]
+    psi0 = torch.from_numpy(a).to(torch.complex64).to(ctx.device).contiguous()
+    out = {}
+    try:
+        for tc in (1, 0):
+            ctx.set_option("qr.gram_tc", tc)
+            psi = psi0.clone()
+            logR = nb.reorthonormalise(psi, ctx=ctx)
+            ctx.synchronize()
+            out[tc] = (logR.cpu().numpy(), psi.cpu().numpy().astype(np.complex128))
+    finally:
+        ctx.set_option("qr.gram_tc", 1)
+    assert np.max(np.abs(out[1][0] - out[0][0]) / np.maximum(np.abs(out[0][0]), 1.0)) < 2e-5
+    for c in range(nconf):
+        q = out[1][1][c]
+        assert np.abs(q.conj() @ q.T - np.eye(N)).max() < 5e-5, c

@@ -336,7 +336,10 @@ typedef struct {
   int plane_wave;        /* 1: sources are plane waves given by index */
   int use_potential;
   int qr_period;         /* k > 0: CholeskyQR of every configuration's orbitals after each
-                            k-th step, determinants rescaled by prod R_ii (mode 0 only);
+                            k-th step; the measured determinants are rescaled to those of
+                            the unstabilised orbitals (mode 0: det S_n by prod_{i<n} R_ii;
+                            mode 1: the pair-matrix minors by prod_{i<n} R_ii^2, the
+                            replaced-column minors by prod_{i<n} R_ii prod_{i<n-1} R_ii);
                             0: never (the reference's unstabilised propagation) */
   double a;              /* (1 + a*phi) coupling when the interaction is local */
   int local_interaction; /* 1: c(p) constant, use a; 0: full Interaction::Initialize */

@@ -35,7 +35,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
 nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
                                  double* G, double* logR);
 nrcps_status rescale_dets(nrcps_context* ctx, double* dets, const double* logR, int N, int nconf, long conf_stride,
-                          long offset);
+                          long offset, int mode);
 
 struct Group {
   int L = 0, N = 0;
@@ -134,7 +134,7 @@ static nrcps_status record_batch(nrcps_batch* b, double* out) {
       if ((st = slater_dets_dispatch(ctx, g.S, nullptr, g.N, na, 0, 0, g.dets, cstride, 2L * t * g.N, g.lu_scr)))
         break;
       if (g.qr_logR && t >= b->params.qr_period &&
-          (st = rescale_dets(ctx, g.dets, g.qr_logR, g.N, na, cstride, 2L * t * g.N)))
+          (st = rescale_dets(ctx, g.dets, g.qr_logR, g.N, na, cstride, 2L * t * g.N, 0)))
         break;
       if (t + 1 >= g.Tmax) break;
       const int nn = g.nact[t + 1];  // configurations measured again at t + 1

@@ -32,7 +32,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
 nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
                                  double* G, double* logR);
 nrcps_status rescale_dets(nrcps_context* ctx, double* dets, const double* logR, int N, int nconf, long conf_stride,
-                          long offset);
+                          long offset, int mode);
 }  // namespace nrcps
 
 struct nrcps_ensemble {
@@ -156,7 +156,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       NRCPS_TRY(slater_dets_dispatch(ctx, e->S, nullptr, N, nc, 0, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
                                  e->lu_scr));
       if (e->qr_logR && t >= j.qr_period)
-        NRCPS_TRY(rescale_dets(ctx, dets, e->qr_logR, N, nc, 2L * T * e->nmeas, 2L * t * e->nmeas));
+        NRCPS_TRY(rescale_dets(ctx, dets, e->qr_logR, N, nc, 2L * T * e->nmeas, 2L * t * e->nmeas, 0));
     } else {
       NRCPS_TRY(pair_impl(ctx, e->psi, e->psi, N, nc, vol, e->w, e->opp, prec, e->S));
       if (e->pw_index) NRCPS_TRY(gather_impl(ctx, e->pw_index, N, e->psi, N, nc, vol, prec, e->P1));
@@ -164,6 +164,8 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       else NRCPS_TRY(overlap_impl(ctx, e->src, N, e->psi, N, nc, vol, prec, e->P1));
       NRCPS_TRY(slater_dets_dispatch(ctx, e->S, e->P1, N, nc, 1, 0, dets, 2L * T * e->nmeas, 2L * t * e->nmeas,
                                  e->lu_scr));
+      if (e->qr_logR && t >= j.qr_period)
+        NRCPS_TRY(rescale_dets(ctx, dets, e->qr_logR, N, nc, 2L * T * e->nmeas, 2L * t * e->nmeas, 1));
     }
     // -------- Hamiltonians on the field of slice t, then the step
     nrcps_position_factor pf{};
@@ -222,9 +224,6 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   NRCPS_REQUIRE(ctx, job->local_interaction || itab, "nrcps_ensemble_create: interaction table missing");
   NRCPS_REQUIRE(ctx, !job->use_potential || pot, "nrcps_ensemble_create: potential table missing");
   NRCPS_REQUIRE(ctx, job->qr_period >= 0, "nrcps_ensemble_create: qr_period < 0");
-  if (job->qr_period > 0 && job->mode != 0)
-    return set_error(ctx, NRCPS_ERR_UNSUPPORTED,
-                     "nrcps_ensemble_create: re-orthonormalisation is built for the one-body measurement (mode 0)");
   if (job->qr_period > 0 && job->n_orb > 64)
     return set_error(ctx, NRCPS_ERR_UNSUPPORTED, "nrcps_ensemble_create: re-orthonormalisation needs N <= 64");
   const int fk = job->field_kind;

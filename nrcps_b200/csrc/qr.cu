@@ -381,19 +381,38 @@ __global__ void __launch_bounds__(APPLY_THREADS) apply_rinv_kernel(void* __restr
   }
 }
 
-// dets[c][t][n-1] *= exp(sum_{i<n} logR[c][i]) for the minors measured at slice t.
+// The determinants measured at slice t on the re-orthonormalised orbitals
+// Q = Psi R^-1, turned into those of Psi, with S_n = sum_{i<=n} log R_ii:
+//  mode 0 (SlaterDet::Run, S = <src|Psi> = <src|Q> R):
+//    dets[c][t][n]    *= exp(S_n)                      (det S_{n+1})
+//  mode 1 (SlaterDet2::Run on the pair matrix Phi(Psi) = R^T Phi(Q) R, whose
+//  column n is replaced by v_s = <src_n|psi_s>, v(Psi) = R^T v(Q)):
+//    dets[c][t][2n+1] *= exp(2 S_n)                    (det Phi_{n+1})
+//    dets[c][t][2n]   *= exp(S_n + S_{n-1})            (det R_{n+1} det R_n)
+// (slater_det2.C:78-148; R upper triangular, so the leading blocks of R^T
+// Phi R involve only the leading blocks of R).
 __global__ void rescale_dets_kernel(double* dets, const double* logR, int N, int nconf, long conf_stride,
-                                    long offset) {
+                                    long offset, int mode) {
   const long total = (long)nconf * N;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
     const long c = e / N;
     const int n = (int)(e % N);
     double s = 0;
-    for (int i = 0; i <= n; ++i) s += logR[c * N + i];
-    const double f = exp(s);
-    double* d = dets + c * conf_stride + offset + 2L * n;
-    d[0] *= f;
-    d[1] *= f;
+    for (int i = 0; i < n; ++i) s += logR[c * N + i];
+    const double s_prev = s;  // S_{n-1}
+    s += logR[c * N + n];     // S_n
+    double* base = dets + c * conf_stride + offset;
+    if (mode == 0) {
+      const double f = exp(s);
+      base[2L * n] *= f;
+      base[2L * n + 1] *= f;
+    } else {
+      const double f1 = exp(2.0 * s), f0 = exp(s + s_prev);
+      base[2L * (2 * n + 1)] *= f1;
+      base[2L * (2 * n + 1) + 1] *= f1;
+      base[2L * (2 * n)] *= f0;
+      base[2L * (2 * n) + 1] *= f0;
+    }
   }
 }
 
@@ -469,9 +488,9 @@ nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol,
 }
 
 nrcps_status rescale_dets(nrcps_context* ctx, double* dets, const double* logR, int N, int nconf, long conf_stride,
-                          long offset) {
+                          long offset, int mode) {
   rescale_dets_kernel<<<grid_for((long)nconf * N, 256), 256, 0, ctx->stream>>>(dets, logR, N, nconf, conf_stride,
-                                                                               offset);
+                                                                               offset, mode);
   ctx->launches++;
   return check_launch(ctx, "rescale_dets_kernel");
 }

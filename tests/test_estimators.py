@@ -118,7 +118,8 @@ def test_device_accumulate_result_rows(golden, name):
     """The device accumulator (nrcps_accumulate) on the reference's raw
     determinants: the slater.<m> rows byte for byte; the cumulant rows, whose
     log and hypot are CUDA's (within an ulp or two of the C library's), within
-    1e-14 relative value for value."""
+    1e-13 of the row's largest value (the sums of the odd powers of log|det|
+    cancel, so single values can be far smaller than the row)."""
     import torch
     import nrcps_b200 as nb
     ctx = nb.default_context()
@@ -135,4 +136,4 @@ def test_device_accumulate_result_rows(golden, name):
                 for m, row in enumerate(rows):
                     want = np.array(files[f"z{k + 1}.{m + 1}"].splitlines()[b].split(), dtype=float)
                     got = np.array(row.split(), dtype=float)
-                    assert np.allclose(got, want, rtol=1e-14, atol=0), (k, m, b)
+                    assert np.allclose(got, want, rtol=0, atol=1e-13 * np.abs(want).max()), (k, m, b)

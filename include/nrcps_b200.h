@@ -107,9 +107,9 @@ const char *nrcps_version(void);
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the
  *                      CUDA-core kernel with FP64 accumulation;
- *   "qr.gram_tc"       1 (default): the Gram matrices of the re-orthonormalisation
- *                      of FP32 orbitals (N <= 32) on the tcgen05 tensor cores
- *                      (TF32 hi/lo, FP32 accumulation); 0: the CUDA-core kernel;
+ *   "qr.gram_tc"       1: the Gram matrices of the re-orthonormalisation of
+ *                      FP32 orbitals (N <= 32) on the tcgen05 tensor cores
+ *                      (TF32 hi/lo); 0 (default): the CUDA-core kernel;
  *   "lu.warp"          1 (default): leading-minor determinants with one warp
  *                      per minor in shared memory (N <= 64); 0: one thread
  *                      per minor with global scratch;

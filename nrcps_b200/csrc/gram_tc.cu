@@ -14,8 +14,11 @@
 // the drain adds D[i][hi j] + D[i][lo j] and +-D[j][lo i] (a transpose
 // within one warp).  Two configurations share a tile: A rows 0-31 hi c0,
 // 32-63 rot(hi) c0, 64-95 hi c1, 96-127 rot(hi) c1; B rows 0-31 hi c0, 32-63
-// lo c0, 64-95 hi c1, 96-127 lo c1 (M = N = 128, K = 8 per MMA, FP32
-// accumulation in TMEM over all of K).
+// lo c0, 64-95 hi c1, 96-127 lo c1 (M = N = 128, K = 8 per MMA).  The
+// tensor core accumulates in FP32 over 256 floats of K only (a chunk): a
+// longer FP32 accumulation in TMEM drifts (a relative bias of ~3e-4 over
+// K = 65536 was measured), so every chunk is drained into FP64 registers
+// while the next accumulates in the other TMEM buffer.
 //
 // The Gram only has to be accurate enough for R^-1 to make the orbitals
 // well conditioned: the measured determinants use the identity
@@ -49,6 +52,7 @@ namespace gtc {
 constexpr int BK = 32;                             // floats of K per k-block: one 128-byte swizzle row
 constexpr int ROWS = 32;                           // operand rows per configuration block
 constexpr int STAGES = 6;
+constexpr int CHUNK = 8;                           // k-blocks (256 floats of K) per FP32 accumulation
 constexpr uint32_t BLOCK_BYTES = ROWS * BK * 4;    // 4 KB: 32 rows of one k-block
 constexpr uint32_t OP_BYTES = 4 * BLOCK_BYTES;     // 16 KB: 128 operand rows
 constexpr uint32_t STAGE_BYTES = 2 * OP_BYTES;     // A then B
@@ -65,6 +69,7 @@ struct Args {
   int N;
   int nr;        // rows per configuration load: N rounded up to 8
   int nkb;       // k-blocks per configuration: 2 V / BK
+  int nch;       // chunks per configuration: ceil(nkb / CHUNK)
   int ntiles;    // configuration pairs
   double* G;     // [nconf][N][N] complex
   int* err;
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
   uint64_t* tempty = tfull + 2;        // [2] TMEM buffer b read out (4 drain warps)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  volatile int* last_commit = abort_flag + 1;  // last local tile whose TMEM-full commit was issued
+  volatile int* last_commit = abort_flag + 1;  // last chunk (of this CTA) whose TMEM-full commit was issued
 
   auto stage_a = [&](int s) { return base + (size_t)s * STAGE_BYTES; };
   auto stage_b = [&](int s) { return base + (size_t)s * STAGE_BYTES + OP_BYTES; };
@@ -236,28 +241,31 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      int i = 0;
+      int i = 0, gc = 0;  // k-block and chunk counters of this CTA
       bool stop = false;
       for (int j = 0; j < n_local && !stop; ++j) {
-        const int b = j & 1;
-        if (j >= 2 && !bar_wait(tempty + b, (uint32_t)((j >> 1) - 1) & 1u, abort_flag, g.err)) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t d = tmem + (uint32_t)(b * 128);
-        for (int kb = 0; kb < g.nkb; ++kb, ++i) {
-          const int s = i % STAGES;
-          if (!bar_wait(conv + s, (uint32_t)(i / STAGES) & 1u, abort_flag, g.err)) {
-            stop = true;
-            break;
-          }
+        for (int ch = 0; ch < g.nch && !stop; ++ch, ++gc) {
+          const int b = gc & 1;
+          if (gc >= 2 && !bar_wait(tempty + b, (uint32_t)((gc >> 1) - 1) & 1u, abort_flag, g.err)) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint64_t ad = smem_desc(stage_a(s)), bd = smem_desc(stage_b(s));
+          const uint32_t d = tmem + (uint32_t)(b * 128);
+          const int kb1 = (ch + 1) * CHUNK < g.nkb ? (ch + 1) * CHUNK : g.nkb;
+          for (int kb = ch * CHUNK; kb < kb1; ++kb, ++i) {
+            const int s = i % STAGES;
+            if (!bar_wait(conv + s, (uint32_t)(i / STAGES) & 1u, abort_flag, g.err)) {
+              stop = true;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint64_t ad = smem_desc(stage_a(s)), bd = smem_desc(stage_b(s));
 #pragma unroll
-          for (int k = 0; k < BK / 8; ++k)  // K = 8 TF32 = 32 bytes per MMA: advance the start address
-            mma_tf32(d, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), (kb > 0 || k > 0) ? 1u : 0u);
-          mma_commit(empty + s);
+            for (int k = 0; k < BK / 8; ++k)  // K = 8 TF32 = 32 bytes per MMA: advance the start address
+              mma_tf32(d, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), (kb > ch * CHUNK || k > 0) ? 1u : 0u);
+            mma_commit(empty + s);
+          }
+          mma_commit(tfull + b);  // completes once every MMA issued so far has
+          *last_commit = gc;
         }
-        mma_commit(tfull + b);  // completes once every MMA issued so far has
-        *last_commit = j;
       }
     }
   } else if (warp < 6) {
@@ -313,21 +321,32 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
     const uint32_t col0 = (uint32_t)(64 * pair_half);  // B hi columns; lo at +32
     float* X = xbuf + (size_t)q * 32 * XLD;
     bool ok = true;
-    for (int j = 0; j < n_local; ++j) {
-      const int b = j & 1;
-      if (ok && !bar_wait(tfull + b, (uint32_t)(j >> 1) & 1u, abort_flag, g.err)) ok = false;
-      ok = __all_sync(0xffffffffu, ok);
-      if (!ok) break;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      float hi[32], lo[32];
-      const uint32_t t0 = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * 128) + col0;
-      tmem_ld32(t0, hi);       // D[row][hi j]
-      tmem_ld32(t0 + 32, lo);  // D[row][lo j]
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) bar_arrive(tempty + b);
+    int gc = 0;
+    for (int j = 0; j < n_local && ok; ++j) {
+      double acc_hi[32], acc_lo[32];  // D[row][hi j], D[row][lo j] summed over the chunks in FP64
 #pragma unroll
-      for (int k = 0; k < 32; ++k) X[lane * XLD + k] = lo[k];
+      for (int k = 0; k < 32; ++k) acc_hi[k] = acc_lo[k] = 0.0;
+      for (int ch = 0; ch < g.nch; ++ch, ++gc) {
+        const int b = gc & 1;
+        if (ok && !bar_wait(tfull + b, (uint32_t)(gc >> 1) & 1u, abort_flag, g.err)) ok = false;
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t t0 = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * 128) + col0;
+        float v[32];
+        tmem_ld32(t0, v);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) acc_hi[k] += (double)v[k];
+        tmem_ld32(t0 + 32, v);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) acc_lo[k] += (double)v[k];
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) bar_arrive(tempty + b);
+      }
+      if (!ok) break;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) X[lane * XLD + k] = (float)acc_lo[k];  // the exchanged term: ~2^-11 of G
       __syncwarp();
       const int t = (int)blockIdx.x + j * (int)gridDim.x;
       const int c = 2 * t + pair_half;
@@ -339,7 +358,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
         for (int k = 0; k < 32; ++k) {
           if (k < g.N) {
             const double x = (double)X[k * XLD + lane];
-            out[2 * k] = (double)hi[k] + (double)lo[k] + (imag ? -x : x);
+            out[2 * k] = acc_hi[k] + acc_lo[k] + (imag ? -x : x);
           }
         }
       }
@@ -349,7 +368,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
   // ---------------------------------------------------------------- teardown
   __syncthreads();
   if (warp == 1) {
-    const int last = *last_commit;
+    const int last = *last_commit;  // every MMA of this CTA is covered by its last chunk commit
     if (last >= 0) bar_drain(tfull + (last & 1), (uint32_t)(last >> 1) & 1u, g.err);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
@@ -387,6 +406,7 @@ nrcps_status gram_tc(nrcps_context* ctx, const void* psi, int N, long vol, int n
   a.N = N;
   a.nr = nr;
   a.nkb = (int)(K / gtc::BK);
+  a.nch = (a.nkb + gtc::CHUNK - 1) / gtc::CHUNK;
   a.ntiles = (nconf + 1) / 2;
   a.G = G;
   a.err = ctx->dev_err;

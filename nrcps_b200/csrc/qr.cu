@@ -310,73 +310,70 @@ __global__ void __launch_bounds__(256, 2) gram4_kernel(const void* __restrict__ 
       }
 }
 
-// psi_{c,t}(p) <- sum_{i <= t} psi_{c,i}(p) Rinv[i][t]; one thread per site
-// at a time, all N orbitals of a configuration in registers (N <= 64),
-// arithmetic in R (FP32 orbitals: Rinv rounded to FP32, see
-// chol_inv_kernel).  Block (chunk, c) stages configuration c's R^-1 in shared
-// memory once and then walks the sites chunk, chunk + chunks, ... of it in
-// strides of its 256 threads.
-constexpr int APPLY_THREADS = 256;
+// psi_{c,t}(p) <- sum_{i <= t} psi_{c,i}(p) Rinv[i][t]; one thread per site,
+// all N orbitals of a configuration in registers (N <= 64), arithmetic in R
+// (FP32 orbitals: Rinv rounded to FP32, see chol_inv_kernel).
 template <typename R, int NMAX>
-__global__ void __launch_bounds__(APPLY_THREADS) apply_rinv_kernel(void* __restrict__ psi, int N, long vol,
-                                                                   int nconf, const double* __restrict__ Rinv) {
+__global__ void __launch_bounds__(256) apply_rinv_kernel(void* __restrict__ psi, int N, long vol, int nconf,
+                                                          const double* __restrict__ Rinv) {
   // R^-1 of this block's configuration: 2 N^2 values in R (FP64), or for FP32
   // N^2 float4 (re, re, im, im) entries that feed packed FMAs
   extern __shared__ __align__(16) double rs_raw[];
   R* rs = reinterpret_cast<R*>(rs_raw);
-  const long c = blockIdx.y;
+  const long sites_per_block = blockDim.x;
+  const long blocks_per_conf = (vol + sites_per_block - 1) / sites_per_block;
+  const long c = blockIdx.x / blocks_per_conf;
   if (c >= nconf) return;
+  const long p = (blockIdx.x % blocks_per_conf) * sites_per_block + threadIdx.x;
+  const bool live = p < vol;
+  cplx<R>* base = reinterpret_cast<cplx<R>*>(psi) + (size_t)c * N * vol + (live ? p : 0);
+  // the orbital loads go out first; their latency covers the fill of R below
+  R xr[NMAX], xi[NMAX];
+#pragma unroll
+  for (int i = 0; i < NMAX; ++i)
+    if (i < N && live) {
+      cplx<R> v = base[(size_t)i * vol];
+      xr[i] = v.re;
+      xi[i] = v.im;
+    }
   if constexpr (sizeof(R) == 4) {
+    // x r = (xr ar - xi ai, xr ai + xi ar): with X = (xr, xi) the packed sums
+    // s = sum X (ar, ar) and u = sum X (ai, ai) give re = s.x - u.y, im = s.y + u.x
     float4* r4 = reinterpret_cast<float4*>(rs_raw);
     for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
       const float ar = (float)Rinv[2L * (c * N * N + e)], ai = (float)Rinv[2L * (c * N * N + e) + 1];
       r4[e] = make_float4(ar, ar, ai, ai);
     }
+    __syncthreads();
+    if (!live) return;
+#pragma unroll
+    for (int t = NMAX - 1; t >= 0; --t) {
+      if (t >= N) continue;
+      float2 sa = make_float2(0.f, 0.f), ua = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int i = 0; i <= t; ++i) {
+        const float4 r = r4[i * N + t];
+        const float2 x = make_float2(xr[i], xi[i]);
+        sa = __ffma2_rn(x, make_float2(r.x, r.y), sa);
+        ua = __ffma2_rn(x, make_float2(r.z, r.w), ua);
+      }
+      base[(size_t)t * vol] = cplx<R>{sa.x - ua.y, sa.y + ua.x};
+    }
   } else {
     for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) rs[e] = (R)Rinv[2L * c * N * N + e];
-  }
-  __syncthreads();
-  cplx<R>* conf = reinterpret_cast<cplx<R>*>(psi) + (size_t)c * N * vol;
-  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < vol; p += (long)gridDim.x * blockDim.x) {
-    cplx<R>* base = conf + p;
-    R xr[NMAX], xi[NMAX];
+    __syncthreads();
+    if (!live) return;
 #pragma unroll
-    for (int i = 0; i < NMAX; ++i)
-      if (i < N) {
-        cplx<R> v = base[(size_t)i * vol];
-        xr[i] = v.re;
-        xi[i] = v.im;
+    for (int t = NMAX - 1; t >= 0; --t) {
+      if (t >= N) continue;
+      R sr = 0, si = 0;
+#pragma unroll
+      for (int i = 0; i <= t; ++i) {
+        const R ar = rs[2 * (i * N + t)], ai = rs[2 * (i * N + t) + 1];
+        sr += xr[i] * ar - xi[i] * ai;
+        si += xr[i] * ai + xi[i] * ar;
       }
-    if constexpr (sizeof(R) == 4) {
-      // x r = (xr ar - xi ai, xr ai + xi ar): with X = (xr, xi) the packed sums
-      // s = sum X (ar, ar) and u = sum X (ai, ai) give re = s.x - u.y, im = s.y + u.x
-      const float4* r4 = reinterpret_cast<const float4*>(rs_raw);
-#pragma unroll
-      for (int t = NMAX - 1; t >= 0; --t) {
-        if (t >= N) continue;
-        float2 sa = make_float2(0.f, 0.f), ua = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int i = 0; i <= t; ++i) {
-          const float4 r = r4[i * N + t];
-          const float2 x = make_float2(xr[i], xi[i]);
-          sa = __ffma2_rn(x, make_float2(r.x, r.y), sa);
-          ua = __ffma2_rn(x, make_float2(r.z, r.w), ua);
-        }
-        base[(size_t)t * vol] = cplx<R>{sa.x - ua.y, sa.y + ua.x};
-      }
-    } else {
-#pragma unroll
-      for (int t = NMAX - 1; t >= 0; --t) {
-        if (t >= N) continue;
-        R sr = 0, si = 0;
-#pragma unroll
-        for (int i = 0; i <= t; ++i) {
-          const R ar = rs[2 * (i * N + t)], ai = rs[2 * (i * N + t) + 1];
-          sr += xr[i] * ar - xi[i] * ai;
-          si += xr[i] * ai + xi[i] * ar;
-        }
-        base[(size_t)t * vol] = cplx<R>{(R)sr, (R)si};
-      }
+      base[(size_t)t * vol] = cplx<R>{(R)sr, (R)si};
     }
   }
 }
@@ -419,25 +416,12 @@ __global__ void rescale_dets_kernel(double* dets, const double* logR, int N, int
 template <int NMAX>
 static nrcps_status launch_apply(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
                                  const double* Rinv) {
-  // blocks per configuration: about 16 site tiles each, at least two waves of
-  // blocks over the SMs
-  const long tiles = (vol + APPLY_THREADS - 1) / APPLY_THREADS;
-  long chunks = (tiles + 15) / 16;
-  const long want = 2L * (ctx->sm_count > 0 ? ctx->sm_count : 148) * 3;
-  while (chunks < tiles && chunks * nconf < want) chunks *= 2;
-  if (chunks > tiles) chunks = tiles;
+  const long bpc = (vol + 255) / 256;
   const size_t sh = sizeof(double) * 2 * N * N;
-  const size_t esz = prec == NRCPS_F64 ? sizeof(cplx<double>) : sizeof(cplx<float>);
-  for (int c0 = 0; c0 < nconf; c0 += 65535) {  // grid.y holds at most 65535 configurations
-    const int nc = nconf - c0 < 65535 ? nconf - c0 : 65535;
-    void* p = static_cast<char*>(psi) + esz * (size_t)c0 * N * vol;
-    const double* r = Rinv + 2L * c0 * N * N;
-    const dim3 grid((unsigned)chunks, (unsigned)nc);
-    if (prec == NRCPS_F64)
-      apply_rinv_kernel<double, NMAX><<<grid, APPLY_THREADS, sh, ctx->stream>>>(p, N, vol, nc, r);
-    else
-      apply_rinv_kernel<float, NMAX><<<grid, APPLY_THREADS, sh, ctx->stream>>>(p, N, vol, nc, r);
-  }
+  if (prec == NRCPS_F64)
+    apply_rinv_kernel<double, NMAX><<<(unsigned)(bpc * nconf), 256, sh, ctx->stream>>>(psi, N, vol, nconf, Rinv);
+  else
+    apply_rinv_kernel<float, NMAX><<<(unsigned)(bpc * nconf), 256, sh, ctx->stream>>>(psi, N, vol, nconf, Rinv);
   ctx->launches++;
   return check_launch(ctx, "apply_rinv_kernel");
 }

@@ -182,7 +182,7 @@ def bench_pair(ctx: Context, L: int, N: int, nconf: int, precision: str, reps: i
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["step", "overlap", "dets", "cv", "qr", "rng", "pair"])
-    ap.add_argument("--gram-tc", type=int, default=1)
+    ap.add_argument("--gram-tc", type=int, default=0)
     ap.add_argument("--L", type=int, default=32)
     ap.add_argument("--orbitals", type=int, default=19456)
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])

@@ -39,8 +39,9 @@ def test_reorthonormalise_against_numpy(N, L, prec):
 
 @pytest.mark.parametrize("N,L,nconf", [(19, 32, 5), (10, 48, 2), (32, 16, 4), (1, 8, 9)])
 def test_tensor_core_gram_against_cuda_cores(N, L, nconf):
-    """The Gram matrices on the tcgen05 tensor cores (TF32 hi/lo, the default
-    for FP32 orbitals with N <= 32) against the CUDA-core kernel, through a
+    """The Gram matrices on the tcgen05 tensor cores (TF32 hi/lo, option
+    "qr.gram_tc" for FP32 orbitals with N <= 32) against the CUDA-core kernel
+    (the default), through a
     whole re-orthonormalisation: the same log R_ii to 2e-5 (FP32 sums over
     2V floats either way) and orthonormal orbitals to the FP32 tolerance of
     the test above (odd configuration counts leave the last tile half
@@ -62,7 +63,7 @@ def test_tensor_core_gram_against_cuda_cores(N, L, nconf):
             ctx.synchronize()
             out[tc] = (logR.cpu().numpy(), psi.cpu().numpy().astype(np.complex128))
     finally:
-        ctx.set_option("qr.gram_tc", 1)
+        ctx.set_option("qr.gram_tc", 0)
     assert np.max(np.abs(out[1][0] - out[0][0]) / np.maximum(np.abs(out[0][0]), 1.0)) < 2e-5
     for c in range(nconf):
         q = out[1][1][c]

@@ -107,6 +107,9 @@ const char *nrcps_version(void);
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the
  *                      CUDA-core kernel with FP64 accumulation;
+ *   "pair.tile"        1 (default): TwoBody pair matrices (n <= 32) by tiles of
+ *                      sites staged in shared memory, one thread-block cluster
+ *                      per configuration; 0: one block per (s, t) pair;
  *   "qr.gram_tc"       1: the Gram matrices of the re-orthonormalisation of
  *                      FP32 orbitals (N <= 32) on the tcgen05 tensor cores
  *                      (TF32 hi/lo); 0 (default): the CUDA-core kernel;

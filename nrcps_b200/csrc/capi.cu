@@ -123,6 +123,8 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
     ctx->lu_warp = value != 0;
   } else if (n == "overlap.tc") {
     ctx->overlap_tc = value != 0;
+  } else if (n == "pair.tile") {
+    ctx->pair_tile = value != 0;
   } else if (n == "qr.gram_tc") {
     ctx->qr_gram_tc = value != 0;
   } else {

@@ -1,9 +1,12 @@
 // measure.cu -- Slater-matrix fills and determinants (the measurement half of
 // every time slice): overlaps S = <src|psi>, the pair matrix of TwoBody, and
 // FP64 LU of every leading minor with the reference's pivoting rule.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace nrcps {
+namespace cg = cooperative_groups;
 
 // ---------------------------------------------------------------- overlap
 // One block per (configuration, orbital t); sources in chunks of 8.  FP64
@@ -116,6 +119,122 @@ __global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1
     phi[2 * e] = sr;
     phi[2 * e + 1] = si;
   }
+}
+
+// Tiled pair matrices for n <= 32 (the path of nrcps_pair_matrix and of the
+// ensemble's pair sink).  One thread-block cluster of up to eight CTAs per
+// configuration; CTA r of C takes every C-th tile of TS sites.  A
+// tile stages a_s(i) = w_i psi1_s(i) and b_t(i) = psi2_t(opp(i)) for all n
+// orbitals in shared memory (each orbital read once; the gathered rows of a
+// configuration are read while its direct rows are still in L2), and thread
+// (block, group) accumulates the 2 x 2 block (s0, s0+1) x (t0, t0+1) of
+// phi over the group's sites: in R within a tile, in FP64 across tiles.  The
+// groups are summed in shared memory and the cluster's CTAs in rank order
+// through distributed shared memory: the result does not depend on timing.
+constexpr int PAIR_THREADS = 256;
+constexpr int PAIR_MAXN = 32;
+
+// TS sites per tile: 128 FP32 / 64 FP64 complex values per staged orbital row
+// (1 KB), so that n = 32 needs 66 KB of shared memory and three CTAs fit an SM
+template <typename R>
+struct PairShape {
+  static constexpr int TS = sizeof(R) == 4 ? 128 : 64;
+  static constexpr int LD = TS + 1;  // padded row: rows s0 and s1 sit in different banks
+  static size_t smem(int n) {
+    const size_t tiles = 2 * (size_t)n * LD * sizeof(cplx<R>);
+    const size_t nb = (n + 1) / 2, red = nb * nb * 8 * sizeof(double);
+    return tiles > red ? tiles : red;
+  }
+};
+
+template <typename R>
+__global__ void __launch_bounds__(PAIR_THREADS) pair_tile_kernel(const void* __restrict__ psi1,
+                                                                 const void* __restrict__ psi2, int n, long vol,
+                                                                 const double* __restrict__ w,
+                                                                 const int* __restrict__ opp,
+                                                                 double* __restrict__ phi) {
+  constexpr int LD = PairShape<R>::LD, PAIR_TS = PairShape<R>::TS;
+  extern __shared__ __align__(16) unsigned char pair_smem[];
+  cplx<R>* A = reinterpret_cast<cplx<R>*>(pair_smem);  // [n][LD]: w_i psi1_s(i)
+  cplx<R>* B = A + (size_t)n * LD;                      // [n][LD]: psi2_t(opp(i))
+  cg::cluster_group cluster = cg::this_cluster();
+  const int split = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
+  const long conf = blockIdx.x / split;
+  const cplx<R>* a_base = reinterpret_cast<const cplx<R>*>(psi1) + (size_t)conf * n * vol;
+  const cplx<R>* b_base = reinterpret_cast<const cplx<R>*>(psi2) + (size_t)conf * n * vol;
+  const int nb = (n + 1) / 2;                 // 2-row blocks
+  const int nblk = nb * nb;                   // (s, t) block pairs
+  const int groups = PAIR_THREADS / nblk;     // >= 1 for n <= 32
+  const int g = threadIdx.x % groups, blk = threadIdx.x / groups;
+  const bool active = blk < nblk;
+  const int s0 = 2 * (active ? blk / nb : 0), t0 = 2 * (active ? blk % nb : 0);
+  const int s1 = s0 + 1 < n ? s0 + 1 : s0, t1 = t0 + 1 < n ? t0 + 1 : t0;
+  double acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+  const long ntiles = (vol + PAIR_TS - 1) / PAIR_TS;
+  for (long tile = rank; tile < ntiles; tile += split) {
+    const long i0 = tile * PAIR_TS;
+    const int ts = (int)(vol - i0 < PAIR_TS ? vol - i0 : PAIR_TS);
+    __syncthreads();  // the previous tile is consumed
+#pragma unroll 4
+    for (int e = threadIdx.x; e < n * PAIR_TS; e += PAIR_THREADS) {
+      const int o = e / PAIR_TS, q = e % PAIR_TS;
+      cplx<R> x{(R)0, (R)0}, y{(R)0, (R)0};
+      if (q < ts) {
+        const long i = i0 + q;
+        x = a_base[(size_t)o * vol + i];
+        const R wi = (R)__ldg(w + i);
+        x.re *= wi;
+        x.im *= wi;
+        y = b_base[(size_t)o * vol + __ldg(opp + i)];
+      }
+      A[o * LD + q] = x;
+      B[o * LD + q] = y;
+    }
+    __syncthreads();
+    if (active) {
+      // sum_i a_s(i) b_t(i) for the 2 x 2 block, complex, no conjugation
+      R r[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) r[k] = (R)0;
+      for (int q = g; q < ts; q += groups) {
+        const cplx<R> a0 = A[s0 * LD + q], a1 = A[s1 * LD + q];
+        const cplx<R> b0 = B[t0 * LD + q], b1 = B[t1 * LD + q];
+        r[0] += a0.re * b0.re - a0.im * b0.im;
+        r[1] += a0.re * b0.im + a0.im * b0.re;
+        r[2] += a0.re * b1.re - a0.im * b1.im;
+        r[3] += a0.re * b1.im + a0.im * b1.re;
+        r[4] += a1.re * b0.re - a1.im * b0.im;
+        r[5] += a1.re * b0.im + a1.im * b0.re;
+        r[6] += a1.re * b1.re - a1.im * b1.im;
+        r[7] += a1.re * b1.im + a1.im * b1.re;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] += (double)r[k];
+    }
+  }
+  // sum the groups of every block pair in shared memory (fixed order), then
+  // the cluster's CTAs in rank order
+  __syncthreads();
+  double* red = reinterpret_cast<double*>(pair_smem);  // [nblk][8], group 0 first
+  for (int gg = 0; gg < groups; ++gg) {
+    if (active && g == gg)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) red[blk * 8 + k] = (gg == 0 ? 0.0 : red[blk * 8 + k]) + acc[k];
+    __syncthreads();
+  }
+  cluster.sync();  // every CTA's sums are in its shared memory
+  if (rank == 0) {
+    for (int e = threadIdx.x; e < nblk * 8; e += PAIR_THREADS) {
+      double v = 0.0;
+      for (int r2 = 0; r2 < split; ++r2) v += cluster.map_shared_rank(red, r2)[e];
+      const int b = e >> 3, k = e & 7;
+      const int s = 2 * (b / nb) + ((k >> 2) & 1), t = 2 * (b % nb) + ((k >> 1) & 1);
+      if (s < n && t < n) phi[2 * ((conf * n + s) * (long)n + t) + (k & 1)] = v;
+    }
+  }
+  cluster.sync();  // peers keep their shared memory until rank 0 has read it
 }
 
 // GeneralizedTwoBody::Run (src/two_body/noarch/two_body_run.C:45-75) batched:
@@ -549,10 +668,49 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
   return check_launch(ctx, "gather_kernel");
 }
 
+template <typename R>
+static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf,
+                                     long vol, const double* w, const int* opp, double* phi) {
+  const size_t smem = PairShape<R>::smem(n);
+  static bool attr_set[16] = {false};
+  if (!attr_set[ctx->device & 15]) {
+    NRCPS_TRY(check_cuda(ctx, cudaFuncSetAttribute(pair_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)PairShape<R>::smem(PAIR_MAXN)),
+                         "pair_tile: smem attribute"));
+    attr_set[ctx->device & 15] = true;
+  }
+  // CTAs per configuration: enough CTAs for about eight per SM, at most 8
+  // (a portable cluster) and no more than the tiles
+  const long ntiles = (vol + PairShape<R>::TS - 1) / PairShape<R>::TS;
+  int split = (int)((8L * ctx->sm_count + nconf - 1) / nconf);
+  if (split > 8) split = 8;
+  if (split > ntiles) split = (int)ntiles;
+  if (split < 1) split = 1;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)split;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)((long)nconf * split));
+  cfg.blockDim = dim3(PAIR_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, pair_tile_kernel<R>, psi1, psi2, n, vol, w, opp, phi);
+  ctx->launches++;
+  return check_cuda(ctx, e, "pair_tile_kernel launch");
+}
+
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
                        const double* w, const int* opp, nrcps_precision prec, double* phi) {
   long blocks = (long)nconf * n * n;
   if (blocks == 0) return NRCPS_OK;
+  if (n <= PAIR_MAXN && ctx->pair_tile && (long)nconf * 8 < (1L << 31)) {
+    if (prec == NRCPS_F64) return launch_pair_tile<double>(ctx, psi1, psi2, n, nconf, vol, w, opp, phi);
+    return launch_pair_tile<float>(ctx, psi1, psi2, n, nconf, vol, w, opp, phi);
+  }
   if (prec == NRCPS_F64) pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
   else pair_kernel<float><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
   ctx->launches++;

@@ -107,6 +107,10 @@ const char *nrcps_version(void);
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the
  *                      CUDA-core kernel with FP64 accumulation;
+ *   "fused.zpos"       1 (default): for a Z2 field with a position factor the
+ *                      fused step reads both weights of every site,
+ *                      (1 +- a) P(x)/V, from a table made ahead of the step;
+ *                      0: forms them per site (the same values);
  *   "pair.tile"        1 (default): TwoBody pair matrices (n <= 32) by tiles of
  *                      sites staged in shared memory, one thread-block cluster
  *                      per configuration; 0: one block per (s, t) pair;

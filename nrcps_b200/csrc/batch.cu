@@ -30,7 +30,8 @@ size_t slater_dets_scratch_bytes(int N, int nconf, int mode);
 nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const void* psi, int nt, int nconf, long vol,
                          nrcps_precision prec, double* S);
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
-                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec);
+                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec,
+                            const void* zpos);
 nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster);
 nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
                                  double* G, double* logR);
@@ -146,7 +147,7 @@ static nrcps_status record_batch(nrcps_batch* b, double* out) {
       pf.dev_conf_base = g.conf_base;
       pf.a = b->params.a;
       pf.dev_pos = nullptr;
-      if ((st = propagate_impl(ctx, g.psi, g.N, nn, d3, g.kinv, g.kinv_f, &pf, prec))) break;
+      if ((st = propagate_impl(ctx, g.psi, g.N, nn, d3, g.kinv, g.kinv_f, &pf, prec, nullptr))) break;
       if (g.qr_logR && (t + 1) % b->params.qr_period == 0 &&
           (st = qr_reorthonormalise(ctx, g.psi, g.N, g.V, nn, prec, g.qr_G, g.qr_logR)))
         break;

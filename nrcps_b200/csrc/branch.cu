@@ -28,7 +28,8 @@ namespace nrcps {
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
                        const double* w, const int* opp, nrcps_precision prec, double* phi);
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
-                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec);
+                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec,
+                            const void* zpos);
 nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster);
 
 namespace {
@@ -257,7 +258,7 @@ extern "C" nrcps_status nrcps_branch_run(nrcps_branch* b, double* dev_corr) {
       pf.dev_conf_base = b->base;
       pf.a = p.a;
       pf.dev_pos = b->pos;
-      NRCPS_TRY(propagate_impl(ctx, b->psi[cur], 2, (int)nn, p.dims, b->kinv, b->kinv_f, &pf, prec));
+      NRCPS_TRY(propagate_impl(ctx, b->psi[cur], 2, (int)nn, p.dims, b->kinv, b->kinv_f, &pf, prec, nullptr));
     }
   }
   return NRCPS_OK;

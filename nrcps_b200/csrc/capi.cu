@@ -79,6 +79,7 @@ extern "C" nrcps_status nrcps_destroy(nrcps_context* ctx) {
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->gen_args) cudaFree(ctx->gen_args);
   if (ctx->kin_f32) cudaFree(ctx->kin_f32);
+  if (ctx->zpos) cudaFree(ctx->zpos);
   if (ctx->tc_split) cudaFree(ctx->tc_split);
   if (ctx->dev_err) cudaFree(ctx->dev_err);
   delete ctx;
@@ -123,6 +124,8 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
     ctx->lu_warp = value != 0;
   } else if (n == "overlap.tc") {
     ctx->overlap_tc = value != 0;
+  } else if (n == "fused.zpos") {
+    ctx->fused_zpos = value != 0;
   } else if (n == "pair.tile") {
     ctx->pair_tile = value != 0;
   } else if (n == "qr.gram_tc") {

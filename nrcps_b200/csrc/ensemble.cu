@@ -27,7 +27,8 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
                        const double* w, const int* opp, nrcps_precision prec, double* phi);
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
-                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec);
+                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec,
+                            const void* zpos);
 nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int* chosen_cluster);
 nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol, int nconf, nrcps_precision prec,
                                  double* G, double* logR);
@@ -48,6 +49,7 @@ struct nrcps_ensemble {
   double* kinv = nullptr;
   float2* kinv_f = nullptr;  // (hi, lo) split of kinv
   double* pos = nullptr;
+  void* zpos = nullptr;        // Z2 fields with the potential: per-site weights (zpos_table_kernel's layout)
   double* itab = nullptr;
   double* w = nullptr;
   int* opp = nullptr;
@@ -198,7 +200,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       pf.bit0 = (uint64_t)t * vol;
       pf.conf_stride = (uint64_t)T * vol;
     }
-    NRCPS_TRY(propagate_impl(ctx, e->psi, N, nc, d3, e->kinv, e->kinv_f, &pf, prec));
+    NRCPS_TRY(propagate_impl(ctx, e->psi, N, nc, d3, e->kinv, e->kinv_f, &pf, prec, e->zpos));
     if (e->qr_logR && (t + 1) % j.qr_period == 0 && t + 1 < T)
       NRCPS_TRY(qr_reorthonormalise(ctx, e->psi, N, vol, nc, prec, e->qr_G, e->qr_logR));
   }
@@ -285,6 +287,26 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   const uint64_t sites = (uint64_t)nc * job->T * V;
   if (fk == NRCPS_FIELD_ZTWO) {
     if ((st = dalloc(ctx, &e->bits, 4 * ((sites + 31) / 32 + 1)))) return fail(st);
+    if (job->use_potential && job->local_interaction) {
+      // the fused step's per-site weights (1 +- a) P/V, P = h (the squared,
+      // scaled potential above): the products the general path forms per site
+      const double wp = (1.0 + job->a) / (double)V, wm = (1.0 - job->a) / (double)V;
+      if (job->precision == NRCPS_F32) {
+        std::vector<float4> t(V);
+        for (long i = 0; i < V; ++i) {
+          const double p = wp * h[i], m = wm * h[i];
+          const float hp = (float)p, hm = (float)m;
+          t[i] = make_float4(hp, (float)(p - (double)hp), hm, (float)(m - (double)hm));
+        }
+        if ((st = dalloc(ctx, (char**)&e->zpos, 16 * V)) || (st = upload(ctx, e->zpos, t.data(), 16 * V)))
+          return fail(st);
+      } else {
+        std::vector<double2> t(V);
+        for (long i = 0; i < V; ++i) t[i] = make_double2(wp * h[i], wm * h[i]);
+        if ((st = dalloc(ctx, (char**)&e->zpos, 16 * V)) || (st = upload(ctx, e->zpos, t.data(), 16 * V)))
+          return fail(st);
+      }
+    }
   } else {
     if ((st = dalloc(ctx, &e->phi, 16 * sites))) return fail(st);
   }
@@ -387,7 +409,7 @@ extern "C" nrcps_status nrcps_ensemble_destroy(nrcps_ensemble* e) {
   if (e->ctx) cudaStreamSynchronize(e->ctx->stream);
   if (e->exec) cudaGraphExecDestroy(e->exec);
   if (e->graph) cudaGraphDestroy(e->graph);
-  void* bufs[] = {e->psi, e->src, e->src_split, e->pw_index, e->kinv, e->kinv_f, e->pos, e->itab, e->w, e->opp,
+  void* bufs[] = {e->psi, e->src, e->src_split, e->pw_index, e->kinv, e->kinv_f, e->pos, e->zpos, e->itab, e->w, e->opp,
                   e->bits, e->phi, e->fld, e->S, e->P1, e->lu_scr, e->qr_G, e->qr_logR};
   for (void* b : bufs)
     if (b) cudaFree(b);

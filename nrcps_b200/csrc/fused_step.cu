@@ -40,6 +40,8 @@ struct FusedArgs {
   const float2* kin_f;    // k(p) split as (hi, lo) floats, hi + lo = k to ~1e-15 (R = float)
   const double* kin_d;    // k(p) in FP64 (R = double)
   const double* pos;      // optional P(x)
+  const void* zpos;       // Z2 fields with P(x): per site the weights (1 + a) P(x)/V and (1 - a) P(x)/V,
+                          // split (hi, lo, hi, lo) as float4 for R = float, (plus, minus) double2 for double
   int field_mode;         // 1 bits, 2 complex phi, 0 complex fld
   const void* field;
   uint64_t off0;          // element/bit offset of configuration 0
@@ -97,6 +99,24 @@ __device__ __forceinline__ cplx<R> apply_kin(const FusedArgs& f, int site, cplx<
   } else {
     R k = __ldg(f.kin_d + site);
     return cplx<R>{x.re * k, x.im * k};
+  }
+}
+
+// x * (hi + lo), packed when PK (FP32 only)
+template <typename R, bool PK>
+__device__ __forceinline__ cplx<R> scale_w(cplx<R> x, R hi, R lo);
+
+// x * w for a Z2 site with a position factor, from the table of both weights
+// of every site: the value apply_w_general gives (the table holds the same
+// products w_plus * P and w_minus * P, split the same way)
+template <typename R, bool PK>
+__device__ __forceinline__ cplx<R> scale_w_zpos(const void* tab, int site, bool up, cplx<R> x) {
+  if constexpr (sizeof(R) == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(tab) + site);
+    return scale_w<R, PK>(x, up ? t.x : t.z, up ? t.y : t.w);
+  } else {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(tab) + site);
+    return scale_w<R, PK>(x, up ? t.x : t.y, (R)0);
   }
 }
 
@@ -266,6 +286,7 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
   };
 
   const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  const bool z2_pos = (f.field_mode == 1) && (f.zpos != nullptr) && ((L * L) % 32 == 0);
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
@@ -402,6 +423,15 @@ __global__ void __launch_bounds__(PullShape<R, L, C, STAGED>::THREADS, PullShape
             x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
           }
         }
+      } else if (z2_pos) {
+        const uint64_t k0 = kb + (uint64_t)site0;
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
+        const int bit = (int)(k0 & 31);
+#pragma unroll
+        for (int xx = 0; xx < L; ++xx) {
+          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+          x[xx] = scale_w_zpos<R, PK>(f.zpos, site0 + xx * L * L, up, x[xx]);
+        }
       } else {
 #pragma unroll
         for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
@@ -497,6 +527,7 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
   };
 
   const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  const bool z2_pos = (f.field_mode == 1) && (f.zpos != nullptr) && ((L * L) % 32 == 0);
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
@@ -605,6 +636,16 @@ __global__ void __launch_bounds__(SplitShape<R, L, C>::THREADS, SplitShape<R, L,
             const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
             v[k] = scale2<R>(v[k], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
           }
+        }
+      } else if (z2_pos) {
+        const uint64_t k0 = kb + (uint64_t)site0;
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
+        const int bit = (int)(k0 & 31);
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+          const int xx = h * H + k;
+          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+          v[k] = scale_w_zpos<R, false>(f.zpos, site0 + xx * L * L, up, v[k]);
         }
       } else {
 #pragma unroll
@@ -765,6 +806,7 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
   };
 
   const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  const bool z2_pos = (f.field_mode == 1) && (f.zpos != nullptr) && ((L * L) % 32 == 0);
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
@@ -904,6 +946,15 @@ __global__ void __launch_bounds__(BulkShape<R, L, C, STAGED, KSM>::THREADS,
             const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
             x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
           }
+        }
+      } else if (z2_pos) {
+        const uint64_t k0 = kb + (uint64_t)site0;
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
+        const int bit = (int)(k0 & 31);
+#pragma unroll
+        for (int xx = 0; xx < L; ++xx) {
+          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+          x[xx] = scale_w_zpos<R, PK>(f.zpos, site0 + xx * L * L, up, x[xx]);
         }
       } else {
 #pragma unroll
@@ -1060,6 +1111,7 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
   };
 
   const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  const bool z2_pos = (f.field_mode == 1) && (f.zpos != nullptr) && ((L * L) % 32 == 0);
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
@@ -1166,6 +1218,15 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
             const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
             x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
           }
+        }
+      } else if (z2_pos) {
+        const uint64_t k0 = kb + (uint64_t)site0;
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
+        const int bit = (int)(k0 & 31);
+#pragma unroll
+        for (int xx = 0; xx < L; ++xx) {
+          const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
+          x[xx] = scale_w_zpos<R, PK>(f.zpos, site0 + xx * L * L, up, x[xx]);
         }
       } else {
 #pragma unroll
@@ -1558,7 +1619,7 @@ nrcps_status fused_choice(nrcps_context* ctx, nrcps_precision prec, int L, int* 
 // One fused step; `kin_table` is (hi, lo) float pairs for prec F32 and FP64 for F64.
 // cluster = 0 selects the autotuned (or default) cluster size.
 nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const void* kin_table,
-                        nrcps_precision prec, const nrcps_position_factor* w, int cluster) {
+                        nrcps_precision prec, const nrcps_position_factor* w, int cluster, const void* zpos) {
   if (!fused_supported(prec, d)) return NRCPS_ERR_UNSUPPORTED;
   FusedArgs f;
   f.psi = psi;
@@ -1567,6 +1628,7 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
   f.kin_f = prec == NRCPS_F32 ? (const float2*)kin_table : nullptr;
   f.kin_d = prec == NRCPS_F64 ? (const double*)kin_table : nullptr;
   f.pos = w->dev_pos;
+  f.zpos = (w->field_mode == 1 && w->dev_pos && ctx->fused_zpos) ? zpos : nullptr;
   f.field_mode = w->field_mode;
   f.field = w->dev_field;
   f.off0 = w->bit0;

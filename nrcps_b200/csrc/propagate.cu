@@ -306,7 +306,23 @@ extern "C" nrcps_status nrcps_interaction_initialize(nrcps_context* ctx, const d
 namespace nrcps {
 bool fused_supported(nrcps_precision prec, const int d[3]);
 nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const void* kin_table,
-                        nrcps_precision prec, const nrcps_position_factor* w, int cluster);
+                        nrcps_precision prec, const nrcps_position_factor* w, int cluster, const void* zpos);
+
+// The per-site weights of a Z2 field times a position factor P:
+// (1 + a) P/V and (1 - a) P/V, each split (hi, lo) into floats (float4 per
+// site) for FP32 orbitals, plain doubles (double2 per site) for FP64.
+__global__ void zpos_table_kernel(void* tab, const double* pos, double w_plus, double w_minus, long n, int f32) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double p = pos[i];
+    const double wp = w_plus * p, wm = w_minus * p;
+    if (f32) {
+      const float hp = (float)wp, hm = (float)wm;
+      reinterpret_cast<float4*>(tab)[i] = make_float4(hp, (float)(wp - (double)hp), hm, (float)(wm - (double)hm));
+    } else {
+      reinterpret_cast<double2*>(tab)[i] = make_double2(wp, wm);
+    }
+  }
+}
 
 // k -> (hi, lo) float pairs with hi + lo = k to ~1e-15.
 __global__ void split_f32_kernel(float2* dst, const double* src, long n) {
@@ -332,9 +348,13 @@ static nrcps_status propagate_t(nrcps_context* ctx, void* psi, int batch, int nc
 
 namespace nrcps {
 // Propagator step for the ensemble and the C ABI.  kin_f32 may be NULL (then
-// an FP32 copy of kin is made in the context when the FP32 fused kernel runs).
+// an FP32 copy of kin is made in the context when the FP32 fused kernel runs);
+// so may zpos, the Z2-times-position-factor weights (zpos_table_kernel), which
+// the fused kernel reads for a Z2 field with a position factor: then they are
+// made in the context.
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
-                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec) {
+                            const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec,
+                            const void* zpos) {
   if (ctx->fused_enabled && fused_supported(prec, d)) {
     const void* table = kin;
     if (prec == NRCPS_F32) {
@@ -354,7 +374,22 @@ nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf,
       }
       table = kin_f32;
     }
-    nrcps_status st = fused_step(ctx, psi, batch, nconf, d, table, prec, w, ctx->fused_cluster);
+    if (w->field_mode == 1 && w->dev_pos && !zpos && ctx->fused_zpos) {
+      const long V = vol_of(d);
+      if (ctx->zpos_len < 16 * V) {
+        if (ctx->zpos) cudaFree(ctx->zpos);
+        ctx->zpos = nullptr;
+        ctx->zpos_len = 0;
+        NRCPS_TRY(check_cuda(ctx, cudaMalloc(&ctx->zpos, 16 * V), "cudaMalloc(Z2 position weights)"));
+        ctx->zpos_len = 16 * V;
+      }
+      zpos_table_kernel<<<grid_for(V, 256), 256, 0, ctx->stream>>>(ctx->zpos, w->dev_pos, (1.0 + w->a) / (double)V,
+                                                                   (1.0 - w->a) / (double)V, V, prec == NRCPS_F32);
+      ctx->launches++;
+      NRCPS_TRY(check_launch(ctx, "zpos_table_kernel"));
+      zpos = ctx->zpos;
+    }
+    nrcps_status st = fused_step(ctx, psi, batch, nconf, d, table, prec, w, ctx->fused_cluster, zpos);
     if (st != NRCPS_ERR_UNSUPPORTED) return st;
   }
   FieldArgs f;
@@ -382,5 +417,5 @@ extern "C" nrcps_status nrcps_propagate(nrcps_context* ctx, void* psi, int batch
   NRCPS_REQUIRE(ctx, w->field_mode >= 0 && w->field_mode <= 2, "nrcps_propagate: bad field_mode");
   NRCPS_TRY(check_dims(ctx, dims));
   if (nconf == 0) return NRCPS_OK;
-  return propagate_impl(ctx, psi, batch, nconf, dims, dev_kin, nullptr, w, prec);
+  return propagate_impl(ctx, psi, batch, nconf, dims, dev_kin, nullptr, w, prec, nullptr);
 }

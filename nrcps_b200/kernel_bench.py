@@ -7,7 +7,7 @@ context's stream, after warm-up), one JSON line per measurement.
     python -m nrcps_b200.kernel_bench cv      --T 64 --batch 256
     python -m nrcps_b200.kernel_bench qr      --L 32 --N 19 --nconf 1024 [--precision f32] [--gram-tc 1|0]
     python -m nrcps_b200.kernel_bench rng     --L 32 --T 64 --nconf 1024
-    python -m nrcps_b200.kernel_bench pair    --L 48 --N 10 --nconf 1024 [--precision f32]
+    python -m nrcps_b200.kernel_bench pair    --L 48 --N 10 --nconf 1024 [--precision f32] [--pair-tile 0]
 
 step:    one transfer-matrix step (nrcps_propagate, Z2 field, a = 0.5) over
          `orbitals` orbitals in batches of 19; GB/s counts one read and one
@@ -183,6 +183,7 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["step", "overlap", "dets", "cv", "qr", "rng", "pair"])
     ap.add_argument("--gram-tc", type=int, default=0)
+    ap.add_argument("--pair-tile", type=int, default=1)
     ap.add_argument("--L", type=int, default=32)
     ap.add_argument("--orbitals", type=int, default=19456)
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
@@ -210,7 +211,9 @@ def main(argv=None) -> int:
     elif a.what == "rng":
         r = bench_rng(ctx, a.L, a.T, a.nconf, a.reps)
     elif a.what == "pair":
+        ctx.set_option("pair.tile", a.pair_tile)
         r = bench_pair(ctx, a.L, a.N, a.nconf, a.precision, a.reps)
+        r["pair_tile"] = a.pair_tile
     else:
         r = bench_dets(ctx, a.N, a.nconf, a.reps)
     print(json.dumps(r), flush=True)

@@ -591,6 +591,46 @@ def test_same_arithmetic_variants_are_bit_identical(ctx, kind, ref_kind, precisi
         ctx.set_option("fused.kind", -1)
 
 
+@pytest.mark.parametrize("kind,precision,L,cluster", [(0, "f32", 32, 8), (4, "f32", 48, 16), (3, "f32", 48, 16),
+                                                      (1, "f32", 48, 16), (11, "f32", 32, 8), (7, "f32", 32, 8),
+                                                      (2, "f32", 24, 4), (0, "f64", 32, 16), (11, "f64", 24, 4),
+                                                      (0, "f32", 16, 1)])
+def test_z2_position_weights_table_is_bit_identical(ctx, kind, precision, L, cluster):
+    """A Z2 field with a position factor P ([K,V,I,V,K]): the fused step reads
+    the weights (1 +- a) P(x)/V of every site from a table made ahead of the
+    step ("fused.zpos" 1) or forms them per site from P ("fused.zpos" 0).
+    The table holds the same products split the same way, so the two agree
+    bit for bit; against the pencil passes they agree to rounding."""
+    psi, kinv, bits = _random_step_inputs(ctx, L, 3, 5, precision, seed=8)
+    rs = np.random.default_rng(L)
+    pos = torch.from_numpy(np.exp(-rs.uniform(0.0, 2.0, L ** 3))).to(ctx.device)
+    outs = []
+    try:
+        ctx.set_option("fused.cluster", cluster)
+        ctx.set_option("fused.kind", kind)
+        for zpos in (0, 1):
+            ctx.set_option("fused.zpos", zpos)
+            q = psi.clone()
+            nb.propagate(q, 5, kinv, bits, 0.5, pos=pos, ctx=ctx)
+            outs.append(q)
+        choice = ctx.fused_choice(precision, L)
+        ctx.set_option("fused.kind", -1)
+        ctx.set_option("fused.cluster", 0)
+        ctx.set_option("propagate.fused", 0)
+        ref = psi.clone()
+        nb.propagate(ref, 5, kinv, bits, 0.5, pos=pos, ctx=ctx)
+        ctx.synchronize()
+    finally:
+        ctx.set_option("propagate.fused", 1)
+        ctx.set_option("fused.zpos", 1)
+        ctx.set_option("fused.cluster", 0)
+        ctx.set_option("fused.kind", -1)
+    assert choice == (kind, cluster)
+    assert torch.equal(outs[0], outs[1])
+    tol = 1e-13 if precision == "f64" else 3e-6
+    assert max_norm_err(outs[1].cpu().numpy(), ref.cpu().numpy()) < tol
+
+
 @pytest.mark.parametrize("kind,ref_kind,L,cluster", [(10, 0, 16, 2), (10, 0, 24, 4), (9, 4, 24, 4), (9, 5, 32, 8)])
 def test_resident_kinetic_slab_variants(ctx, kind, ref_kind, L, cluster):
     """Kinds 9 and 10 read k(p) from the CTA's resident slab in shared

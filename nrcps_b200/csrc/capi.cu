@@ -64,11 +64,12 @@ extern "C" nrcps_status nrcps_create(int device, nrcps_context** out) {
   nrcps_context* ctx = new nrcps_context();
   ctx->device = device;
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
-  if (cudaMalloc((void**)&ctx->dev_err, sizeof(int)) != cudaSuccess ||
-      cudaMemset(ctx->dev_err, 0, sizeof(int)) != cudaSuccess) {
+  if (cudaMalloc((void**)&ctx->dev_err, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMemset(ctx->dev_err, 0, 2 * sizeof(int)) != cudaSuccess) {
     delete ctx;
     return NRCPS_ERR_CUDA;
   }
+  ctx->dev_pair_flag = ctx->dev_err + 1;
   *out = ctx;
   return NRCPS_OK;
 }
@@ -113,7 +114,7 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
     if (value < -1 || value > 1) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.split out of range");
     ctx->fused_split = (int)value;
   } else if (n == "fused.kind") {
-    if (value < -1 || value > 12) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
+    if (value < -1 || value > 14) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
     ctx->fused_kind = (int)value;
   } else if (n == "fused.wait_ns") {
     if (value < 1000) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.wait_ns below 1000 ns");

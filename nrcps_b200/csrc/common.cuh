@@ -105,7 +105,8 @@ struct Context {
   // TF32 hi / lo split of the sources for nrcps_overlap's tensor-core path (grown on demand)
   void* tc_split = nullptr;
   size_t tc_split_bytes = 0;
-  int* dev_err = nullptr;  // device flag set by kernels whose bounded waits time out
+  int* dev_err = nullptr;
+  int* dev_pair_flag = nullptr;  // the word after dev_err: 1 = the last checked opposite-site table is no involution  // device flag set by kernels whose bounded waits time out
   // Time limit of every mbarrier wait in the fused step (nanoseconds of the
   // GPU's global timer; the legitimate waits take microseconds).
   unsigned long long fused_wait_ns = 2000000000ull;
@@ -139,6 +140,13 @@ size_t overlap_tc_split_bytes(int ns, long vol);
 nrcps_status overlap_tc_prepare(nrcps_context* ctx, const double* src, int ns, long vol, float* split);
 nrcps_status overlap_tc(nrcps_context* ctx, const float* split, int ns, const void* psi, int nt, int nconf, long vol,
                         double* S);
+
+// true when opp (host) is an involution of [0, vol), as TwoBody's parity mirror is
+inline bool is_involution(const int* opp, long vol) {
+  for (long i = 0; i < vol; ++i)
+    if (opp[i] < 0 || opp[i] >= vol || opp[opp[i]] != i) return false;
+  return true;
+}
 
 inline unsigned grid_for(long n, int block, long cap = 148L * 64) {
   long g = (n + block - 1) / block;

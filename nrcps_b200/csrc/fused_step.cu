@@ -1079,8 +1079,9 @@ __device__ __forceinline__ void st_async(uint32_t addr, cplx<R> v, uint32_t bar)
                  : "memory");
 }
 
-template <typename R, int L, int C, bool PK = false>
-__global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<R, L, C, false>::MIN_BLOCKS)
+template <typename R, int L, int C, bool PK = false, int MINB = 0>
+__global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
+                                  MINB > 0 ? MINB : PullShape<R, L, C, false>::MIN_BLOCKS)
     fused_step_async_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
   static_assert(C > 1, "the write-back goes to cluster peers");
@@ -1294,17 +1295,18 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
 // into L2 instead of staged (four CTAs per SM); 9, 10: kinds 6, 3 with the
 // CTA's slab of the kinetic table resident in shared memory (FP32 only);
 // 11, 12: kinds 7, 8 with the x pass written back by st.async onto the
-// owners' mbarriers (one cluster barrier per orbital).
+// owners' mbarriers (one cluster barrier per orbital); 13, 14: kinds 11, 12
+// compiled for five CTAs per SM (fewer registers per thread, more warps).
 template <typename R, int L, int C, int KIND = 0>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
-  static_assert(KIND < 4 || KIND == 7 || KIND == 11 || sizeof(R) == 4,
+  static_assert(KIND < 4 || KIND == 7 || KIND == 11 || KIND == 13 || sizeof(R) == 4,
                 "packed transforms and the resident k(p) slab are FP32");
   constexpr int THREADS = KIND == 1 ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
   constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
                           : (KIND == 3 || KIND == 6) ? BulkShape<R, L, C, false>::SMEM
                           : (KIND == 9 || KIND == 10) ? BulkShape<R, L, C, false, true>::SMEM
-                          : (KIND == 7 || KIND == 8 || KIND == 11 || KIND == 12) ? PullShape<R, L, C, false>::SMEM
+                          : (KIND == 7 || KIND == 8 || KIND >= 11) ? PullShape<R, L, C, false>::SMEM
                                                      : Sh::SMEM;
   void (*kern)(FusedArgs);
   if constexpr (KIND == 1) kern = fused_step_split_kernel<R, L, C>;
@@ -1319,6 +1321,8 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   else if constexpr (KIND == 8) kern = fused_step_kernel<R, L, C, true, false>;
   else if constexpr (KIND == 11) kern = fused_step_async_kernel<R, L, C, false>;
   else if constexpr (KIND == 12) kern = fused_step_async_kernel<R, L, C, true>;
+  else if constexpr (KIND == 13) kern = fused_step_async_kernel<R, L, C, false, 5>;
+  else if constexpr (KIND == 14) kern = fused_step_async_kernel<R, L, C, true, 5>;
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");
@@ -1399,6 +1403,8 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 32, 8, 7, launch_fused<float, 32, 8, 7>},
     {NRCPS_F32, 32, 8, 11, launch_fused<float, 32, 8, 11>},
     {NRCPS_F32, 32, 8, 12, launch_fused<float, 32, 8, 12>},
+    {NRCPS_F32, 32, 8, 13, launch_fused<float, 32, 8, 13>},
+    {NRCPS_F32, 32, 8, 14, launch_fused<float, 32, 8, 14>},
     {NRCPS_F32, 32, 16, 11, launch_fused<float, 32, 16, 11>},
     {NRCPS_F32, 32, 8, 8, launch_fused<float, 32, 8, 8>},
     {NRCPS_F32, 32, 8, 6, launch_fused<float, 32, 8, 6>},

@@ -123,118 +123,165 @@ __global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1
 
 // Tiled pair matrices for n <= 32 (the path of nrcps_pair_matrix and of the
 // ensemble's pair sink).  One thread-block cluster of up to eight CTAs per
-// configuration; CTA r of C takes every C-th tile of TS sites.  A
-// tile stages a_s(i) = w_i psi1_s(i) and b_t(i) = psi2_t(opp(i)) for all n
-// orbitals in shared memory (each orbital read once; the gathered rows of a
-// configuration are read while its direct rows are still in L2), and thread
-// (block, group) accumulates the 2 x 2 block (s0, s0+1) x (t0, t0+1) of
-// phi over the group's sites: in R within a tile, in FP64 across tiles.  The
+// configuration; CTA r of C takes every C-th tile of ts sites.
+//
+// TwoBody's opposite-parity index is an involution (opp(opp(i)) = i), so the
+// sites pair up: a tile stages, for every site i of the tile with i <= opp(i),
+// the term of i, a_s = w_i psi1_s(i) and b_t = psi2_t(opp(i)), and (when
+// i < opp(i)) the term of j = opp(i), a_s = w_j psi1_s(j) and b_t = psi2_t(i).
+// Every term is summed exactly once and every orbital element is read once
+// (the gathered rows are the rows the pair's other term reads directly);
+// tiles whose sites all have i > opp(i) are skipped after reading opp.  When
+// `bad_opp` points at a nonzero word (the table is not an involution) the
+// tiles stage the term of every site instead: the plain gather.
+//
+// Thread (block, group) accumulates a PB x PB block of phi over the group's
+// slots of every tile, in R within a tile and in FP64 across tiles; the
 // groups are summed in shared memory and the cluster's CTAs in rank order
 // through distributed shared memory: the result does not depend on timing.
 constexpr int PAIR_THREADS = 256;
 constexpr int PAIR_MAXN = 32;
+constexpr int PB = 4;                // register block: PB x PB complex pair-matrix entries per thread
+constexpr int PAIR_E = PB * PB * 2;  // doubles per block
 
-// TS sites per tile: 128 FP32 / 64 FP64 complex values per staged orbital row
-// (1 KB), so that n = 32 needs 66 KB of shared memory and three CTAs fit an SM
 template <typename R>
 struct PairShape {
-  static constexpr int TS = sizeof(R) == 4 ? 128 : 64;
-  static constexpr int LD = TS + 1;  // padded row: rows s0 and s1 sit in different banks
-  static size_t smem(int n) {
-    const size_t tiles = 2 * (size_t)n * LD * sizeof(cplx<R>);
-    const size_t nb = (n + 1) / 2, red = nb * nb * 8 * sizeof(double);
-    return tiles > red ? tiles : red;
+  static int rows(int n) { return (n + PB - 1) / PB * PB; }  // staged rows, padded to whole blocks
+  // sites per tile: at most about 24 KB of staged rows per array
+  static int ts(int n) {
+    const int budget = (sizeof(R) == 4 ? 1536 : 768) / rows(n);
+    int t = 16;
+    while (t * 2 <= budget && t < 128) t *= 2;
+    return t;
   }
+  static int ld(int n) { return 2 * ts(n) + 1; }  // slots per staged row, padded: rows start in different banks
+  static size_t tiles(int n) {
+    const size_t t = 2 * (size_t)rows(n) * ld(n) * sizeof(cplx<R>);
+    const size_t nb = rows(n) / PB, red = nb * nb * PAIR_E * sizeof(double);
+    return ((t > red ? t : red) + 15) / 16 * 16;
+  }
+  static size_t smem(int n) { return tiles(n) + (size_t)PAIR_E * PAIR_THREADS * sizeof(double); }
 };
 
 template <typename R>
-__global__ void __launch_bounds__(PAIR_THREADS) pair_tile_kernel(const void* __restrict__ psi1,
-                                                                 const void* __restrict__ psi2, int n, long vol,
-                                                                 const double* __restrict__ w,
-                                                                 const int* __restrict__ opp,
-                                                                 double* __restrict__ phi) {
-  constexpr int LD = PairShape<R>::LD, PAIR_TS = PairShape<R>::TS;
+__global__ void __launch_bounds__(PAIR_THREADS, 2)
+    pair_tile_kernel(const void* __restrict__ psi1, const void* __restrict__ psi2, int n, long vol,
+                     const double* __restrict__ w, const int* __restrict__ opp, const int* __restrict__ bad_opp,
+                     int ts, size_t tiles_bytes, double* __restrict__ phi) {
   extern __shared__ __align__(16) unsigned char pair_smem[];
-  cplx<R>* A = reinterpret_cast<cplx<R>*>(pair_smem);  // [n][LD]: w_i psi1_s(i)
-  cplx<R>* B = A + (size_t)n * LD;                      // [n][LD]: psi2_t(opp(i))
+  const int LD = 2 * ts + 1;
+  const int nb = (n + PB - 1) / PB, rows = nb * PB;
+  cplx<R>* A = reinterpret_cast<cplx<R>*>(pair_smem);  // [rows][LD]: w psi1 of each slot's term
+  cplx<R>* B = A + (size_t)rows * LD;                   // [rows][LD]: psi2 at the term's partner site
+  double* accs = reinterpret_cast<double*>(pair_smem + tiles_bytes);  // [PAIR_E][threads]: FP64 sums
   cg::cluster_group cluster = cg::this_cluster();
   const int split = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
   const long conf = blockIdx.x / split;
-  const cplx<R>* a_base = reinterpret_cast<const cplx<R>*>(psi1) + (size_t)conf * n * vol;
-  const cplx<R>* b_base = reinterpret_cast<const cplx<R>*>(psi2) + (size_t)conf * n * vol;
-  const int nb = (n + 1) / 2;                 // 2-row blocks
-  const int nblk = nb * nb;                   // (s, t) block pairs
-  const int groups = PAIR_THREADS / nblk;     // >= 1 for n <= 32
+  const cplx<R>* p1 = reinterpret_cast<const cplx<R>*>(psi1) + (size_t)conf * n * vol;
+  const cplx<R>* p2 = reinterpret_cast<const cplx<R>*>(psi2) + (size_t)conf * n * vol;
+  const bool paired = !(bad_opp && *bad_opp);
+  // staging: thread -> (slot q of the tile, orbital lane)
+  const int q = threadIdx.x % ts, olane = threadIdx.x / ts, ostride = PAIR_THREADS / ts;
+  // accumulation: thread -> (PB x PB block, group)
+  const int nblk = nb * nb;
+  const int groups = PAIR_THREADS / nblk;  // >= 4 for n <= 32
   const int g = threadIdx.x % groups, blk = threadIdx.x / groups;
   const bool active = blk < nblk;
-  const int s0 = 2 * (active ? blk / nb : 0), t0 = 2 * (active ? blk % nb : 0);
-  const int s1 = s0 + 1 < n ? s0 + 1 : s0, t1 = t0 + 1 < n ? t0 + 1 : t0;
-  double acc[8];
+  const int abase = (active ? blk / nb : 0) * PB * LD, bbase = (active ? blk % nb : 0) * PB * LD;
+  for (int e = threadIdx.x; e < (rows - n) * LD; e += PAIR_THREADS) {  // the padding rows stay zero
+    A[n * LD + e] = cplx<R>{(R)0, (R)0};
+    B[n * LD + e] = cplx<R>{(R)0, (R)0};
+  }
 #pragma unroll
-  for (int k = 0; k < 8; ++k) acc[k] = 0.0;
-  const long ntiles = (vol + PAIR_TS - 1) / PAIR_TS;
+  for (int k = 0; k < PAIR_E; ++k) accs[k * PAIR_THREADS + threadIdx.x] = 0.0;
+  const long ntiles = (vol + ts - 1) / ts;
   for (long tile = rank; tile < ntiles; tile += split) {
-    const long i0 = tile * PAIR_TS;
-    const int ts = (int)(vol - i0 < PAIR_TS ? vol - i0 : PAIR_TS);
-    __syncthreads();  // the previous tile is consumed
-#pragma unroll 4
-    for (int e = threadIdx.x; e < n * PAIR_TS; e += PAIR_THREADS) {
-      const int o = e / PAIR_TS, q = e % PAIR_TS;
-      cplx<R> x{(R)0, (R)0}, y{(R)0, (R)0};
-      if (q < ts) {
-        const long i = i0 + q;
-        x = a_base[(size_t)o * vol + i];
-        const R wi = (R)__ldg(w + i);
-        x.re *= wi;
-        x.im *= wi;
-        y = b_base[(size_t)o * vol + __ldg(opp + i)];
+    const long i = tile * ts + q;
+    const bool valid = i < vol;
+    const long j = valid ? (long)__ldg(opp + i) : 0;
+    const bool take = valid && (!paired || i <= j);
+    const bool second = paired && valid && i < j;
+    // also the barrier after the previous tile's accumulation
+    if (!__syncthreads_or(take)) continue;
+    const R wi = take ? (R)__ldg(w + i) : (R)0, wj = second ? (R)__ldg(w + j) : (R)0;
+    for (int o = olane; o < n; o += ostride) {
+      const cplx<R>* r1 = p1 + (size_t)o * vol;
+      const cplx<R>* r2 = p2 + (size_t)o * vol;
+      cplx<R> a1{(R)0, (R)0}, b1{(R)0, (R)0}, a2{(R)0, (R)0}, b2{(R)0, (R)0};
+      if (take) {
+        a1 = r1[i];
+        b1 = r2[j];
       }
-      A[o * LD + q] = x;
-      B[o * LD + q] = y;
+      if (second) {
+        a2 = r1[j];
+        b2 = r2[i];
+      }
+      A[o * LD + q] = cplx<R>{a1.re * wi, a1.im * wi};
+      B[o * LD + q] = b1;
+      A[o * LD + ts + q] = cplx<R>{a2.re * wj, a2.im * wj};
+      B[o * LD + ts + q] = b2;
     }
     __syncthreads();
     if (active) {
-      // sum_i a_s(i) b_t(i) for the 2 x 2 block, complex, no conjugation
-      R r[8];
+      // sum over the slots of a_s b_t (complex, no conjugation), in R
+      R r[PB][PB][2];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) r[k] = (R)0;
-      for (int q = g; q < ts; q += groups) {
-        const cplx<R> a0 = A[s0 * LD + q], a1 = A[s1 * LD + q];
-        const cplx<R> b0 = B[t0 * LD + q], b1 = B[t1 * LD + q];
-        r[0] += a0.re * b0.re - a0.im * b0.im;
-        r[1] += a0.re * b0.im + a0.im * b0.re;
-        r[2] += a0.re * b1.re - a0.im * b1.im;
-        r[3] += a0.re * b1.im + a0.im * b1.re;
-        r[4] += a1.re * b0.re - a1.im * b0.im;
-        r[5] += a1.re * b0.im + a1.im * b0.re;
-        r[6] += a1.re * b1.re - a1.im * b1.im;
-        r[7] += a1.re * b1.im + a1.im * b1.re;
+      for (int a = 0; a < PB; ++a)
+#pragma unroll
+        for (int b = 0; b < PB; ++b) r[a][b][0] = r[a][b][1] = (R)0;
+      for (int slot = g; slot < 2 * ts; slot += groups) {
+        cplx<R> av[PB], bv[PB];
+#pragma unroll
+        for (int k = 0; k < PB; ++k) {
+          av[k] = A[abase + k * LD + slot];
+          bv[k] = B[bbase + k * LD + slot];
+        }
+#pragma unroll
+        for (int a = 0; a < PB; ++a)
+#pragma unroll
+          for (int b = 0; b < PB; ++b) {
+            r[a][b][0] += av[a].re * bv[b].re - av[a].im * bv[b].im;
+            r[a][b][1] += av[a].re * bv[b].im + av[a].im * bv[b].re;
+          }
       }
+      // the tile's sums into this thread's FP64 sums (shared memory)
 #pragma unroll
-      for (int k = 0; k < 8; ++k) acc[k] += (double)r[k];
+      for (int a = 0; a < PB; ++a)
+#pragma unroll
+        for (int b = 0; b < PB; ++b)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) accs[((a * PB + b) * 2 + c) * PAIR_THREADS + threadIdx.x] += (double)r[a][b][c];
     }
   }
-  // sum the groups of every block pair in shared memory (fixed order), then
-  // the cluster's CTAs in rank order
+  // sum the groups of every block (fixed order), then the cluster's CTAs in
+  // rank order
   __syncthreads();
-  double* red = reinterpret_cast<double*>(pair_smem);  // [nblk][8], group 0 first
-  for (int gg = 0; gg < groups; ++gg) {
-    if (active && g == gg)
-#pragma unroll
-      for (int k = 0; k < 8; ++k) red[blk * 8 + k] = (gg == 0 ? 0.0 : red[blk * 8 + k]) + acc[k];
-    __syncthreads();
+  double* red = reinterpret_cast<double*>(pair_smem);  // [nblk][PAIR_E], over the staged tiles
+  for (int e = threadIdx.x; e < nblk * PAIR_E; e += PAIR_THREADS) {
+    const int b = e / PAIR_E, k = e % PAIR_E;
+    double v = 0.0;
+    for (int gg = 0; gg < groups; ++gg) v += accs[k * PAIR_THREADS + b * groups + gg];
+    red[e] = v;
   }
   cluster.sync();  // every CTA's sums are in its shared memory
   if (rank == 0) {
-    for (int e = threadIdx.x; e < nblk * 8; e += PAIR_THREADS) {
+    for (int e = threadIdx.x; e < nblk * PAIR_E; e += PAIR_THREADS) {
       double v = 0.0;
       for (int r2 = 0; r2 < split; ++r2) v += cluster.map_shared_rank(red, r2)[e];
-      const int b = e >> 3, k = e & 7;
-      const int s = 2 * (b / nb) + ((k >> 2) & 1), t = 2 * (b % nb) + ((k >> 1) & 1);
+      const int b = e / PAIR_E, k = e % PAIR_E;
+      const int s = PB * (b / nb) + (k / 2) / PB, t = PB * (b % nb) + (k / 2) % PB;
       if (s < n && t < n) phi[2 * ((conf * n + s) * (long)n + t) + (k & 1)] = v;
     }
   }
   cluster.sync();  // peers keep their shared memory until rank 0 has read it
+}
+
+// *bad = 1 unless opp is an involution of [0, vol) (TwoBody's parity mirror is)
+__global__ void opp_involution_check_kernel(const int* __restrict__ opp, long vol, int* bad) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < vol; i += (long)gridDim.x * blockDim.x) {
+    const int j = opp[i];
+    if (j < 0 || j >= vol || opp[j] != i) *bad = 1;
+  }
 }
 
 // GeneralizedTwoBody::Run (src/two_body/noarch/two_body_run.C:45-75) batched:
@@ -670,19 +717,22 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
 
 template <typename R>
 static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf,
-                                     long vol, const double* w, const int* opp, double* phi) {
+                                     long vol, const double* w, const int* opp, const int* bad_opp, double* phi) {
+  const int ts = PairShape<R>::ts(n);
   const size_t smem = PairShape<R>::smem(n);
   static bool attr_set[16] = {false};
   if (!attr_set[ctx->device & 15]) {
+    size_t most = 0;
+    for (int m = 1; m <= PAIR_MAXN; ++m) most = PairShape<R>::smem(m) > most ? PairShape<R>::smem(m) : most;
     NRCPS_TRY(check_cuda(ctx, cudaFuncSetAttribute(pair_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)PairShape<R>::smem(PAIR_MAXN)),
+                                                   (int)most),
                          "pair_tile: smem attribute"));
     attr_set[ctx->device & 15] = true;
   }
-  // CTAs per configuration: enough CTAs for about eight per SM, at most 8
+  // CTAs per configuration: enough CTAs for about four per SM, at most 8
   // (a portable cluster) and no more than the tiles
-  const long ntiles = (vol + PairShape<R>::TS - 1) / PairShape<R>::TS;
-  int split = (int)((8L * ctx->sm_count + nconf - 1) / nconf);
+  const long ntiles = (vol + ts - 1) / ts;
+  int split = (int)((4L * ctx->sm_count + nconf - 1) / nconf);
   if (split > 8) split = 8;
   if (split > ntiles) split = (int)ntiles;
   if (split < 1) split = 1;
@@ -698,18 +748,29 @@ static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const
   cfg.stream = ctx->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, pair_tile_kernel<R>, psi1, psi2, n, vol, w, opp, phi);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, pair_tile_kernel<R>, psi1, psi2, n, vol, w, opp, bad_opp, ts,
+                                     PairShape<R>::tiles(n), phi);
   ctx->launches++;
   return check_cuda(ctx, e, "pair_tile_kernel launch");
 }
 
+// opp_checked: the caller has checked on the host that opp is an
+// involution of [0, vol); otherwise the device checks it before the tiles.
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
-                       const double* w, const int* opp, nrcps_precision prec, double* phi) {
+                       const double* w, const int* opp, nrcps_precision prec, double* phi, bool opp_checked) {
   long blocks = (long)nconf * n * n;
   if (blocks == 0) return NRCPS_OK;
   if (n <= PAIR_MAXN && ctx->pair_tile && (long)nconf * 8 < (1L << 31)) {
-    if (prec == NRCPS_F64) return launch_pair_tile<double>(ctx, psi1, psi2, n, nconf, vol, w, opp, phi);
-    return launch_pair_tile<float>(ctx, psi1, psi2, n, nconf, vol, w, opp, phi);
+    const int* bad = nullptr;
+    if (!opp_checked) {
+      NRCPS_TRY(check_cuda(ctx, cudaMemsetAsync(ctx->dev_pair_flag, 0, sizeof(int), ctx->stream), "pair flag"));
+      opp_involution_check_kernel<<<grid_for(vol, 256), 256, 0, ctx->stream>>>(opp, vol, ctx->dev_pair_flag);
+      ctx->launches++;
+      NRCPS_TRY(check_launch(ctx, "opp_involution_check_kernel"));
+      bad = ctx->dev_pair_flag;
+    }
+    if (prec == NRCPS_F64) return launch_pair_tile<double>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
+    return launch_pair_tile<float>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
   }
   if (prec == NRCPS_F64) pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
   else pair_kernel<float><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
@@ -762,7 +823,7 @@ extern "C" nrcps_status nrcps_pair_matrix(nrcps_context* ctx, const void* dev_ps
   NRCPS_REQUIRE(ctx, n >= 0 && nconf >= 0 && vol > 0, "nrcps_pair_matrix: bad arguments");
   if ((long)n * nconf == 0) return NRCPS_OK;
   NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_w && dev_opposite && dev_phi, "nrcps_pair_matrix: null pointer");
-  return pair_impl(ctx, dev_psi1, dev_psi2, n, nconf, vol, dev_w, dev_opposite, prec, dev_phi);
+  return pair_impl(ctx, dev_psi1, dev_psi2, n, nconf, vol, dev_w, dev_opposite, prec, dev_phi, false);
 }
 
 extern "C" nrcps_status nrcps_shifted_pair_matrix(nrcps_context* ctx, const void* dev_psi1, const void* dev_psi2,

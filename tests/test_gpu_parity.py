@@ -5,6 +5,7 @@ Tolerances: RNG and field integers bit-exact; FP64 propagation, overlaps and
 determinants within 1e-12 relative; FP32 propagation within 1e-5 relative on
 the correlators (the BASELINE target for the fast mode).
 """
+import ctypes
 import json
 import os
 
@@ -19,6 +20,7 @@ from conftest import GOLDEN
 pytestmark = pytest.mark.gpu
 
 nb = pytest.importorskip("nrcps_b200")
+from nrcps_b200 import _capi as C  # noqa: E402
 
 FP64_REL = 1e-12
 FP32_REL = 1e-5
@@ -225,6 +227,37 @@ def test_pair_matrix_tiles_match_oracle(ctx, n, dims, nconf):
                     assert max_norm_err(phi, r) < tol, (tile, dt)
             finally:
                 ctx.set_option("pair.tile", 1)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_pair_matrix_with_a_table_that_is_no_involution(ctx, precision):
+    """The tiled kernel pairs each site with its opposite (opp(opp(i)) = i,
+    as TwoBody's parity mirror); nrcps_pair_matrix checks that on the device
+    and, for any other table (here a random permutation), sums every site's
+    term through the plain gather: the same pair matrices as the oracle."""
+    rs = np.random.default_rng(21)
+    dims, n, nconf = (8, 8, 8), 10, 3
+    vol = int(np.prod(dims))
+    psi1 = rs.standard_normal((nconf, n, vol)) + 1j * rs.standard_normal((nconf, n, vol))
+    psi2 = rs.standard_normal((nconf, n, vol)) + 1j * rs.standard_normal((nconf, n, vol))
+    w = rs.uniform(0.0, 1.0, vol)
+    opp = rs.permutation(vol).astype(np.int32)
+    assert np.any(opp[opp] != np.arange(vol))
+    dt, tol = (torch.complex128, FP64_REL) if precision == "f64" else (torch.complex64, 1e-6)
+    p1 = torch.from_numpy(psi1).to(ctx.device).to(dt)
+    p2 = torch.from_numpy(psi2).to(ctx.device).to(dt)
+    out = torch.empty((nconf, n, n), dtype=torch.complex128, device=ctx.device)
+    wd = torch.from_numpy(w).to(ctx.device)
+    od = torch.from_numpy(opp).to(ctx.device)
+    ctx.check(nb.lib().nrcps_pair_matrix(ctx.handle, ctypes.c_void_p(p1.data_ptr()), ctypes.c_void_p(p2.data_ptr()),
+                                         n, nconf, vol, ctypes.c_void_p(wd.data_ptr()), ctypes.c_void_p(od.data_ptr()),
+                                         C.F64 if precision == "f64" else C.F32, ctypes.c_void_p(out.data_ptr())),
+              "pair_matrix")
+    got = out.cpu().numpy()
+    for c in range(nconf):
+        r = O.pair_matrix(p1[c].cpu().numpy().astype(np.complex128), p2[c].cpu().numpy().astype(np.complex128),
+                          w, opp)
+        assert max_norm_err(got[c], r) < tol
 
 
 def test_lu_cases_match_reference(golden, ctx):
@@ -569,7 +602,7 @@ def test_packed_variants_agree(ctx, kind, L, cluster):
     (5, 4, "f32", 8, 32), (6, 4, "f32", 8, 32), (8, 4, "f32", 8, 32), (7, 0, "f32", 8, 32), (7, 0, "f64", 16, 32),
     (9, 4, "f32", 8, 32), (10, 0, "f32", 8, 32), (11, 0, "f32", 8, 32), (12, 4, "f32", 8, 32),
     (11, 3, "f32", 16, 32), (11, 0, "f64", 16, 32), (11, 0, "f32", 2, 16), (11, 0, "f32", 4, 24),
-    (11, 0, "f64", 4, 24)])
+    (11, 0, "f64", 4, 24), (13, 0, "f32", 8, 32), (14, 4, "f32", 8, 32)])
 def test_same_arithmetic_variants_are_bit_identical(ctx, kind, ref_kind, precision, cluster, L):
     """Variants that differ only in how the slab reaches shared memory or how
     the exchange moves it (peer loads and stores, bulk copies, or peer loads

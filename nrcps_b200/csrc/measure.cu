@@ -31,8 +31,10 @@ __global__ void __launch_bounds__(256) overlap_kernel(const double* __restrict__
       for (int k = 0; k < 8; ++k) {
         if (s0 + k < ns) {
           double2 a = reinterpret_cast<const double2*>(src)[(long)(s0 + k) * vol + i];
-          ar[k] += a.x * qr + a.y * qi;
-          ai[k] += a.x * qi - a.y * qr;
+          ar[k] = fma(a.x, qr, ar[k]);  // two fused multiply-adds per component
+          ar[k] = fma(a.y, qi, ar[k]);
+          ai[k] = fma(a.x, qi, ai[k]);
+          ai[k] = fma(-a.y, qr, ai[k]);
         }
       }
     }
@@ -141,11 +143,12 @@ __global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1
 // through distributed shared memory: the result does not depend on timing.
 constexpr int PAIR_THREADS = 256;
 constexpr int PAIR_MAXN = 32;
-constexpr int PB = 4;                // register block: PB x PB complex pair-matrix entries per thread
-constexpr int PAIR_E = PB * PB * 2;  // doubles per block
+constexpr int PAIR_FLUSH = 4;  // FP32 sums: staged tiles summed in FP32 before one FP64 sum
 
-template <typename R>
+// PB x PB complex pair-matrix entries per thread (PB = 4 or 5)
+template <typename R, int PB>
 struct PairShape {
+  static constexpr int E = PB * PB * 2;  // doubles per block
   static int rows(int n) { return (n + PB - 1) / PB * PB; }  // staged rows, padded to whole blocks
   // sites per tile: at most about 24 KB of staged rows per array
   static int ts(int n) {
@@ -157,23 +160,26 @@ struct PairShape {
   static int ld(int n) { return 2 * ts(n) + 1; }  // slots per staged row, padded: rows start in different banks
   static size_t tiles(int n) {
     const size_t t = 2 * (size_t)rows(n) * ld(n) * sizeof(cplx<R>);
-    const size_t nb = rows(n) / PB, red = nb * nb * PAIR_E * sizeof(double);
+    const size_t nb = rows(n) / PB, red = nb * nb * E * sizeof(double);
     return ((t > red ? t : red) + 15) / 16 * 16;
   }
-  static size_t smem(int n) { return tiles(n) + (size_t)PAIR_E * PAIR_THREADS * sizeof(double); }
+  // FP32 sums are flushed into per-thread FP64 sums in shared memory
+  static size_t smem(int n) { return tiles(n) + (sizeof(R) == 4 ? (size_t)E * PAIR_THREADS * sizeof(double) : 0); }
 };
 
-template <typename R>
+template <typename R, int PB>
 __global__ void __launch_bounds__(PAIR_THREADS, 2)
     pair_tile_kernel(const void* __restrict__ psi1, const void* __restrict__ psi2, int n, long vol,
                      const double* __restrict__ w, const int* __restrict__ opp, const int* __restrict__ bad_opp,
                      int ts, size_t tiles_bytes, double* __restrict__ phi) {
+  constexpr int E = PairShape<R, PB>::E;
+  constexpr bool F32 = sizeof(R) == 4;
   extern __shared__ __align__(16) unsigned char pair_smem[];
   const int LD = 2 * ts + 1;
   const int nb = (n + PB - 1) / PB, rows = nb * PB;
   cplx<R>* A = reinterpret_cast<cplx<R>*>(pair_smem);  // [rows][LD]: w psi1 of each slot's term
   cplx<R>* B = A + (size_t)rows * LD;                   // [rows][LD]: psi2 at the term's partner site
-  double* accs = reinterpret_cast<double*>(pair_smem + tiles_bytes);  // [PAIR_E][threads]: FP64 sums
+  double* accs = reinterpret_cast<double*>(pair_smem + tiles_bytes);  // FP32 only: [E][threads] FP64 sums
   cg::cluster_group cluster = cg::this_cluster();
   const int split = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
   const long conf = blockIdx.x / split;
@@ -192,8 +198,18 @@ __global__ void __launch_bounds__(PAIR_THREADS, 2)
     A[n * LD + e] = cplx<R>{(R)0, (R)0};
     B[n * LD + e] = cplx<R>{(R)0, (R)0};
   }
+  if constexpr (F32) {
 #pragma unroll
-  for (int k = 0; k < PAIR_E; ++k) accs[k * PAIR_THREADS + threadIdx.x] = 0.0;
+    for (int k = 0; k < E; ++k) accs[k * PAIR_THREADS + threadIdx.x] = 0.0;
+  }
+  // running sums in R: over PAIR_FLUSH staged tiles for FP32 (then into the
+  // FP64 sums), over all tiles for FP64
+  R r[PB][PB][2];
+#pragma unroll
+  for (int a = 0; a < PB; ++a)
+#pragma unroll
+    for (int b = 0; b < PB; ++b) r[a][b][0] = r[a][b][1] = (R)0;
+  int staged = 0;
   const long ntiles = (vol + ts - 1) / ts;
   for (long tile = rank; tile < ntiles; tile += split) {
     const long i = tile * ts + q;
@@ -223,12 +239,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, 2)
     }
     __syncthreads();
     if (active) {
-      // sum over the slots of a_s b_t (complex, no conjugation), in R
-      R r[PB][PB][2];
-#pragma unroll
-      for (int a = 0; a < PB; ++a)
-#pragma unroll
-        for (int b = 0; b < PB; ++b) r[a][b][0] = r[a][b][1] = (R)0;
+      // sum over the slots of a_s b_t (complex, no conjugation): two fused
+      // multiply-adds per real component
       for (int slot = g; slot < 2 * ts; slot += groups) {
         cplx<R> av[PB], bv[PB];
 #pragma unroll
@@ -240,11 +252,30 @@ __global__ void __launch_bounds__(PAIR_THREADS, 2)
         for (int a = 0; a < PB; ++a)
 #pragma unroll
           for (int b = 0; b < PB; ++b) {
-            r[a][b][0] += av[a].re * bv[b].re - av[a].im * bv[b].im;
-            r[a][b][1] += av[a].re * bv[b].im + av[a].im * bv[b].re;
+            r[a][b][0] = fma(av[a].re, bv[b].re, r[a][b][0]);
+            r[a][b][0] = fma(-av[a].im, bv[b].im, r[a][b][0]);
+            r[a][b][1] = fma(av[a].re, bv[b].im, r[a][b][1]);
+            r[a][b][1] = fma(av[a].im, bv[b].re, r[a][b][1]);
           }
       }
-      // the tile's sums into this thread's FP64 sums (shared memory)
+      if constexpr (F32) {
+        if (++staged == PAIR_FLUSH) {
+          staged = 0;
+#pragma unroll
+          for (int a = 0; a < PB; ++a)
+#pragma unroll
+            for (int b = 0; b < PB; ++b)
+#pragma unroll
+              for (int c = 0; c < 2; ++c) {
+                accs[((a * PB + b) * 2 + c) * PAIR_THREADS + threadIdx.x] += (double)r[a][b][c];
+                r[a][b][c] = (R)0;
+              }
+        }
+      }
+    }
+  }
+  if constexpr (F32) {
+    if (active) {
 #pragma unroll
       for (int a = 0; a < PB; ++a)
 #pragma unroll
@@ -256,19 +287,36 @@ __global__ void __launch_bounds__(PAIR_THREADS, 2)
   // sum the groups of every block (fixed order), then the cluster's CTAs in
   // rank order
   __syncthreads();
-  double* red = reinterpret_cast<double*>(pair_smem);  // [nblk][PAIR_E], over the staged tiles
-  for (int e = threadIdx.x; e < nblk * PAIR_E; e += PAIR_THREADS) {
-    const int b = e / PAIR_E, k = e % PAIR_E;
-    double v = 0.0;
-    for (int gg = 0; gg < groups; ++gg) v += accs[k * PAIR_THREADS + b * groups + gg];
-    red[e] = v;
+  double* red = reinterpret_cast<double*>(pair_smem);  // [nblk][E], over the staged tiles
+  if constexpr (F32) {
+    for (int e = threadIdx.x; e < nblk * E; e += PAIR_THREADS) {
+      const int b = e / E, k = e % E;
+      double v = 0.0;
+      for (int gg = 0; gg < groups; ++gg) v += accs[k * PAIR_THREADS + b * groups + gg];
+      red[e] = v;
+    }
+  } else {
+    for (int gg = 0; gg < groups; ++gg) {
+      if (active && g == gg) {
+#pragma unroll
+        for (int a = 0; a < PB; ++a)
+#pragma unroll
+          for (int b = 0; b < PB; ++b)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              const int e = blk * E + (a * PB + b) * 2 + c;
+              red[e] = (gg == 0 ? 0.0 : red[e]) + (double)r[a][b][c];
+            }
+      }
+      __syncthreads();
+    }
   }
   cluster.sync();  // every CTA's sums are in its shared memory
   if (rank == 0) {
-    for (int e = threadIdx.x; e < nblk * PAIR_E; e += PAIR_THREADS) {
+    for (int e = threadIdx.x; e < nblk * E; e += PAIR_THREADS) {
       double v = 0.0;
       for (int r2 = 0; r2 < split; ++r2) v += cluster.map_shared_rank(red, r2)[e];
-      const int b = e / PAIR_E, k = e % PAIR_E;
+      const int b = e / E, k = e % E;
       const int s = PB * (b / nb) + (k / 2) / PB, t = PB * (b % nb) + (k / 2) % PB;
       if (s < n && t < n) phi[2 * ((conf * n + s) * (long)n + t) + (k & 1)] = v;
     }
@@ -344,8 +392,10 @@ __global__ void __launch_bounds__(256) inner_ptrs_kernel(const double* const* __
   double re = 0.0, im = 0.0;
   for (long i = threadIdx.x; i < vol; i += blockDim.x) {
     double2 x = a[i], y = b[i];
-    re += x.x * y.x + x.y * y.y;
-    im += x.x * y.y - x.y * y.x;
+    re = fma(x.x, y.x, re);
+    re = fma(x.y, y.y, re);
+    im = fma(x.x, y.y, im);
+    im = fma(-x.y, y.x, im);
   }
   __shared__ double red[2][8];
   for (int o = 16; o > 0; o >>= 1) {
@@ -715,17 +765,18 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
   return check_launch(ctx, "gather_kernel");
 }
 
-template <typename R>
+template <typename R, int PB>
 static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf,
                                      long vol, const double* w, const int* opp, const int* bad_opp, double* phi) {
-  const int ts = PairShape<R>::ts(n);
-  const size_t smem = PairShape<R>::smem(n);
+  using Sh = PairShape<R, PB>;
+  const int ts = Sh::ts(n);
+  const size_t smem = Sh::smem(n);
   static bool attr_set[16] = {false};
   if (!attr_set[ctx->device & 15]) {
     size_t most = 0;
-    for (int m = 1; m <= PAIR_MAXN; ++m) most = PairShape<R>::smem(m) > most ? PairShape<R>::smem(m) : most;
-    NRCPS_TRY(check_cuda(ctx, cudaFuncSetAttribute(pair_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)most),
+    for (int m = 1; m <= PAIR_MAXN; ++m) most = Sh::smem(m) > most ? Sh::smem(m) : most;
+    NRCPS_TRY(check_cuda(ctx, cudaFuncSetAttribute(pair_tile_kernel<R, PB>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most),
                          "pair_tile: smem attribute"));
     attr_set[ctx->device & 15] = true;
   }
@@ -748,8 +799,8 @@ static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const
   cfg.stream = ctx->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, pair_tile_kernel<R>, psi1, psi2, n, vol, w, opp, bad_opp, ts,
-                                     PairShape<R>::tiles(n), phi);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, pair_tile_kernel<R, PB>, psi1, psi2, n, vol, w, opp, bad_opp, ts,
+                                     Sh::tiles(n), phi);
   ctx->launches++;
   return check_cuda(ctx, e, "pair_tile_kernel launch");
 }
@@ -769,8 +820,11 @@ nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, i
       NRCPS_TRY(check_launch(ctx, "opp_involution_check_kernel"));
       bad = ctx->dev_pair_flag;
     }
-    if (prec == NRCPS_F64) return launch_pair_tile<double>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
-    return launch_pair_tile<float>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
+    if (prec == NRCPS_F64) return launch_pair_tile<double, 4>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
+    // FP32: the block edge (4 or 5) that pads n the least
+    const int p4 = (n + 3) / 4 * 4, p5 = (n + 4) / 5 * 5;
+    if (p5 < p4) return launch_pair_tile<float, 5>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
+    return launch_pair_tile<float, 4>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
   }
   if (prec == NRCPS_F64) pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
   else pair_kernel<float><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);

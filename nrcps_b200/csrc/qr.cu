@@ -95,15 +95,23 @@ __global__ void __launch_bounds__(256) gram_tile_kernel(const void* __restrict__
       for (int q = grp; q < GT; q += 4) {
         const cplx<R> a0 = tile[i0 * (GT + 1) + q], a1 = tile[i1 * (GT + 1) + q];
         const cplx<R> b0 = tile[j0 * (GT + 1) + q], b1 = tile[j1 * (GT + 1) + q];
-        // conj(a) b
-        s[0] += a0.re * b0.re + a0.im * b0.im;
-        s[1] += a0.re * b0.im - a0.im * b0.re;
-        s[2] += a0.re * b1.re + a0.im * b1.im;
-        s[3] += a0.re * b1.im - a0.im * b1.re;
-        s[4] += a1.re * b0.re + a1.im * b0.im;
-        s[5] += a1.re * b0.im - a1.im * b0.re;
-        s[6] += a1.re * b1.re + a1.im * b1.im;
-        s[7] += a1.re * b1.im - a1.im * b1.re;
+        // conj(a) b: two fused multiply-adds per component
+        s[0] = fma(a0.re, b0.re, s[0]);
+        s[0] = fma(a0.im, b0.im, s[0]);
+        s[1] = fma(a0.re, b0.im, s[1]);
+        s[1] = fma(-a0.im, b0.re, s[1]);
+        s[2] = fma(a0.re, b1.re, s[2]);
+        s[2] = fma(a0.im, b1.im, s[2]);
+        s[3] = fma(a0.re, b1.im, s[3]);
+        s[3] = fma(-a0.im, b1.re, s[3]);
+        s[4] = fma(a1.re, b0.re, s[4]);
+        s[4] = fma(a1.im, b0.im, s[4]);
+        s[5] = fma(a1.re, b0.im, s[5]);
+        s[5] = fma(-a1.im, b0.re, s[5]);
+        s[6] = fma(a1.re, b1.re, s[6]);
+        s[6] = fma(a1.im, b1.im, s[6]);
+        s[7] = fma(a1.re, b1.im, s[7]);
+        s[7] = fma(-a1.im, b1.re, s[7]);
       }
 #pragma unroll
       for (int k = 0; k < 8; ++k) acc[b][k] += (double)s[k];
@@ -370,8 +378,10 @@ __global__ void __launch_bounds__(256) apply_rinv_kernel(void* __restrict__ psi,
 #pragma unroll
       for (int i = 0; i <= t; ++i) {
         const R ar = rs[2 * (i * N + t)], ai = rs[2 * (i * N + t) + 1];
-        sr += xr[i] * ar - xi[i] * ai;
-        si += xr[i] * ai + xi[i] * ar;
+        sr = fma(xr[i], ar, sr);
+        sr = fma(-xi[i], ai, sr);
+        si = fma(xr[i], ai, si);
+        si = fma(xi[i], ar, si);
       }
       base[(size_t)t * vol] = cplx<R>{(R)sr, (R)si};
     }

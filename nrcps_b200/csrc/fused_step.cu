@@ -256,7 +256,11 @@ struct PullShape {
   static constexpr int THREADS = Base::THREADS;
   static constexpr size_t SMEM = STAGED ? Base::SMEM : sizeof(cplx<R>) * (size_t)Base::WORK + 32;
   static constexpr int FIT = (int)(228 * 1024 / (SMEM + 1024));
-  static constexpr int MIN_BLOCKS = STAGED ? Base::MIN_BLOCKS : (FIT > 4 ? 4 : (FIT < 1 ? 1 : FIT));
+  // L >= 48: a pencil alone takes 2 L registers, so leave each thread 168
+  static constexpr int WARP_THREADS = (THREADS + 31) / 32 * 32;
+  static constexpr int REG_FIT = L >= 48 ? 65536 / (WARP_THREADS * 168) : 4;
+  static constexpr int CAP = REG_FIT < 4 ? REG_FIT : 4;
+  static constexpr int MIN_BLOCKS = STAGED ? Base::MIN_BLOCKS : (FIT > CAP ? CAP : (FIT < 1 ? 1 : FIT));
 };
 
 template <typename R, int L, int C, bool PK = false, bool STAGED = true>
@@ -1416,6 +1420,9 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 32, 8, 0, launch_fused<float, 32, 8>},
     {NRCPS_F32, 32, 8, 2, launch_fused<float, 32, 8, 2>},
     {NRCPS_F32, 32, 8, 1, launch_fused<float, 32, 8, 1>},
+    {NRCPS_F32, 48, 12, 11, launch_fused<float, 48, 12, 11>},
+    {NRCPS_F32, 48, 12, 7, launch_fused<float, 48, 12, 7>},
+    {NRCPS_F32, 48, 12, 3, launch_fused<float, 48, 12, 3>},
     {NRCPS_F32, 48, 16, 4, launch_fused<float, 48, 16, 4>},
     {NRCPS_F32, 48, 16, 0, launch_fused<float, 48, 16>},
     {NRCPS_F32, 48, 16, 3, launch_fused<float, 48, 16, 3>},

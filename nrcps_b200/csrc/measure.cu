@@ -145,14 +145,15 @@ constexpr int PAIR_THREADS = 256;
 constexpr int PAIR_MAXN = 32;
 constexpr int PAIR_FLUSH = 4;  // FP32 sums: staged tiles summed in FP32 before one FP64 sum
 
-// PB x PB complex pair-matrix entries per thread (PB = 4 or 5)
+// PB x PB complex pair-matrix entries per thread
 template <typename R, int PB>
 struct PairShape {
   static constexpr int E = PB * PB * 2;  // doubles per block
   static int rows(int n) { return (n + PB - 1) / PB * PB; }  // staged rows, padded to whole blocks
-  // sites per tile: at most about 24 KB of staged rows per array
+  // sites per tile: at most about 12 KB of staged rows per array, so that
+  // with the FP32 path's FP64 sums (64 KB) two CTAs fit an SM
   static int ts(int n) {
-    const int budget = (sizeof(R) == 4 ? 1536 : 768) / rows(n);
+    const int budget = 768 / rows(n);
     int t = 16;
     while (t * 2 <= budget && t < 128) t *= 2;
     return t;
@@ -220,6 +221,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 2)
     // also the barrier after the previous tile's accumulation
     if (!__syncthreads_or(take)) continue;
     const R wi = take ? (R)__ldg(w + i) : (R)0, wj = second ? (R)__ldg(w + j) : (R)0;
+#pragma unroll 4
     for (int o = olane; o < n; o += ostride) {
       const cplx<R>* r1 = p1 + (size_t)o * vol;
       const cplx<R>* r2 = p2 + (size_t)o * vol;
@@ -821,9 +823,6 @@ nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, i
       bad = ctx->dev_pair_flag;
     }
     if (prec == NRCPS_F64) return launch_pair_tile<double, 4>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
-    // FP32: the block edge (4 or 5) that pads n the least
-    const int p4 = (n + 3) / 4 * 4, p5 = (n + 4) / 5 * 5;
-    if (p5 < p4) return launch_pair_tile<float, 5>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
     return launch_pair_tile<float, 4>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
   }
   if (prec == NRCPS_F64) pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);

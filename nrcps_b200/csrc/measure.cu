@@ -137,50 +137,43 @@ __global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1
 // `bad_opp` points at a nonzero word (the table is not an involution) the
 // tiles stage the term of every site instead: the plain gather.
 //
-// Thread (block, group) accumulates a PB x PB block of phi over the group's
+// Thread (block, group) accumulates a 2 x 2 block of phi over the group's
 // slots of every tile, in R within a tile and in FP64 across tiles; the
 // groups are summed in shared memory and the cluster's CTAs in rank order
 // through distributed shared memory: the result does not depend on timing.
 constexpr int PAIR_THREADS = 256;
 constexpr int PAIR_MAXN = 32;
-constexpr int PAIR_FLUSH = 4;  // FP32 sums: staged tiles summed in FP32 before one FP64 sum
+constexpr int PB = 2;                // register block: PB x PB complex pair-matrix entries per thread
+constexpr int PAIR_E = PB * PB * 2;  // doubles per block
 
-// PB x PB complex pair-matrix entries per thread
-template <typename R, int PB>
+template <typename R>
 struct PairShape {
-  static constexpr int E = PB * PB * 2;  // doubles per block
   static int rows(int n) { return (n + PB - 1) / PB * PB; }  // staged rows, padded to whole blocks
-  // sites per tile: at most about 12 KB of staged rows per array, so that
-  // with the FP32 path's FP64 sums (64 KB) two CTAs fit an SM
+  // sites per tile: at most about 20 KB of staged rows per array (four CTAs per SM)
   static int ts(int n) {
-    const int budget = 768 / rows(n);
+    const int budget = (sizeof(R) == 4 ? 1280 : 640) / rows(n);
     int t = 16;
     while (t * 2 <= budget && t < 128) t *= 2;
     return t;
   }
   static int ld(int n) { return 2 * ts(n) + 1; }  // slots per staged row, padded: rows start in different banks
-  static size_t tiles(int n) {
+  static size_t smem(int n) {
     const size_t t = 2 * (size_t)rows(n) * ld(n) * sizeof(cplx<R>);
-    const size_t nb = rows(n) / PB, red = nb * nb * E * sizeof(double);
-    return ((t > red ? t : red) + 15) / 16 * 16;
+    const size_t nb = rows(n) / PB, red = nb * nb * PAIR_E * sizeof(double);
+    return t > red ? t : red;
   }
-  // FP32 sums are flushed into per-thread FP64 sums in shared memory
-  static size_t smem(int n) { return tiles(n) + (sizeof(R) == 4 ? (size_t)E * PAIR_THREADS * sizeof(double) : 0); }
 };
 
-template <typename R, int PB>
-__global__ void __launch_bounds__(PAIR_THREADS, 2)
+template <typename R>
+__global__ void __launch_bounds__(PAIR_THREADS, 4)
     pair_tile_kernel(const void* __restrict__ psi1, const void* __restrict__ psi2, int n, long vol,
                      const double* __restrict__ w, const int* __restrict__ opp, const int* __restrict__ bad_opp,
-                     int ts, size_t tiles_bytes, double* __restrict__ phi) {
-  constexpr int E = PairShape<R, PB>::E;
-  constexpr bool F32 = sizeof(R) == 4;
+                     int ts, double* __restrict__ phi) {
   extern __shared__ __align__(16) unsigned char pair_smem[];
   const int LD = 2 * ts + 1;
   const int nb = (n + PB - 1) / PB, rows = nb * PB;
   cplx<R>* A = reinterpret_cast<cplx<R>*>(pair_smem);  // [rows][LD]: w psi1 of each slot's term
   cplx<R>* B = A + (size_t)rows * LD;                   // [rows][LD]: psi2 at the term's partner site
-  double* accs = reinterpret_cast<double*>(pair_smem + tiles_bytes);  // FP32 only: [E][threads] FP64 sums
   cg::cluster_group cluster = cg::this_cluster();
   const int split = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
   const long conf = blockIdx.x / split;
@@ -191,26 +184,19 @@ __global__ void __launch_bounds__(PAIR_THREADS, 2)
   const int q = threadIdx.x % ts, olane = threadIdx.x / ts, ostride = PAIR_THREADS / ts;
   // accumulation: thread -> (PB x PB block, group)
   const int nblk = nb * nb;
-  const int groups = PAIR_THREADS / nblk;  // >= 4 for n <= 32
+  const int groups = PAIR_THREADS / nblk;  // >= 1 for n <= 32
   const int g = threadIdx.x % groups, blk = threadIdx.x / groups;
   const bool active = blk < nblk;
   const int abase = (active ? blk / nb : 0) * PB * LD, bbase = (active ? blk % nb : 0) * PB * LD;
-  for (int e = threadIdx.x; e < (rows - n) * LD; e += PAIR_THREADS) {  // the padding rows stay zero
+  for (int e = threadIdx.x; e < (rows - n) * LD; e += PAIR_THREADS) {  // the padding row stays zero
     A[n * LD + e] = cplx<R>{(R)0, (R)0};
     B[n * LD + e] = cplx<R>{(R)0, (R)0};
   }
-  if constexpr (F32) {
-#pragma unroll
-    for (int k = 0; k < E; ++k) accs[k * PAIR_THREADS + threadIdx.x] = 0.0;
-  }
-  // running sums in R: over PAIR_FLUSH staged tiles for FP32 (then into the
-  // FP64 sums), over all tiles for FP64
-  R r[PB][PB][2];
+  double acc[PB][PB][2];
 #pragma unroll
   for (int a = 0; a < PB; ++a)
 #pragma unroll
-    for (int b = 0; b < PB; ++b) r[a][b][0] = r[a][b][1] = (R)0;
-  int staged = 0;
+    for (int b = 0; b < PB; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
   const long ntiles = (vol + ts - 1) / ts;
   for (long tile = rank; tile < ntiles; tile += split) {
     const long i = tile * ts + q;
@@ -241,8 +227,13 @@ __global__ void __launch_bounds__(PAIR_THREADS, 2)
     }
     __syncthreads();
     if (active) {
-      // sum over the slots of a_s b_t (complex, no conjugation): two fused
-      // multiply-adds per real component
+      // sum over the slots of a_s b_t (complex, no conjugation) in R: two
+      // fused multiply-adds per real component; then into the FP64 sums
+      R r[PB][PB][2];
+#pragma unroll
+      for (int a = 0; a < PB; ++a)
+#pragma unroll
+        for (int b = 0; b < PB; ++b) r[a][b][0] = r[a][b][1] = (R)0;
       for (int slot = g; slot < 2 * ts; slot += groups) {
         cplx<R> av[PB], bv[PB];
 #pragma unroll
@@ -260,65 +251,39 @@ __global__ void __launch_bounds__(PAIR_THREADS, 2)
             r[a][b][1] = fma(av[a].im, bv[b].re, r[a][b][1]);
           }
       }
-      if constexpr (F32) {
-        if (++staged == PAIR_FLUSH) {
-          staged = 0;
 #pragma unroll
-          for (int a = 0; a < PB; ++a)
+      for (int a = 0; a < PB; ++a)
 #pragma unroll
-            for (int b = 0; b < PB; ++b)
-#pragma unroll
-              for (int c = 0; c < 2; ++c) {
-                accs[((a * PB + b) * 2 + c) * PAIR_THREADS + threadIdx.x] += (double)r[a][b][c];
-                r[a][b][c] = (R)0;
-              }
+        for (int b = 0; b < PB; ++b) {
+          acc[a][b][0] += (double)r[a][b][0];
+          acc[a][b][1] += (double)r[a][b][1];
         }
-      }
     }
   }
-  if constexpr (F32) {
-    if (active) {
+  // sum the groups of every block in shared memory (fixed order), then the
+  // cluster's CTAs in rank order
+  __syncthreads();
+  double* red = reinterpret_cast<double*>(pair_smem);  // [nblk][PAIR_E], over the staged tiles
+  for (int gg = 0; gg < groups; ++gg) {
+    if (active && g == gg) {
 #pragma unroll
       for (int a = 0; a < PB; ++a)
 #pragma unroll
         for (int b = 0; b < PB; ++b)
 #pragma unroll
-          for (int c = 0; c < 2; ++c) accs[((a * PB + b) * 2 + c) * PAIR_THREADS + threadIdx.x] += (double)r[a][b][c];
+          for (int c = 0; c < 2; ++c) {
+            const int e = blk * PAIR_E + (a * PB + b) * 2 + c;
+            red[e] = (gg == 0 ? 0.0 : red[e]) + acc[a][b][c];
+          }
     }
-  }
-  // sum the groups of every block (fixed order), then the cluster's CTAs in
-  // rank order
-  __syncthreads();
-  double* red = reinterpret_cast<double*>(pair_smem);  // [nblk][E], over the staged tiles
-  if constexpr (F32) {
-    for (int e = threadIdx.x; e < nblk * E; e += PAIR_THREADS) {
-      const int b = e / E, k = e % E;
-      double v = 0.0;
-      for (int gg = 0; gg < groups; ++gg) v += accs[k * PAIR_THREADS + b * groups + gg];
-      red[e] = v;
-    }
-  } else {
-    for (int gg = 0; gg < groups; ++gg) {
-      if (active && g == gg) {
-#pragma unroll
-        for (int a = 0; a < PB; ++a)
-#pragma unroll
-          for (int b = 0; b < PB; ++b)
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-              const int e = blk * E + (a * PB + b) * 2 + c;
-              red[e] = (gg == 0 ? 0.0 : red[e]) + (double)r[a][b][c];
-            }
-      }
-      __syncthreads();
-    }
+    __syncthreads();
   }
   cluster.sync();  // every CTA's sums are in its shared memory
   if (rank == 0) {
-    for (int e = threadIdx.x; e < nblk * E; e += PAIR_THREADS) {
+    for (int e = threadIdx.x; e < nblk * PAIR_E; e += PAIR_THREADS) {
       double v = 0.0;
       for (int r2 = 0; r2 < split; ++r2) v += cluster.map_shared_rank(red, r2)[e];
-      const int b = e / E, k = e % E;
+      const int b = e / PAIR_E, k = e % PAIR_E;
       const int s = PB * (b / nb) + (k / 2) / PB, t = PB * (b % nb) + (k / 2) % PB;
       if (s < n && t < n) phi[2 * ((conf * n + s) * (long)n + t) + (k & 1)] = v;
     }
@@ -767,18 +732,18 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
   return check_launch(ctx, "gather_kernel");
 }
 
-template <typename R, int PB>
+template <typename R>
 static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf,
                                      long vol, const double* w, const int* opp, const int* bad_opp, double* phi) {
-  using Sh = PairShape<R, PB>;
+  using Sh = PairShape<R>;
   const int ts = Sh::ts(n);
   const size_t smem = Sh::smem(n);
   static bool attr_set[16] = {false};
   if (!attr_set[ctx->device & 15]) {
     size_t most = 0;
     for (int m = 1; m <= PAIR_MAXN; ++m) most = Sh::smem(m) > most ? Sh::smem(m) : most;
-    NRCPS_TRY(check_cuda(ctx, cudaFuncSetAttribute(pair_tile_kernel<R, PB>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most),
+    NRCPS_TRY(check_cuda(ctx, cudaFuncSetAttribute(pair_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)most),
                          "pair_tile: smem attribute"));
     attr_set[ctx->device & 15] = true;
   }
@@ -801,8 +766,7 @@ static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const
   cfg.stream = ctx->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, pair_tile_kernel<R, PB>, psi1, psi2, n, vol, w, opp, bad_opp, ts,
-                                     Sh::tiles(n), phi);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, pair_tile_kernel<R>, psi1, psi2, n, vol, w, opp, bad_opp, ts, phi);
   ctx->launches++;
   return check_cuda(ctx, e, "pair_tile_kernel launch");
 }
@@ -822,8 +786,8 @@ nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, i
       NRCPS_TRY(check_launch(ctx, "opp_involution_check_kernel"));
       bad = ctx->dev_pair_flag;
     }
-    if (prec == NRCPS_F64) return launch_pair_tile<double, 4>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
-    return launch_pair_tile<float, 4>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
+    if (prec == NRCPS_F64) return launch_pair_tile<double>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
+    return launch_pair_tile<float>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
   }
   if (prec == NRCPS_F64) pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
   else pair_kernel<float><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);

@@ -182,11 +182,12 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
   const bool paired = !(bad_opp && *bad_opp);
   // staging: thread -> (slot q of the tile, orbital lane)
   const int q = threadIdx.x % ts, olane = threadIdx.x / ts, ostride = PAIR_THREADS / ts;
-  // accumulation: thread -> (PB x PB block, group)
+  // accumulation: thread -> (PB x PB block, group), blocks fastest: the
+  // lanes of a warp read one slot of at most 2 nb rows, in distinct banks
   const int nblk = nb * nb;
   const int groups = PAIR_THREADS / nblk;  // >= 1 for n <= 32
-  const int g = threadIdx.x % groups, blk = threadIdx.x / groups;
-  const bool active = blk < nblk;
+  const int g = threadIdx.x / nblk, blk = threadIdx.x % nblk;
+  const bool active = g < groups;
   const int abase = (active ? blk / nb : 0) * PB * LD, bbase = (active ? blk % nb : 0) * PB * LD;
   for (int e = threadIdx.x; e < (rows - n) * LD; e += PAIR_THREADS) {  // the padding row stays zero
     A[n * LD + e] = cplx<R>{(R)0, (R)0};

@@ -103,9 +103,7 @@ const char *nrcps_version(void);
  *                      11, 12: kinds 7, 8 with the x pass written back by
  *                      st.async onto the owner CTA's mbarrier (one cluster
  *                      barrier per orbital); 13, 14: kinds 11, 12 compiled
- *                      for five CTAs per SM (FP32, L = 32); 15: kind 11
- *                      with each thread's pencil of k(p) in tensor memory
- *                      (FP32, L = 32 and 48);
+ *                      for five CTAs per SM (FP32, L = 32);
  *   "overlap.tc"       1 (default): dense-source overlaps of FP32 orbitals
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the

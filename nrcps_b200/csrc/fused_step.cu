@@ -1083,74 +1083,15 @@ __device__ __forceinline__ void st_async(uint32_t addr, cplx<R> v, uint32_t bar)
                  : "memory");
 }
 
-// k(p) in tensor memory (TK): every thread of passes 1 and 5 applies the
-// kinetic factor to one pencil along y, (xl, z) fixed, and a CTA keeps the
-// same slab for the whole persistent kernel.  So each thread stores the L
-// (hi, lo) pairs of its pencil once, in its own TMEM lane (warp w owns lanes
-// 32 (w % 4) .. + 31; warps 4-7 use a second column block), and reads them
-// back with tcgen05.ld instead of L2 loads.  Columns 2y, 2y + 1 hold hi, lo.
-template <int L, int THREADS>
-struct KinTmem {
-  static constexpr int WARPS = (THREADS + 31) / 32;
-  static constexpr int BLOCKS = (WARPS + 3) / 4;  // column blocks
-  static constexpr int NEED = BLOCKS * 2 * L;
-  static constexpr int COLS = NEED <= 32 ? 32 : NEED <= 64 ? 64 : NEED <= 128 ? 128 : NEED <= 256 ? 256 : 512;
-  static_assert(L % 8 == 0, "k(p) moves in chunks of 8 sites");
-};
-
-// Shared memory of the TK kernel: at least enough that no more CTAs fit an SM
-// than tensor memory holds columns for (every resident CTA gets its columns
-// at once: an allocation never waits on a CTA that itself waits for a
-// cluster peer)
-template <typename R, int L, int C>
-struct TkShape {
-  static constexpr size_t BASE = PullShape<R, L, C, false>::SMEM;
-  static constexpr int MAX_CTAS = 512 / KinTmem<L, FusedShape<R, L, C>::THREADS>::COLS;
-  static constexpr size_t FLOOR = (233472 / (MAX_CTAS + 1) - 1024 + 16) / 16 * 16;
-  static constexpr size_t SMEM = BASE > FLOOR ? BASE : FLOOR;
-  static_assert((int)(233472 / (SMEM + 1024)) <= MAX_CTAS, "TMEM of the resident CTAs");
-};
-
-__device__ __forceinline__ uint32_t kin_taddr(uint32_t base, int tid, int L) {
-  const int w = tid >> 5;
-  return base + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)((w >> 2) * 2 * L);
-}
-
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15, %16};" ::"r"(taddr),
-      "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]),
-      "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
-      : "memory");
-}
-
-// 16 columns (8 sites' hi, lo) of this thread's lane; waits for them
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-template <typename R, int L, int C, bool PK = false, int MINB = 0, bool TK = false>
+template <typename R, int L, int C, bool PK = false, int MINB = 0>
 __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
                                   MINB > 0 ? MINB : PullShape<R, L, C, false>::MIN_BLOCKS)
     fused_step_async_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
   static_assert(C > 1, "the write-back goes to cluster peers");
-  static_assert(!TK || sizeof(R) == 4, "k(p) in tensor memory: FP32 (hi, lo) pairs");
   constexpr int S = Sh::S, LP = Sh::LP, REGION = Sh::REGION;
   constexpr int V = L * L * L;
   constexpr uint32_t SLAB_BYTES = (uint32_t)(Sh::STAGE * sizeof(cplx<R>));  // bytes written back into a CTA
-  using KT = KinTmem<L, Sh::THREADS>;
-  static_assert(!TK || TkShape<R, L, C>::MAX_CTAS >= 1, "TMEM of one CTA");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   cplx<R>* sm = reinterpret_cast<cplx<R>*>(smem_raw);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Sh::WORK);  // write-backs into this CTA's slab
@@ -1162,7 +1103,6 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
   // with parity p and p + 1 and read only after the latter: every CTA sees
   // the same words and leaves at the same barrier.
   int* abort_words = reinterpret_cast<int*>(bar + 2);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 3);  // TK: the TMEM columns' base address
 
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
@@ -1174,35 +1114,6 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
   auto slab = [&](long orb) {
     return reinterpret_cast<const cplx<R>*>(f.psi) + (size_t)orb * V + (size_t)c * S * L * L;
   };
-
-  uint32_t kin_t = 0;  // TK: this thread's TMEM lane and column block
-  if constexpr (TK) {
-    if (tid < 32) {
-      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                   "r"(KT::COLS)
-                   : "memory");
-      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    kin_t = kin_taddr(*tmem_slot, tid, L);
-    // this thread's pencil of k(p): sites (c S + xl, y, z), y = 0 .. L-1
-    const int site0 = (c * S + tid / L) * L * L + tid % L;
-#pragma unroll
-    for (int y0 = 0; y0 < L; y0 += 8) {
-      float v[16];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const float2 t = __ldg(f.kin_f + site0 + (y0 + k) * L);
-        v[2 * k] = t.x;
-        v[2 * k + 1] = t.y;
-      }
-      tmem_st16(kin_t + 2 * y0, v);
-    }
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  }
 
   const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
   const bool z2_pos = (f.field_mode == 1) && (f.zpos != nullptr) && ((L * L) % 32 == 0);
@@ -1218,7 +1129,6 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
     mbar_init(idle);
   }
   cluster.sync();  // mbarriers and abort words are set up before any peer uses them
-  if constexpr (TK) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   // this CTA's region c and abort words; mapa turns them into every peer's copy
   const uint32_t my_region = smem_u32(sm + c * REGION);
   const uint32_t my_words = smem_u32(abort_words);
@@ -1240,33 +1150,17 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
       const int z = tid % L, xl = tid / L;
       const int site0 = (c * S + xl) * L * L + z;
       const cplx<R>* src = slab(orb);
-      if constexpr (TK) {
 #pragma unroll
-        for (int y = 0; y < L; ++y) {
-          const float2 t = __ldcg(reinterpret_cast<const float2*>(src) + (xl * L + y) * L + z);
-          x[y] = cplx<R>{t.x, t.y};
+      for (int y = 0; y < L; ++y) {
+        cplx<R> v;
+        if constexpr (sizeof(R) == 4) {
+          float2 t = __ldcg(reinterpret_cast<const float2*>(src) + (xl * L + y) * L + z);
+          v = cplx<R>{t.x, t.y};
+        } else {
+          double2 t = __ldcg(reinterpret_cast<const double2*>(src) + (xl * L + y) * L + z);
+          v = cplx<R>{t.x, t.y};
         }
-#pragma unroll
-        for (int y0 = 0; y0 < L; y0 += 8) {
-          float k[16];
-          tmem_ld16(kin_t + 2 * y0, k);
-#pragma unroll
-          for (int j = 0; j < 8; ++j) x[y0 + j] = scale_w<R, PK>(x[y0 + j], k[2 * j], k[2 * j + 1]);
-        }
-        (void)site0;
-      } else {
-#pragma unroll
-        for (int y = 0; y < L; ++y) {
-          cplx<R> v;
-          if constexpr (sizeof(R) == 4) {
-            float2 t = __ldcg(reinterpret_cast<const float2*>(src) + (xl * L + y) * L + z);
-            v = cplx<R>{t.x, t.y};
-          } else {
-            double2 t = __ldcg(reinterpret_cast<const double2*>(src) + (xl * L + y) * L + z);
-            v = cplx<R>{t.x, t.y};
-          }
-          x[y] = apply_kin<R, PK>(f, site0 + y * L, v);
-        }
+        x[y] = apply_kin<R, PK>(f, site0 + y * L, v);
       }
       fft::dft<L, -1, R, PK>(x);
 #pragma unroll
@@ -1380,26 +1274,13 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
 #pragma unroll
       for (int y = 0; y < L; ++y) x[y] = sm[off(y / S, xl, y % S, z)];
       fft::dft<L, +1, R, PK>(x);
-      if constexpr (TK) {
 #pragma unroll
-        for (int y0 = 0; y0 < L; y0 += 8) {
-          float k[16];
-          tmem_ld16(kin_t + 2 * y0, k);
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const cplx<R> v = scale_w<R, PK>(x[y0 + j], k[2 * j], k[2 * j + 1]);
-            __stcs(reinterpret_cast<float2*>(gpsi) + site0 + (y0 + j) * L, make_float2(v.re, v.im));
-          }
-        }
-      } else {
-#pragma unroll
-        for (int y = 0; y < L; ++y) {
-          cplx<R> v = apply_kin<R, PK>(f, site0 + y * L, x[y]);
-          if constexpr (sizeof(R) == 4)
-            __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(v.re, v.im));
-          else
-            __stcs(reinterpret_cast<double2*>(gpsi) + site0 + y * L, make_double2(v.re, v.im));
-        }
+      for (int y = 0; y < L; ++y) {
+        cplx<R> v = apply_kin<R, PK>(f, site0 + y * L, x[y]);
+        if constexpr (sizeof(R) == 4)
+          __stcs(reinterpret_cast<float2*>(gpsi) + site0 + y * L, make_float2(v.re, v.im));
+        else
+          __stcs(reinterpret_cast<double2*>(gpsi) + site0 + y * L, make_double2(v.re, v.im));
       }
     }
     // pass 1 of the next orbital writes, per thread, the elements this thread
@@ -1408,15 +1289,7 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
   }
   // leaving early: write-backs this CTA expected land (or time out) first
   if (aborted && outstanding && tid == 0) mbar_wait_bounded<true>(bar, x_phase, f, nullptr);
-  if constexpr (TK) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   cluster.sync();
-  if constexpr (TK) {
-    if (tid < 32) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(KT::COLS)
-                   : "memory");
-    }
-  }
 }
 
 // KIND 0: one lane per pencil, exchange through peers' shared memory;
@@ -1427,8 +1300,7 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
 // CTA's slab of the kinetic table resident in shared memory (FP32 only);
 // 11, 12: kinds 7, 8 with the x pass written back by st.async onto the
 // owners' mbarriers (one cluster barrier per orbital); 13, 14: kinds 11, 12
-// compiled for five CTAs per SM (fewer registers per thread, more warps);
-// 15: kind 11 with each thread's pencil of k(p) held in tensor memory.
+// compiled for five CTAs per SM (fewer registers per thread, more warps).
 template <typename R, int L, int C, int KIND = 0>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
@@ -1438,7 +1310,6 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
                           : (KIND == 3 || KIND == 6) ? BulkShape<R, L, C, false>::SMEM
                           : (KIND == 9 || KIND == 10) ? BulkShape<R, L, C, false, true>::SMEM
-                          : (KIND == 15) ? TkShape<R, L, C>::SMEM
                           : (KIND == 7 || KIND == 8 || KIND >= 11) ? PullShape<R, L, C, false>::SMEM
                                                      : Sh::SMEM;
   void (*kern)(FusedArgs);
@@ -1456,7 +1327,6 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   else if constexpr (KIND == 12) kern = fused_step_async_kernel<R, L, C, true>;
   else if constexpr (KIND == 13) kern = fused_step_async_kernel<R, L, C, false, 5>;
   else if constexpr (KIND == 14) kern = fused_step_async_kernel<R, L, C, true, 5>;
-  else if constexpr (KIND == 15) kern = fused_step_async_kernel<R, L, C, false, 0, true>;
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");
@@ -1538,7 +1408,6 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 32, 8, 11, launch_fused<float, 32, 8, 11>},
     {NRCPS_F32, 32, 8, 12, launch_fused<float, 32, 8, 12>},
     {NRCPS_F32, 32, 8, 13, launch_fused<float, 32, 8, 13>},
-    {NRCPS_F32, 32, 8, 15, launch_fused<float, 32, 8, 15>},
     {NRCPS_F32, 32, 8, 14, launch_fused<float, 32, 8, 14>},
     {NRCPS_F32, 32, 16, 11, launch_fused<float, 32, 16, 11>},
     {NRCPS_F32, 32, 8, 8, launch_fused<float, 32, 8, 8>},
@@ -1552,7 +1421,6 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 32, 8, 2, launch_fused<float, 32, 8, 2>},
     {NRCPS_F32, 32, 8, 1, launch_fused<float, 32, 8, 1>},
     {NRCPS_F32, 48, 12, 11, launch_fused<float, 48, 12, 11>},
-    {NRCPS_F32, 48, 12, 15, launch_fused<float, 48, 12, 15>},
     {NRCPS_F32, 48, 12, 7, launch_fused<float, 48, 12, 7>},
     {NRCPS_F32, 48, 12, 3, launch_fused<float, 48, 12, 3>},
     {NRCPS_F32, 48, 16, 4, launch_fused<float, 48, 16, 4>},

@@ -1083,6 +1083,17 @@ __device__ __forceinline__ void st_async(uint32_t addr, cplx<R> v, uint32_t bar)
                  : "memory");
 }
 
+// Shared memory of the st.async kernel: the padded slab, the mbarriers and
+// abort words, and (when the CTA's rows of an x-plane fill whole 32-bit
+// words) the orbital's Z2 field words, fetched during pass 1 for pass 3.
+template <typename R, int L, int C>
+struct AsyncShape {
+  using Base = FusedShape<R, L, C>;
+  static constexpr bool FW = (Base::S * L) % 32 == 0 && (L * L) % 32 == 0;
+  static constexpr int W = FW ? Base::S * L / 32 : 0;  // words per x-plane of the CTA's rows
+  static constexpr size_t SMEM = PullShape<R, L, C, false>::SMEM + (size_t)(4 * L * W + 15) / 16 * 16;
+};
+
 template <typename R, int L, int C, bool PK = false, int MINB = 0>
 __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
                                   MINB > 0 ? MINB : PullShape<R, L, C, false>::MIN_BLOCKS)
@@ -1103,6 +1114,8 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
   // with parity p and p + 1 and read only after the latter: every CTA sees
   // the same words and leaves at the same barrier.
   int* abort_words = reinterpret_cast<int*>(bar + 2);
+  using AS = AsyncShape<R, L, C>;
+  uint32_t* fw = reinterpret_cast<uint32_t*>(bar + 4);  // [L][AS::W]: the orbital's field words (Z2)
 
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
@@ -1145,6 +1158,15 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
     cplx<R>* gpsi = reinterpret_cast<cplx<R>*>(f.psi) + (size_t)orb * V;
     cplx<R> x[L];
     if (tid == 0 && orb + n_clusters < f.n_orb_total) prefetch_l2(slab(orb + n_clusters), SLAB_BYTES);
+    // the field words pass 3 reads: the CTA's S rows of every x-plane (from
+    // shared memory when the configuration's field starts on a word)
+    const bool fw_ok = AS::FW && (z2_fast || z2_pos) && (kb & 31) == 0;
+    if constexpr (AS::FW) {
+      if (fw_ok) {
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (kb >> 5) + c * AS::W;
+        for (int e = tid; e < L * AS::W; e += Sh::THREADS) fw[e] = __ldg(words + (e / AS::W) * (L * L / 32) + e % AS::W);
+      }
+    }
     // ---- 1. k(p), forward DFT along y from the slab (L2): thread -> (xl, z)
     {
       const int z = tid % L, xl = tid / L;
@@ -1207,7 +1229,30 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
         x[xx] = ld_cluster<R>(mapa_u32(my_region, (uint32_t)(xx / S)) +
                               (uint32_t)((((xx % S) * S + yl) * LP + z) * sizeof(cplx<R>)));
       fft::dft<L, -1, R, PK>(x);
-      if (z2_fast) {
+      if (fw_ok) {
+        // words from shared memory: bit (yl L + z) of the CTA's rows of plane xx
+        const uint32_t* wrow = fw + (yl * L + z) / 32;
+        const int bit = (yl * L + z) % 32;
+        if (z2_pos) {
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (wrow[xx * AS::W] >> bit) & 1u;
+            x[xx] = scale_w_zpos<R, PK>(f.zpos, site0 + xx * L * L, up, x[xx]);
+          }
+        } else if (w_exact) {
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (wrow[xx * AS::W] >> bit) & 1u;
+            x[xx] = scale_w1<R, PK>(x[xx], up ? wp_hi : wm_hi);
+          }
+        } else {
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) {
+            const bool up = (wrow[xx * AS::W] >> bit) & 1u;
+            x[xx] = scale_w<R, PK>(x[xx], up ? wp_hi : wm_hi, up ? wp_lo : wm_lo);
+          }
+        }
+      } else if (z2_fast) {
         const uint64_t k0 = kb + (uint64_t)site0;
         const uint32_t* words = reinterpret_cast<const uint32_t*>(f.field) + (k0 >> 5);
         const int bit = (int)(k0 & 31);
@@ -1310,7 +1355,8 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
                           : (KIND == 3 || KIND == 6) ? BulkShape<R, L, C, false>::SMEM
                           : (KIND == 9 || KIND == 10) ? BulkShape<R, L, C, false, true>::SMEM
-                          : (KIND == 7 || KIND == 8 || KIND >= 11) ? PullShape<R, L, C, false>::SMEM
+                          : (KIND >= 11) ? AsyncShape<R, L, C>::SMEM
+                          : (KIND == 7 || KIND == 8) ? PullShape<R, L, C, false>::SMEM
                                                      : Sh::SMEM;
   void (*kern)(FusedArgs);
   if constexpr (KIND == 1) kern = fused_step_split_kernel<R, L, C>;

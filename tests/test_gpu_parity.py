@@ -665,6 +665,33 @@ def test_z2_position_weights_table_is_bit_identical(ctx, kind, precision, L, clu
     assert max_norm_err(outs[1].cpu().numpy(), ref.cpu().numpy()) < tol
 
 
+@pytest.mark.parametrize("off0", [0, 7, 32 * 5 + 3])
+@pytest.mark.parametrize("L,cluster", [(32, 8), (48, 12)])
+def test_st_async_kernel_field_words_at_any_bit_offset(ctx, off0, L, cluster):
+    """Kind 11 reads the Z2 field words of its rows from shared memory when
+    the configuration's field starts on a 32-bit word, and from L2 otherwise
+    (a field window at an odd bit offset, as the branching driver's
+    sub-streams have): both bit-identical to the peer-access kernel (kind 0,
+    or kind 3 where kind 0 has no cluster of that size)."""
+    psi, kinv, _ = _random_step_inputs(ctx, L, 3, 5, "f32", seed=9)
+    # configuration c reads bits off0 + c (V - 1) .. + V - 1: mixed word alignment
+    bits = nb.draw_z2_bits("RANLXS2", 11, 0, 3 * L ** 3 + 1024, ctx)
+    ref_kind = 0 if cluster == 8 else 3
+    out = []
+    try:
+        ctx.set_option("fused.cluster", cluster)
+        for kind in (ref_kind, 11):
+            ctx.set_option("fused.kind", kind)
+            q = psi.clone()
+            nb.propagate(q, 5, kinv, bits, 0.5, off0=off0, conf_stride=L ** 3 - 1, ctx=ctx)
+            out.append(q)
+        ctx.synchronize()
+    finally:
+        ctx.set_option("fused.cluster", 0)
+        ctx.set_option("fused.kind", -1)
+    assert torch.equal(out[0], out[1])
+
+
 @pytest.mark.parametrize("kind,ref_kind,L,cluster", [(10, 0, 16, 2), (10, 0, 24, 4), (9, 4, 24, 4), (9, 5, 32, 8)])
 def test_resident_kinetic_slab_variants(ctx, kind, ref_kind, L, cluster):
     """Kinds 9 and 10 read k(p) from the CTA's resident slab in shared

@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--cluster", type=int, default=0, help="force the fused kernel's cluster size (0: autotuned)")
     ap.add_argument("--no-fused", action="store_true", help="pencil passes instead of the fused kernel")
     ap.add_argument("--split", type=int, default=-1, help="fused kernel lane split: -1 autotuned, 0, 1")
-    ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 peer access, 1 split, 2 bulk staged, 3 bulk L2, 4-6 packed 0/2/3, 7/8 peer access L2, 9/10 kinds 6/3 with k(p) in shared memory")
+    ap.add_argument("--kind", type=int, default=-1, help="fused kernel kind: -1 autotuned, 0 peer access, 1 split, 2 bulk staged, 3 bulk L2, 4-6 packed 0/2/3, 7/8 peer access L2, 9/10 kinds 6/3 with k(p) in shared memory, 11/12 kinds 7/8 with st.async write-backs")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU path measurement")
     ap.add_argument("--qr", type=int, default=-1, help="re-orthonormalise every k slices (-1: 8 for f32, 0 for f64)")
     ap.add_argument("--workload", default="batched", choices=["batched", "uneven", "cv", "trapped"],

@@ -102,8 +102,7 @@ const char *nrcps_version(void);
  *                      kinetic table resident in shared memory (FP32);
  *                      11, 12: kinds 7, 8 with the x pass written back by
  *                      st.async onto the owner CTA's mbarrier (one cluster
- *                      barrier per orbital); 13, 14: kinds 11, 12 compiled
- *                      for five CTAs per SM (FP32, L = 32);
+ *                      barrier per orbital);
  *   "overlap.tc"       1 (default): dense-source overlaps of FP32 orbitals
  *                      on the tcgen05 tensor cores (TF32 hi/lo split, FP32
  *                      accumulation) where V is a multiple of 16; 0: the

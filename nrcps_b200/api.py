@@ -70,7 +70,7 @@ class Context:
 
     def set_option(self, name: str, value: int) -> None:
         """nrcps_set_option: "propagate.fused" (1/0), "fused.cluster" (0 = autotuned),
-        "fused.split" (-1 = autotuned, 0, 1), "fused.kind" (-1 = autotuned, 0..14)."""
+        "fused.split" (-1 = autotuned, 0, 1), "fused.kind" (-1 = autotuned, 0..12)."""
         self.check(lib().nrcps_set_option(self.handle, name.encode(), int(value)), "set_option")
 
     def autotune(self, precision: str, L: int) -> int:

@@ -114,7 +114,7 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
     if (value < -1 || value > 1) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.split out of range");
     ctx->fused_split = (int)value;
   } else if (n == "fused.kind") {
-    if (value < -1 || value > 14) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
+    if (value < -1 || value > 12) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.kind out of range");
     ctx->fused_kind = (int)value;
   } else if (n == "fused.wait_ns") {
     if (value < 1000) return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "fused.wait_ns below 1000 ns");

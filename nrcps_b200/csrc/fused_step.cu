@@ -1094,9 +1094,8 @@ struct AsyncShape {
   static constexpr size_t SMEM = PullShape<R, L, C, false>::SMEM + (size_t)(4 * L * W + 15) / 16 * 16;
 };
 
-template <typename R, int L, int C, bool PK = false, int MINB = 0>
-__global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
-                                  MINB > 0 ? MINB : PullShape<R, L, C, false>::MIN_BLOCKS)
+template <typename R, int L, int C, bool PK = false>
+__global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<R, L, C, false>::MIN_BLOCKS)
     fused_step_async_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
   static_assert(C > 1, "the write-back goes to cluster peers");
@@ -1344,12 +1343,11 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS,
 // into L2 instead of staged (four CTAs per SM); 9, 10: kinds 6, 3 with the
 // CTA's slab of the kinetic table resident in shared memory (FP32 only);
 // 11, 12: kinds 7, 8 with the x pass written back by st.async onto the
-// owners' mbarriers (one cluster barrier per orbital); 13, 14: kinds 11, 12
-// compiled for five CTAs per SM (fewer registers per thread, more warps).
+// owners' mbarriers (one cluster barrier per orbital).
 template <typename R, int L, int C, int KIND = 0>
 static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int ctas_per_sm_hint) {
   using Sh = FusedShape<R, L, C>;
-  static_assert(KIND < 4 || KIND == 7 || KIND == 11 || KIND == 13 || sizeof(R) == 4,
+  static_assert(KIND < 4 || KIND == 7 || KIND == 11 || sizeof(R) == 4,
                 "packed transforms and the resident k(p) slab are FP32");
   constexpr int THREADS = KIND == 1 ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
   constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
@@ -1371,8 +1369,6 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   else if constexpr (KIND == 8) kern = fused_step_kernel<R, L, C, true, false>;
   else if constexpr (KIND == 11) kern = fused_step_async_kernel<R, L, C, false>;
   else if constexpr (KIND == 12) kern = fused_step_async_kernel<R, L, C, true>;
-  else if constexpr (KIND == 13) kern = fused_step_async_kernel<R, L, C, false, 5>;
-  else if constexpr (KIND == 14) kern = fused_step_async_kernel<R, L, C, true, 5>;
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");
@@ -1453,8 +1449,6 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 32, 8, 7, launch_fused<float, 32, 8, 7>},
     {NRCPS_F32, 32, 8, 11, launch_fused<float, 32, 8, 11>},
     {NRCPS_F32, 32, 8, 12, launch_fused<float, 32, 8, 12>},
-    {NRCPS_F32, 32, 8, 13, launch_fused<float, 32, 8, 13>},
-    {NRCPS_F32, 32, 8, 14, launch_fused<float, 32, 8, 14>},
     {NRCPS_F32, 32, 16, 11, launch_fused<float, 32, 16, 11>},
     {NRCPS_F32, 32, 8, 8, launch_fused<float, 32, 8, 8>},
     {NRCPS_F32, 32, 8, 6, launch_fused<float, 32, 8, 6>},
@@ -1593,8 +1587,8 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
-  // Two rounds over the variants, each timed on 3 launches after one
-  // untimed launch; a variant's time is its faster round (single rounds
+  // Three rounds over the variants, each timed on 3 launches after one
+  // untimed launch; a variant's time is its fastest round (single rounds
   // varied by ~15 % between neighbouring variants on B200).
   float best = 1e30f;
   int best_i = -1;
@@ -1605,7 +1599,7 @@ nrcps_status fused_autotune(nrcps_context* ctx, nrcps_precision prec, int L, int
     round_ms[i] = 1e30f;
     ok[i] = kVariants[i].prec == prec && kVariants[i].L == L;
   }
-  for (int round = 0; round < 2; ++round) {
+  for (int round = 0; round < 3; ++round) {
     for (int i = 0; i < kNumVariants; ++i) {
       if (!ok[i]) continue;
       if (kVariants[i].fn(ctx, f, 0) != NRCPS_OK) {

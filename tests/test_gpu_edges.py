@@ -78,7 +78,7 @@ def test_bad_arguments_are_statuses(ctx):
     from nrcps_b200._capi import NrcpsError
     dev = ctx.device
     with pytest.raises(NrcpsError, match="INVALID_ARGUMENT"):
-        ctx.set_option("fused.kind", 15)
+        ctx.set_option("fused.kind", 13)
     with pytest.raises(NrcpsError, match="INVALID_ARGUMENT"):
         ctx.set_option("no.such.option", 1)
     bits = torch.zeros(1024, dtype=torch.int32, device=dev)

@@ -238,11 +238,21 @@ NCU_TRAFFIC_PER_ORBITAL = {
     ("f32", 32, 7, 8): ((645.4e6 + 583.7e6) / 2432,
                         "ncu, kind 7 cluster 8, 2432 orbitals: 645.4 MB read + 583.7 MB written, scaled by orbitals "
                         "(profiles/fused_step_L32_f32.md)"),
+    ("f32", 32, 11, 8): ((640.81e6 + 577.95e6) / 2432,
+                         "ncu, kind 11 cluster 8, 2432 orbitals: 640.8 MB read + 577.9 MB written, scaled by orbitals "
+                         "(profiles/fused_step_async_L32_f32.md)"),
+    ("f32", 48, 11, 12): ((898.52e6 + 840.19e6) / 1007,
+                          "ncu, kind 11 cluster 12, 1007 orbitals: 898.5 MB read + 840.2 MB written, scaled by "
+                          "orbitals (profiles/fused_step_async_L48_f32_trapped.md)"),
 }
 # FP32-pipe figures of the same captures (FMA pipe and issue active, % of peak)
 NCU_PIPES = {
     ("f32", 32, 7, 8): {"fma_pipe_pct": 41.1, "issue_active_pct": 49.0, "warps_per_sm": 15.4,
                         "source": "profiles/fused_step_L32_f32.md"},
+    ("f32", 32, 11, 8): {"fma_pipe_pct": 41.7, "issue_active_pct": 51.3, "warps_per_sm": 15.0,
+                         "source": "profiles/fused_step_async_L32_f32.md"},
+    ("f32", 48, 11, 12): {"fma_pipe_pct": 36.8, "issue_active_pct": 43.3, "warps_per_sm": 11.3,
+                          "source": "profiles/fused_step_async_L48_f32_trapped.md"},
 }
 
 
@@ -437,6 +447,7 @@ def trapped_core(ctx, n_conf: int, steps: int, warmup: int, cpu_slices: int, pre
         rel = np.max(np.abs(prec["f32"] - prec["f64"]) / np.abs(prec["f64"]), axis=1)
     fp32_tflops = fft_flops_per_orbital_step(L) * n_conf * N / (kms / 1000) / 1e12
     fp32_peak = fp32_peak_tflops(ctx_sm_count(ctx), sm_mhz)
+    traffic = NCU_TRAFFIC_PER_ORBITAL.get(("f32", L, kind, cluster))
     out = {"metric": "trapped config·slices/s", "value": value, "unit": UNIT, "ms_per_step": ms, "steps": steps,
            "warmup": warmup, "dtype": "f32",
            "config": {"workload": f"trapped few-body L={L}^3 T={T}, SHO N={N}+{N} (lambda 4), [K,V,I,V,K] harmonic "
@@ -448,7 +459,10 @@ def trapped_core(ctx, n_conf: int, steps: int, warmup: int, cpu_slices: int, pre
                    "h2d_bytes_per_step": src_host.numel() * 16, "d2h_bytes_per_step": dets_host.numel() * 16},
            "gpu_launches_per_step": launches + 1,
            "roofline": {"bound": "hbm", "achieved": round(step_gbs, 1), "peak": peak, "unit": "GB/s",
-                        "frac": round(step_gbs / peak, 4), "traffic": None, "peak_source": peak_src,
+                        "frac": round(step_gbs / peak, 4),
+                        "traffic": round(traffic[0] * n_conf * N) if traffic else None,
+                        "traffic_source": traffic[1] if traffic else "no ncu capture of this variant",
+                        "peak_source": peak_src,
                         "kernel": "fused transfer-matrix step with the trap folded in (kind %d, cluster %d), "
                                   "%d configs x %d orbitals, %.3f ms/launch" % (kind, cluster, n_conf, N, kms),
                         "fp32": {"convention": "10 V log2 V flops per orbital-step",

@@ -256,9 +256,10 @@ struct PullShape {
   static constexpr int THREADS = Base::THREADS;
   static constexpr size_t SMEM = STAGED ? Base::SMEM : sizeof(cplx<R>) * (size_t)Base::WORK + 32;
   static constexpr int FIT = (int)(228 * 1024 / (SMEM + 1024));
-  // L >= 48: a pencil alone takes 2 L registers, so leave each thread 168
+  // a pencil alone takes 2 L registers: leave each thread 128 at L = 32
+  // and 168 at L >= 48
   static constexpr int WARP_THREADS = (THREADS + 31) / 32 * 32;
-  static constexpr int REG_FIT = L >= 48 ? 65536 / (WARP_THREADS * 168) : 4;
+  static constexpr int REG_FIT = L >= 48 ? 65536 / (WARP_THREADS * 168) : L >= 32 ? 65536 / (WARP_THREADS * 128) : 4;
   static constexpr int CAP = REG_FIT < 4 ? REG_FIT : 4;
   static constexpr int MIN_BLOCKS = STAGED ? Base::MIN_BLOCKS : (FIT > CAP ? CAP : (FIT < 1 ? 1 : FIT));
 };
@@ -1449,6 +1450,8 @@ static const FusedVariant kVariants[] = {
     {NRCPS_F32, 32, 8, 7, launch_fused<float, 32, 8, 7>},
     {NRCPS_F32, 32, 8, 11, launch_fused<float, 32, 8, 11>},
     {NRCPS_F32, 32, 8, 12, launch_fused<float, 32, 8, 12>},
+    {NRCPS_F32, 32, 4, 11, launch_fused<float, 32, 4, 11>},
+    {NRCPS_F32, 32, 2, 11, launch_fused<float, 32, 2, 11>},
     {NRCPS_F32, 32, 16, 11, launch_fused<float, 32, 16, 11>},
     {NRCPS_F32, 32, 8, 8, launch_fused<float, 32, 8, 8>},
     {NRCPS_F32, 32, 8, 6, launch_fused<float, 32, 8, 6>},

@@ -665,6 +665,27 @@ def test_z2_position_weights_table_is_bit_identical(ctx, kind, precision, L, clu
     assert max_norm_err(outs[1].cpu().numpy(), ref.cpu().numpy()) < tol
 
 
+@pytest.mark.parametrize("cluster", [2, 4])
+def test_st_async_kernel_cluster_sizes_are_bit_identical(ctx, cluster):
+    """Kind 11 with 2 or 4 CTAs per cluster (16 or 8 x-planes per CTA) runs
+    every pencil through the same arithmetic as with 8: bit for bit."""
+    psi, kinv, bits = _random_step_inputs(ctx, 32, 3, 5, "f32", seed=10)
+    out = []
+    try:
+        ctx.set_option("fused.kind", 11)
+        for c in (8, cluster):
+            ctx.set_option("fused.cluster", c)
+            q = psi.clone()
+            nb.propagate(q, 5, kinv, bits, 0.5, ctx=ctx)
+            out.append(q)
+            assert ctx.fused_choice("f32", 32) == (11, c)
+        ctx.synchronize()
+    finally:
+        ctx.set_option("fused.cluster", 0)
+        ctx.set_option("fused.kind", -1)
+    assert torch.equal(out[0], out[1])
+
+
 @pytest.mark.parametrize("off0", [0, 7, 32 * 5 + 3])
 @pytest.mark.parametrize("L,cluster", [(32, 8), (48, 12)])
 def test_st_async_kernel_field_words_at_any_bit_offset(ctx, off0, L, cluster):

@@ -149,33 +149,20 @@ constexpr int PAIR_E = PB * PB * 2;  // doubles per block
 template <typename R>
 struct PairShape {
   static int rows(int n) { return (n + PB - 1) / PB * PB; }  // staged rows, padded to whole blocks
-  // sites per tile: two buffers of about 20 KB each (four CTAs per SM)
+  // sites per tile: at most about 20 KB of staged rows per array (four CTAs per SM)
   static int ts(int n) {
-    const int budget = (sizeof(R) == 4 ? 640 : 320) / rows(n);
+    const int budget = (sizeof(R) == 4 ? 1280 : 640) / rows(n);
     int t = 16;
     while (t * 2 <= budget && t < 128) t *= 2;
     return t;
   }
   static int ld(int n) { return 2 * ts(n) + 1; }  // slots per staged row, padded: rows start in different banks
-  static size_t buffer(int n) { return 2 * (size_t)rows(n) * ld(n) * sizeof(cplx<R>); }  // A and B of one tile
   static size_t smem(int n) {
-    const size_t t = 2 * buffer(n);
+    const size_t t = 2 * (size_t)rows(n) * ld(n) * sizeof(cplx<R>);
     const size_t nb = rows(n) / PB, red = nb * nb * PAIR_E * sizeof(double);
     return t > red ? t : red;
   }
 };
-
-// One element global -> shared without the register file; src_bytes 0
-// fills the destination with zeros (the source is not read).
-template <typename R>
-__device__ __forceinline__ void cp_async_cplx(cplx<R>* dst, const cplx<R>* src, bool copy) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-  const uint32_t n = copy ? (uint32_t)sizeof(cplx<R>) : 0u;
-  if constexpr (sizeof(R) == 4)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-  else
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-}
 
 template <typename R>
 __global__ void __launch_bounds__(PAIR_THREADS, 4)
@@ -185,8 +172,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
   extern __shared__ __align__(16) unsigned char pair_smem[];
   const int LD = 2 * ts + 1;
   const int nb = (n + PB - 1) / PB, rows = nb * PB;
-  const size_t BUF = 2 * (size_t)rows * LD;  // complex elements of one buffer: A then B
-  cplx<R>* buf0 = reinterpret_cast<cplx<R>*>(pair_smem);
+  cplx<R>* A = reinterpret_cast<cplx<R>*>(pair_smem);  // [rows][LD]: w psi1 of each slot's term
+  cplx<R>* B = A + (size_t)rows * LD;                   // [rows][LD]: psi2 at the term's partner site
   cg::cluster_group cluster = cg::this_cluster();
   const int split = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
   const long conf = blockIdx.x / split;
@@ -203,112 +190,77 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
   const bool active = g < groups;
   const int abase = (active ? blk / nb : 0) * PB * LD, bbase = (active ? blk % nb : 0) * PB * LD;
   for (int e = threadIdx.x; e < (rows - n) * LD; e += PAIR_THREADS) {  // the padding row stays zero
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      buf0[b * BUF + n * LD + e] = cplx<R>{(R)0, (R)0};
-      buf0[b * BUF + (size_t)rows * LD + n * LD + e] = cplx<R>{(R)0, (R)0};
-    }
+    A[n * LD + e] = cplx<R>{(R)0, (R)0};
+    B[n * LD + e] = cplx<R>{(R)0, (R)0};
   }
   double acc[PB][PB][2];
 #pragma unroll
   for (int a = 0; a < PB; ++a)
 #pragma unroll
     for (int b = 0; b < PB; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-
-  // Issues the copies of tile `tile` into buffer `b` (this thread's slots);
-  // returns whether any site of the tile has a term here (block-uniform).
-  // The weights of this thread's two slots come back in wi, wj.
-  auto stage = [&](long tile, int b, R& wi, R& wj) -> bool {
+  const long ntiles = (vol + ts - 1) / ts;
+  for (long tile = rank; tile < ntiles; tile += split) {
     const long i = tile * ts + q;
     const bool valid = i < vol;
     const long j = valid ? (long)__ldg(opp + i) : 0;
     const bool take = valid && (!paired || i <= j);
     const bool second = paired && valid && i < j;
-    const bool any = __syncthreads_or(take);  // also: every thread is done with buffer b's previous tile
-    if (any) {
-      wi = take ? (R)__ldg(w + i) : (R)0;
-      wj = second ? (R)__ldg(w + j) : (R)0;
-      cplx<R>* A = buf0 + b * BUF;
-      cplx<R>* B = A + (size_t)rows * LD;
-      const long ii = take ? i : 0, jj = take ? j : 0;
-      for (int o = olane; o < n; o += ostride) {
-        const cplx<R>* r1 = p1 + (size_t)o * vol;
-        const cplx<R>* r2 = p2 + (size_t)o * vol;
-        cp_async_cplx<R>(A + o * LD + q, r1 + ii, take);
-        cp_async_cplx<R>(B + o * LD + q, r2 + jj, take);
-        cp_async_cplx<R>(A + o * LD + ts + q, r1 + jj, second);
-        cp_async_cplx<R>(B + o * LD + ts + q, r2 + ii, second);
+    // also the barrier after the previous tile's accumulation
+    if (!__syncthreads_or(take)) continue;
+    const R wi = take ? (R)__ldg(w + i) : (R)0, wj = second ? (R)__ldg(w + j) : (R)0;
+#pragma unroll 4
+    for (int o = olane; o < n; o += ostride) {
+      const cplx<R>* r1 = p1 + (size_t)o * vol;
+      const cplx<R>* r2 = p2 + (size_t)o * vol;
+      cplx<R> a1{(R)0, (R)0}, b1{(R)0, (R)0}, a2{(R)0, (R)0}, b2{(R)0, (R)0};
+      if (take) {
+        a1 = r1[i];
+        b1 = r2[j];
       }
+      if (second) {
+        a2 = r1[j];
+        b2 = r2[i];
+      }
+      A[o * LD + q] = cplx<R>{a1.re * wi, a1.im * wi};
+      B[o * LD + q] = b1;
+      A[o * LD + ts + q] = cplx<R>{a2.re * wj, a2.im * wj};
+      B[o * LD + ts + q] = b2;
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    return any;
-  };
-
-  const long ntiles = (vol + ts - 1) / ts;
-  long tile = rank;
-  int b = 0;
-  R wi = (R)0, wj = (R)0;
-  bool act = tile < ntiles ? stage(tile, 0, wi, wj) : false;
-  while (tile < ntiles) {
-    const long tn = tile + split;
-    R wi_n = (R)0, wj_n = (R)0;
-    bool act_n = false;
-    if (tn < ntiles) act_n = stage(tn, b ^ 1, wi_n, wj_n);  // the next tile's copies fly during this tile's sums
-    else asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_group 1;" ::: "memory");  // this thread's copies of `tile` have landed
-    if (act) {
-      // w into this thread's own A slots, then every slot is complete
-      cplx<R>* A = buf0 + b * BUF;
-      for (int o = olane; o < n; o += ostride) {
-        cplx<R>& a1 = A[o * LD + q];
-        cplx<R>& a2 = A[o * LD + ts + q];
-        a1 = cplx<R>{a1.re * wi, a1.im * wi};
-        a2 = cplx<R>{a2.re * wj, a2.im * wj};
-      }
-      __syncthreads();
-      if (active) {
-        // sum over the slots of a_s b_t (complex, no conjugation) in R: two
-        // fused multiply-adds per real component; then into the FP64 sums
-        const cplx<R>* As = A;
-        const cplx<R>* Bs = A + (size_t)rows * LD;
-        R r[PB][PB][2];
+    __syncthreads();
+    if (active) {
+      // sum over the slots of a_s b_t (complex, no conjugation) in R: two
+      // fused multiply-adds per real component; then into the FP64 sums
+      R r[PB][PB][2];
 #pragma unroll
-        for (int a = 0; a < PB; ++a)
+      for (int a = 0; a < PB; ++a)
 #pragma unroll
-          for (int c = 0; c < PB; ++c) r[a][c][0] = r[a][c][1] = (R)0;
-        for (int slot = g; slot < 2 * ts; slot += groups) {
-          cplx<R> av[PB], bv[PB];
+        for (int b = 0; b < PB; ++b) r[a][b][0] = r[a][b][1] = (R)0;
+      for (int slot = g; slot < 2 * ts; slot += groups) {
+        cplx<R> av[PB], bv[PB];
 #pragma unroll
-          for (int k = 0; k < PB; ++k) {
-            av[k] = As[abase + k * LD + slot];
-            bv[k] = Bs[bbase + k * LD + slot];
-          }
-#pragma unroll
-          for (int a = 0; a < PB; ++a)
-#pragma unroll
-            for (int c = 0; c < PB; ++c) {
-              r[a][c][0] = fma(av[a].re, bv[c].re, r[a][c][0]);
-              r[a][c][0] = fma(-av[a].im, bv[c].im, r[a][c][0]);
-              r[a][c][1] = fma(av[a].re, bv[c].im, r[a][c][1]);
-              r[a][c][1] = fma(av[a].im, bv[c].re, r[a][c][1]);
-            }
+        for (int k = 0; k < PB; ++k) {
+          av[k] = A[abase + k * LD + slot];
+          bv[k] = B[bbase + k * LD + slot];
         }
 #pragma unroll
         for (int a = 0; a < PB; ++a)
 #pragma unroll
-          for (int c = 0; c < PB; ++c) {
-            acc[a][c][0] += (double)r[a][c][0];
-            acc[a][c][1] += (double)r[a][c][1];
+          for (int b = 0; b < PB; ++b) {
+            r[a][b][0] = fma(av[a].re, bv[b].re, r[a][b][0]);
+            r[a][b][0] = fma(-av[a].im, bv[b].im, r[a][b][0]);
+            r[a][b][1] = fma(av[a].re, bv[b].im, r[a][b][1]);
+            r[a][b][1] = fma(av[a].im, bv[b].re, r[a][b][1]);
           }
       }
+#pragma unroll
+      for (int a = 0; a < PB; ++a)
+#pragma unroll
+        for (int b = 0; b < PB; ++b) {
+          acc[a][b][0] += (double)r[a][b][0];
+          acc[a][b][1] += (double)r[a][b][1];
+        }
     }
-    tile = tn;
-    b ^= 1;
-    act = act_n;
-    wi = wi_n;
-    wj = wj_n;
   }
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
   // sum the groups of every block in shared memory (fixed order), then the
   // cluster's CTAs in rank order
   __syncthreads();
@@ -318,11 +270,11 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
 #pragma unroll
       for (int a = 0; a < PB; ++a)
 #pragma unroll
-        for (int c = 0; c < PB; ++c)
+        for (int b = 0; b < PB; ++b)
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            const int e = blk * PAIR_E + (a * PB + c) * 2 + k;
-            red[e] = (gg == 0 ? 0.0 : red[e]) + acc[a][c][k];
+          for (int c = 0; c < 2; ++c) {
+            const int e = blk * PAIR_E + (a * PB + b) * 2 + c;
+            red[e] = (gg == 0 ? 0.0 : red[e]) + acc[a][b][c];
           }
     }
     __syncthreads();
@@ -332,9 +284,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     for (int e = threadIdx.x; e < nblk * PAIR_E; e += PAIR_THREADS) {
       double v = 0.0;
       for (int r2 = 0; r2 < split; ++r2) v += cluster.map_shared_rank(red, r2)[e];
-      const int bb = e / PAIR_E, k = e % PAIR_E;
-      const int s_ = PB * (bb / nb) + (k / 2) / PB, t = PB * (bb % nb) + (k / 2) % PB;
-      if (s_ < n && t < n) phi[2 * ((conf * n + s_) * (long)n + t) + (k & 1)] = v;
+      const int b = e / PAIR_E, k = e % PAIR_E;
+      const int s = PB * (b / nb) + (k / 2) / PB, t = PB * (b % nb) + (k / 2) % PB;
+      if (s < n && t < n) phi[2 * ((conf * n + s) * (long)n + t) + (k & 1)] = v;
     }
   }
   cluster.sync();  // peers keep their shared memory until rank 0 has read it

@@ -365,7 +365,7 @@ __global__ void gauss_flags_kernel(const double* u, long npairs, int* flag) {
 }
 
 // Exclusive scan of int flags, one block of 1024 threads per tile of 1024,
-// tile sums then scanned on one block (npairs <= 1024 * 1024 per call).
+// tile sums then scanned on one block (any number of tiles).
 __global__ void scan_tiles_kernel(const int* in, int* out, int* tile_sums, long n) {
   __shared__ int s[1024];
   long i = (long)blockIdx.x * 1024 + threadIdx.x;
@@ -383,7 +383,11 @@ __global__ void scan_tiles_kernel(const int* in, int* out, int* tile_sums, long 
 }
 __global__ void scan_sums_kernel(int* tile_sums, int ntiles, int* total) {
   __shared__ int s[1024];
-  int v = threadIdx.x < ntiles ? tile_sums[threadIdx.x] : 0;
+  // thread t owns tiles [t per, (t + 1) per)
+  const int per = (ntiles + 1023) / 1024, b0 = threadIdx.x * per;
+  int v = 0;
+  for (int k = 0; k < per; ++k)
+    if (b0 + k < ntiles) v += tile_sums[b0 + k];
   s[threadIdx.x] = v;
   __syncthreads();
   for (int off = 1; off < 1024; off <<= 1) {
@@ -392,7 +396,13 @@ __global__ void scan_sums_kernel(int* tile_sums, int ntiles, int* total) {
     s[threadIdx.x] += t;
     __syncthreads();
   }
-  if (threadIdx.x < ntiles) tile_sums[threadIdx.x] = s[threadIdx.x] - v;
+  int run = s[threadIdx.x] - v;  // tiles before this thread's range
+  for (int k = 0; k < per; ++k)
+    if (b0 + k < ntiles) {
+      const int t = tile_sums[b0 + k];
+      tile_sums[b0 + k] = run;
+      run += t;
+    }
   if (threadIdx.x == 1023) *total = s[1023];
 }
 // out value index k = rank of the accepted pair; last_pair[k] remembers the
@@ -552,10 +562,13 @@ extern "C" nrcps_status nrcps_draw_fields(nrcps_context* ctx, int kind, long see
   long done = 0;
   while (done < need_total) {
     long need = need_total - done;
-    long npairs = (long)(need * 1.35) + 4096;  // acceptance pi/4 = 0.785
-    if (npairs > 1024L * 1024) npairs = 1024L * 1024;
+    // pairs per round: acceptance pi/4 = 0.785; up to 32 M pairs (0.9 GB of
+    // working memory), so a large draw takes few host round trips
+    long npairs = (long)(need * 1.35) + 4096;
+    if (npairs > 32L * 1024 * 1024) npairs = 32L * 1024 * 1024;
+    const long ntiles_max = (npairs + 1023) / 1024;
     size_t bytes_u = sizeof(double) * 2 * npairs;
-    size_t bytes_i = sizeof(int) * (3 * npairs + 2048 + 16);
+    size_t bytes_i = sizeof(int) * (3 * npairs + ntiles_max + 16);
     nrcps_status st;
     char* base = (char*)scratch(ctx, bytes_u + bytes_i, &st);
     if (!base) return st;
@@ -564,7 +577,7 @@ extern "C" nrcps_status nrcps_draw_fields(nrcps_context* ctx, int kind, long see
     int* rank = flag + npairs;
     int* pair_of_rank = rank + npairs;
     int* tiles = pair_of_rank + npairs;
-    int* total = tiles + 2048;
+    int* total = tiles + ntiles_max;
     NRCPS_TRY(generate(ctx, kind, seed, *offset, 2 * (uint64_t)npairs, rng::OUT_UNIFORM, u, nullptr));
     unsigned g = grid_for(npairs, 256, (long)ctx->sm_count * 8);
     gauss_flags_kernel<<<g, 256, 0, ctx->stream>>>(u, npairs, flag);

@@ -89,6 +89,21 @@ def test_gauss_fields_stream_exact(ctx, field):
     assert np.max(np.abs(nxt.cpu().numpy()[0] - r.fields(field, vol, 1)[0])) < 1e-13
 
 
+def test_gauss_fields_large_draw_is_one_stream(ctx):
+    """A draw larger than one round of the Gaussian sampler (32 M candidate
+    pairs, so this one takes two rounds and a host read of the consumed
+    stream length between them) equals the same stream drawn slice by slice,
+    and ends at the same stream position."""
+    vol, slices = 48 ** 3, 240  # 26.5 M values
+    big, off = nb.draw_fields("RANLXS2", 5, "GAUSS", vol, slices, 0, ctx)
+    pos = 0
+    for t0 in range(0, slices, 60):
+        part, pos = nb.draw_fields("RANLXS2", 5, "GAUSS", vol, 60, pos, ctx)
+        assert torch.equal(part, big[t0:t0 + 60])
+    assert pos == off
+    del big
+
+
 def test_z2_bits(ctx):
     first, count = 96 * 7 + 5, 100_000
     bits = nb.draw_z2_bits("RANLXS2", 11, first, count, ctx).cpu().numpy().view(np.uint32)

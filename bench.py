@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--cv-extra", type=int, default=1 << 20, help="cv: extra field draws for <g>")
     ap.add_argument("--cv-epochs", type=int, default=6)
     ap.add_argument("--jobs", type=int, default=512, help="jobs of the uneven workload")
+    ap.add_argument("--uneven-groups", action="store_true",
+                    help="uneven: also time every (L, N) group alone and the field draw alone")
     ap.add_argument("--precision-configs", type=int, default=64,
                     help="configurations of the FP32-vs-FP64 precision report (0: skip)")
     return ap.parse_args()
@@ -834,12 +836,43 @@ def uneven_core(ctx, n_jobs: int, steps: int, warmup: int, precision: str = "f32
     return out
 
 
+def uneven_breakdown(ctx, n_jobs: int, precision: str = "f32"):
+    """Where the uneven step goes: every (L, N) group run alone as its own
+    batch (its own field draw included) and the whole step's Gaussian field
+    draw alone; a sum of the groups close to the whole step means the groups'
+    launches already fill the GPU one after another."""
+    import nrcps_b200 as nb
+    jobs = uneven_jobs(n_jobs)
+    full = nb.Batch(jobs, seed=99, field="GAUSS", a=0.3, precision=precision, ctx=ctx)
+    n_orb = full.n_orb
+    full.run()
+    full_ms = cuda_ms(full.run, 2)
+    full.close()
+    sites = sum(j.T * j.L ** 3 for j in jobs)
+    draw_ms = cuda_ms(lambda: nb.draw_fields("RANLXS2", 99, "GAUSS", sites // 8, 8, 0, ctx), 1)
+    groups = {}
+    for j, n in zip(jobs, n_orb):
+        groups.setdefault((j.L, n), []).append(j)
+    out = {}
+    for (L, N), js in sorted(groups.items()):
+        b = nb.Batch(js, seed=99, field="GAUSS", a=0.3, precision=precision, ctx=ctx)
+        b.run()
+        ms = cuda_ms(b.run, 2)
+        b.close()
+        out[f"L{L}_N{N}"] = {"jobs": len(js), "config_slices": sum(j.T for j in js),
+                             "orbital_steps": sum(j.T for j in js) * N, "ms_alone": round(ms, 2)}
+    return {"whole_step_ms": round(full_ms, 1), "field_draw_ms": round(draw_ms, 1),
+            "sum_of_groups_alone_ms": round(sum(v["ms_alone"] for v in out.values()), 1), "groups": out}
+
+
 def run_uneven(a):
     import nrcps_b200 as nb
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
     ctx = nb.Context(0)
     line = uneven_core(ctx, a.jobs, a.steps, a.warmup, a.precision)
+    if a.uneven_groups:
+        line["breakdown"] = uneven_breakdown(ctx, a.jobs, a.precision)
     line.update({"n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                  "data": "synthetic (device-drawn Gaussian fields)"})
     print(json.dumps(line))

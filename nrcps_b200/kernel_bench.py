@@ -56,17 +56,24 @@ def _time(fn, reps: int, warmup: int = 2) -> float:
     return e0.elapsed_time(e1) / reps
 
 
-def bench_step(ctx: Context, L: int, orbitals: int, precision: str, kind: int, cluster: int, reps: int) -> dict:
+def bench_step(ctx: Context, L: int, orbitals: int, precision: str, kind: int, cluster: int, reps: int,
+               field: str = "z2") -> dict:
     dims = (L, L, L)
     batch = 19
     nconf = max(1, orbitals // batch)
     psi = torch.randn((nconf * batch,) + dims, dtype=torch.complex64 if precision == "f32" else torch.complex128,
                       device=ctx.device)
-    bits = draw_z2_bits("RANLXS2", 7, 0, nconf * L ** 3, ctx)
     kinv = torch.from_numpy(1.0 / kinetic_table(dims, "PERFECT", 1.0, 0.5, 2.0)).to(ctx.device)
     pf = C.PositionFactor()
-    pf.field_mode, pf.dev_field, pf.bit0, pf.conf_stride = 1, bits.data_ptr(), 0, L ** 3
-    pf.a, pf.dev_pos = 0.5, None
+    if field == "gauss":  # Gaussian phi, a = 0.3: the general position-factor path
+        from .api import draw_fields
+        fld, _ = draw_fields("RANLXS2", 7, "GAUSS", L ** 3, nconf, 0, ctx)
+        pf.field_mode, pf.dev_field, pf.bit0, pf.conf_stride = 2, fld.data_ptr(), 0, L ** 3
+        pf.a, pf.dev_pos = 0.3, None
+    else:
+        fld = draw_z2_bits("RANLXS2", 7, 0, nconf * L ** 3, ctx)
+        pf.field_mode, pf.dev_field, pf.bit0, pf.conf_stride = 1, fld.data_ptr(), 0, L ** 3
+        pf.a, pf.dev_pos = 0.5, None
     d3 = np.array(dims, dtype=np.int32)
     ctx.set_option("fused.kind", kind)
     ctx.set_option("fused.cluster", cluster)
@@ -84,7 +91,7 @@ def bench_step(ctx: Context, L: int, orbitals: int, precision: str, kind: int, c
         ctx.set_option("fused.kind", -1)
         ctx.set_option("fused.cluster", 0)
     esize = 8 if precision == "f32" else 16
-    return {"kernel": "step", "L": L, "orbitals": nconf * batch, "precision": precision, "kind": kind,
+    return {"kernel": "step", "field": field, "L": L, "orbitals": nconf * batch, "precision": precision, "kind": kind,
             "cluster": cluster, "ms": round(ms, 4), "GBps": round(2.0 * L ** 3 * esize * nconf * batch / ms / 1e6, 1)}
 
 
@@ -184,6 +191,7 @@ def main(argv=None) -> int:
     ap.add_argument("what", choices=["step", "overlap", "dets", "cv", "qr", "rng", "pair"])
     ap.add_argument("--gram-tc", type=int, default=0)
     ap.add_argument("--pair-tile", type=int, default=1)
+    ap.add_argument("--field", default="z2", choices=["z2", "gauss"], help="step: Z2 bits or Gaussian phi")
     ap.add_argument("--L", type=int, default=32)
     ap.add_argument("--orbitals", type=int, default=19456)
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
@@ -199,7 +207,7 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     ctx = Context(0)
     if a.what == "step":
-        r = bench_step(ctx, a.L, a.orbitals, a.precision, a.kind, a.cluster, a.reps)
+        r = bench_step(ctx, a.L, a.orbitals, a.precision, a.kind, a.cluster, a.reps, a.field)
     elif a.what == "overlap":
         r = bench_overlap(ctx, a.L, a.ns, a.nconf, a.tc, a.reps)
     elif a.what == "cv":

@@ -111,12 +111,6 @@ const char *nrcps_version(void);
  *                      fused step reads both weights of every site,
  *                      (1 +- a) P(x)/V, from a table made ahead of the step;
  *                      0: forms them per site (the same values);
- *   "field.weights"    1 (default): ensembles and batches of FP32 orbitals
- *                      with a local non-Z2 field turn each run's field into
- *                      the per-site weights (1 + a phi)/V (times the
- *                      potential), split into FP32 hi + lo pairs, once per
- *                      run instead of once per orbital and step (the same
- *                      values); 0: form them in the step;
  *   "pair.tile"        1 (default): TwoBody pair matrices (n <= 32) by tiles of
  *                      sites staged in shared memory, one thread-block cluster
  *                      per configuration; 0: one block per (s, t) pair;

@@ -27,8 +27,6 @@ namespace nrcps {
 nrcps_status slater_dets_dispatch(nrcps_context* ctx, const double* S, const double* psi1, int N, int nconf, int mode,
                                   int log_det, double* out, long out_conf_stride, long out_offset, double* scr);
 size_t slater_dets_scratch_bytes(int N, int nconf, int mode);
-nrcps_status gauss_weights_in_place(nrcps_context* ctx, double* phi, uint64_t n, double a, long vol,
-                                    const double* pos, const uint64_t* seg_end, const int* seg_L, int nseg);
 nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const void* psi, int nt, int nconf, long vol,
                          nrcps_precision prec, double* S);
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
@@ -100,10 +98,6 @@ struct nrcps_batch {
   long out_doubles = 0;
   uint64_t sites = 0;              // field sites of one run
   double* phi = nullptr;           // Gaussian / Z3 fields, interleaved complex
-  bool phi_table = false;          // phi holds the weights of field mode 3 once a run's fields are drawn
-  uint64_t* seg_end = nullptr;     // device, per job: end of its field sites (the weights' lattice sizes)
-  int* seg_L = nullptr;            // device, per job: L
-  int njobs = 0;
   uint32_t* bits = nullptr;        // Z2 fields
   uint64_t stream_pos = 0;         // generator position (uniforms) of the next run
   cudaGraph_t graph = nullptr;
@@ -146,7 +140,7 @@ static nrcps_status record_batch(nrcps_batch* b, double* out) {
       if (t + 1 >= g.Tmax) break;
       const int nn = g.nact[t + 1];  // configurations measured again at t + 1
       nrcps_position_factor pf{};
-      pf.field_mode = b->bits ? 1 : (b->phi_table ? 3 : 2);
+      pf.field_mode = b->bits ? 1 : 2;
       pf.dev_field = b->bits ? (const void*)b->bits : (const void*)b->phi;
       pf.bit0 = (uint64_t)t * g.V;
       pf.conf_stride = 0;
@@ -192,8 +186,6 @@ extern "C" nrcps_status nrcps_batch_destroy(nrcps_batch* b) {
     if (g.stream) cudaStreamDestroy(g.stream);
   }
   if (b->phi) cudaFree(b->phi);
-  if (b->seg_end) cudaFree(b->seg_end);
-  if (b->seg_L) cudaFree(b->seg_L);
   if (b->bits) cudaFree(b->bits);
   delete b;
   return NRCPS_OK;
@@ -320,23 +312,6 @@ extern "C" nrcps_status nrcps_batch_create(nrcps_context* ctx, const nrcps_batch
   } else {
     if ((st = check_cuda(ctx, cudaMalloc((void**)&b->phi, 16 * (size_t)b->sites), "cudaMalloc(phi)")))
       return fail(st);
-    b->phi_table = params->precision == NRCPS_F32 && ctx->gauss_table;
-    if (b->phi_table) {
-      std::vector<uint64_t> ends(njobs);
-      std::vector<int> Ls(njobs);
-      for (int j = 0; j < njobs; ++j) {
-        ends[j] = base[j] + (uint64_t)jobs[j].n_conf * jobs[j].T * jobs[j].L * jobs[j].L * jobs[j].L;
-        Ls[j] = jobs[j].L;
-      }
-      b->njobs = njobs;
-      if ((st = check_cuda(ctx, cudaMalloc((void**)&b->seg_end, 8 * (size_t)njobs), "cudaMalloc(seg_end)")) ||
-          (st = check_cuda(ctx, cudaMalloc((void**)&b->seg_L, 4 * (size_t)njobs), "cudaMalloc(seg_L)")) ||
-          (st = check_cuda(ctx, cudaMemcpy(b->seg_end, ends.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice),
-                           "upload seg_end")) ||
-          (st = check_cuda(ctx, cudaMemcpy(b->seg_L, Ls.data(), 4 * (size_t)njobs, cudaMemcpyHostToDevice),
-                           "upload seg_L")))
-        return fail(st);
-    }
   }
   *out = b;
   return NRCPS_OK;
@@ -367,9 +342,6 @@ extern "C" nrcps_status nrcps_batch_run(nrcps_batch* b, double* dev_out) {
   } else {
     NRCPS_TRY(nrcps_draw_fields(ctx, b->params.rng_kind, b->params.seed, b->params.field_kind, (long)b->sites, 1,
                                 &b->stream_pos, b->phi));
-    if (b->phi_table)
-      NRCPS_TRY(gauss_weights_in_place(ctx, b->phi, b->sites, b->params.a, 0, nullptr, b->seg_end, b->seg_L,
-                                       b->njobs));
   }
   if (b->exec && b->out_captured != dev_out) {
     cudaGraphExecDestroy(b->exec);

@@ -127,8 +127,6 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
     ctx->overlap_tc = value != 0;
   } else if (n == "fused.zpos") {
     ctx->fused_zpos = value != 0;
-  } else if (n == "field.weights") {
-    ctx->gauss_table = value != 0;
   } else if (n == "pair.tile") {
     ctx->pair_tile = value != 0;
   } else if (n == "qr.gram_tc") {

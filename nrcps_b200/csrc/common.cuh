@@ -99,8 +99,7 @@ struct Context {
   int fused_kind = -1;    // -1: autotuned; else the fused kernel's kind (0..10)
   int lu_warp = 1;        // 1: warp-per-minor determinant kernel for N <= 64; 0: thread-per-minor kernel
   int overlap_tc = 1;     // 1: tensor-core overlap for FP32 orbitals where the shape allows; 0: CUDA cores
-  int fused_zpos = 1;
-  int gauss_table = 1;    // 1: FP32 runs of non-Z2 local fields read per-site weights made once per run (field mode 3)     // 1: Z2 fields with a position factor read per-site weight tables in the fused step
+  int fused_zpos = 1;     // 1: Z2 fields with a position factor read per-site weight tables in the fused step
   int pair_tile = 1;      // 1: pair matrices by the tiled cluster kernel (n <= 32); 0: one block per (s, t)
   int qr_gram_tc = 0;     // 1: QR Gram matrices of FP32 orbitals on the tensor cores (N <= 32); 0: CUDA cores
   // TF32 hi / lo split of the sources for nrcps_overlap's tensor-core path (grown on demand)

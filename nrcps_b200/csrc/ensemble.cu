@@ -26,8 +26,6 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
                          nrcps_precision prec, double* S);
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
                        const double* w, const int* opp, nrcps_precision prec, double* phi, bool opp_checked);
-nrcps_status gauss_weights_in_place(nrcps_context* ctx, double* phi, uint64_t n, double a, long vol,
-                                    const double* pos, const uint64_t* seg_end, const int* seg_L, int nseg);
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
                             const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec,
                             const void* zpos);
@@ -52,7 +50,6 @@ struct nrcps_ensemble {
   float2* kinv_f = nullptr;  // (hi, lo) split of kinv
   double* pos = nullptr;
   void* zpos = nullptr;        // Z2 fields with the potential: per-site weights (zpos_table_kernel's layout)
-  bool phi_table = false;      // phi holds the weights of field mode 3 once a run's fields are drawn
   double* itab = nullptr;
   double* w = nullptr;
   int* opp = nullptr;
@@ -199,8 +196,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       pf.bit0 = (uint64_t)t * vol;
       pf.conf_stride = (uint64_t)T * vol;
     } else {
-      pf.field_mode = e->phi_table ? 3 : 2;
-      if (e->phi_table) pf.dev_pos = nullptr;  // folded into the weights
+      pf.field_mode = 2;
       pf.dev_field = e->phi;
       pf.bit0 = (uint64_t)t * vol;
       pf.conf_stride = (uint64_t)T * vol;
@@ -315,7 +311,6 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
     }
   } else {
     if ((st = dalloc(ctx, &e->phi, 16 * sites))) return fail(st);
-    e->phi_table = job->precision == NRCPS_F32 && job->local_interaction && ctx->gauss_table;
   }
   if ((st = dalloc(ctx, &e->S, 16 * (size_t)nc * N * N))) return fail(st);
   if ((st = dalloc(ctx, &e->lu_scr, slater_dets_scratch_bytes(N, nc, job->mode)))) return fail(st);
@@ -352,7 +347,6 @@ extern "C" nrcps_status nrcps_ensemble_run(nrcps_ensemble* e, uint64_t first_con
                                 &e->gauss_offset, e->phi));
     e->gauss_next_conf += j.n_conf;
   }
-  if (e->phi_table) NRCPS_TRY(gauss_weights_in_place(ctx, e->phi, sites, j.a, e->vol, e->pos, nullptr, nullptr, 0));
   long gen_launches = ctx->launches - n0;
   // ---- the time loop, captured once per output buffer and replayed
   if (e->exec && e->dets_captured != dev_dets) {

@@ -42,7 +42,7 @@ struct FusedArgs {
   const double* pos;      // optional P(x)
   const void* zpos;       // Z2 fields with P(x): per site the weights (1 + a) P(x)/V and (1 - a) P(x)/V,
                           // split (hi, lo, hi, lo) as float4 for R = float, (plus, minus) double2 for double
-  int field_mode;         // 1 bits, 2 complex phi, 0 complex fld, 3 weight table (FP32 orbitals)
+  int field_mode;         // 1 bits, 2 complex phi, 0 complex fld
   const void* field;
   uint64_t off0;          // element/bit offset of configuration 0
   uint64_t conf_stride;
@@ -61,16 +61,6 @@ template <typename R>
 __device__ __forceinline__ cplx<R> apply_w_general(const FusedArgs& f, uint64_t kb, int site, cplx<R> x) {
   double wr, wi;
   const uint64_t k = kb + (uint64_t)site;
-  if (sizeof(R) == 4 && f.field_mode == 3) {
-    // the weights of mode 2 (position factor folded in), split ahead of the
-    // step into (re hi, re lo, im hi, im lo) floats: the same products
-    const float4 t = __ldg(reinterpret_cast<const float4*>(f.field) + k);
-    if (t.z == 0.f && t.w == 0.f) return scale2<R>(x, (R)t.x, (R)t.y);
-    cplx<R> y;
-    y.re = mul2<R>(x.re, (R)t.x, (R)t.y) - mul2<R>(x.im, (R)t.z, (R)t.w);
-    y.im = mul2<R>(x.re, (R)t.z, (R)t.w) + mul2<R>(x.im, (R)t.x, (R)t.y);
-    return y;
-  }
   if (f.field_mode == 1) {
     uint32_t word = __ldg(reinterpret_cast<const uint32_t*>(f.field) + (k >> 5));
     wr = ((word >> (k & 31)) & 1u) ? f.w_plus : f.w_minus;

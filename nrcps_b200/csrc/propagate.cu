@@ -26,7 +26,7 @@ struct PencilGeom {
 enum PencilOp { OP_NONE = 0, OP_PRE_MUL = 1, OP_POST_MUL = 2, OP_MID_FIELD = 3 };
 
 struct FieldArgs {
-  int mode;              // 0 complex fld, 1 Z2 bits, 2 interleaved complex phi, 3 weight table
+  int mode;              // 0 complex fld, 1 Z2 bits, 2 interleaved complex phi
   const void* field;
   uint64_t bit0;         // element (mode 0/2) or bit (mode 1) offset of configuration 0
   uint64_t conf_stride;  // elements or bits between configurations
@@ -48,9 +48,6 @@ __device__ __forceinline__ cplx<R> field_factor(const FieldArgs& f, long conf, l
     uint32_t word = reinterpret_cast<const uint32_t*>(f.field)[k >> 5];
     double phi = ((word >> (k & 31)) & 1u) ? 1.0 : -1.0;
     w = cplx<R>{(R)((1.0 + f.a * phi) / f.vol), (R)0};
-  } else if (f.mode == 3) {  // (re hi, re lo, im hi, im lo); the position factor is folded in
-    const float4 t = reinterpret_cast<const float4*>(f.field)[k];
-    return cplx<R>{(R)((double)t.x + (double)t.y), (R)((double)t.z + (double)t.w)};
   } else {
     double2 phi = reinterpret_cast<const double2*>(f.field)[k];
     w = cplx<R>{(R)((1.0 + f.a * phi.x) / f.vol), (R)((f.a * phi.y) / f.vol)};
@@ -314,49 +311,6 @@ nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, con
 // The per-site weights of a Z2 field times a position factor P:
 // (1 + a) P/V and (1 - a) P/V, each split (hi, lo) into floats (float4 per
 // site) for FP32 orbitals, plain doubles (double2 per site) for FP64.
-// Field mode 3 for FP32 orbitals: the weights of mode 2,
-// wr = (1 + a Re phi)/V and wi = a Im phi/V (times P(x) when given), formed in
-// FP64 exactly as the fused step forms them per site and split into
-// (re hi, re lo, im hi, im lo) floats, written over phi in place (16 bytes
-// per site either way).  Without segments the array is one lattice of `vol`
-// sites (site i is lattice site i % vol); with them, element i belongs to the
-// first segment s with seg_end[s] > i, a lattice of seg_L[s]^3 sites (the
-// jobs of a batch, in job order).
-__global__ void gauss_weights_kernel(double* phi, uint64_t n, double a, const double* pos, long vol,
-                                     const uint64_t* seg_end, const int* seg_L, int nseg) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    long v = vol;
-    if (seg_end) {
-      int lo = 0, hi = nseg - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi) / 2;
-        if (seg_end[mid] > i) hi = mid;
-        else lo = mid + 1;
-      }
-      v = (long)seg_L[lo] * seg_L[lo] * seg_L[lo];
-    }
-    const double inv_vol = 1.0 / (double)v;
-    const double2 p = reinterpret_cast<const double2*>(phi)[i];
-    double wr = (1.0 + a * p.x) * inv_vol, wi = (a * p.y) * inv_vol;
-    if (pos) {
-      const double q = pos[i % (uint64_t)vol];
-      wr *= q;
-      wi *= q;
-    }
-    const float hr = (float)wr, hi = (float)wi;
-    reinterpret_cast<float4*>(phi)[i] = make_float4(hr, (float)(wr - (double)hr), hi, (float)(wi - (double)hi));
-  }
-}
-
-nrcps_status gauss_weights_in_place(nrcps_context* ctx, double* phi, uint64_t n, double a, long vol,
-                                    const double* pos, const uint64_t* seg_end, const int* seg_L, int nseg) {
-  if (n == 0) return NRCPS_OK;
-  gauss_weights_kernel<<<grid_for((long)n, 256, (long)ctx->sm_count * 16), 256, 0, ctx->stream>>>(
-      phi, n, a, pos, vol, seg_end, seg_L, nseg);
-  ctx->launches++;
-  return check_launch(ctx, "gauss_weights_kernel");
-}
-
 __global__ void zpos_table_kernel(void* tab, const double* pos, double w_plus, double w_minus, long n, int f32) {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const double p = pos[i];

@@ -275,34 +275,6 @@ def test_pair_matrix_with_a_table_that_is_no_involution(ctx, precision):
         assert max_norm_err(got[c], r) < tol
 
 
-def test_field_weight_table_is_bit_identical(golden, ctx):
-    """FP32 runs of a local Gaussian field: the run's field turned once into
-    per-site FP32 hi + lo weights ("field.weights" 1, the default) gives the
-    same determinants bit for bit as forming the weights in every step (0),
-    for an ensemble (Gaussian a=0.3) and an uneven batch (jobs of different
-    L, each weight divided by its own volume)."""
-    g = golden("ensemble_gauss.npz")
-    args = json.loads(str(g["args"]))
-    out = {}
-    jobs = [nb.BatchJob(L=L, T=T, n_conf=c, fermi_energy=ef) for L, T, c, ef in
-            [(16, 6, 2, 0.08), (24, 4, 1, 0.03), (16, 5, 1, 0.08), (32, 3, 2, 0.02)]]
-    try:
-        for wt in (0, 1):
-            ctx.set_option("field.weights", wt)
-            job = _job_from_golden(args, "f32")
-            ens = _ensemble_from_golden(g, args, job, ctx)
-            d = ens.run(0).clone()
-            ens.close()
-            b = nb.Batch(jobs, seed=99, field="GAUSS", a=0.3, precision="f32", ctx=ctx)
-            out[wt] = (d, [x.clone() for x in b.run()])
-            b.close()
-    finally:
-        ctx.set_option("field.weights", 1)
-    assert torch.equal(out[0][0], out[1][0])
-    for x, y in zip(out[0][1], out[1][1]):
-        assert torch.equal(x, y)
-
-
 def test_lu_cases_match_reference(golden, ctx):
     """Determinants against ludcmp: 1e-12 relative, or 1e-13 of the Hadamard
     bound (product of row norms) for the deliberately near-singular cases,

@@ -1095,7 +1095,10 @@ struct AsyncShape {
   static constexpr size_t SMEM = PullShape<R, L, C, false>::SMEM + (size_t)(4 * L * W + 15) / 16 * 16;
 };
 
-template <typename R, int L, int C, bool PK = false>
+// FK: 1 = compiled for Z2 fields only (with or without a position factor),
+// 2 = for every other field only; one instance per field class keeps the
+// other class's code, and its registers, out of the kernel.
+template <typename R, int L, int C, bool PK = false, int FK = 1>
 __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<R, L, C, false>::MIN_BLOCKS)
     fused_step_async_kernel(FusedArgs f) {
   using Sh = FusedShape<R, L, C>;
@@ -1128,8 +1131,8 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
     return reinterpret_cast<const cplx<R>*>(f.psi) + (size_t)orb * V + (size_t)c * S * L * L;
   };
 
-  const bool z2_fast = (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
-  const bool z2_pos = (f.field_mode == 1) && (f.zpos != nullptr) && ((L * L) % 32 == 0);
+  const bool z2_fast = FK == 1 && (f.field_mode == 1) && (f.pos == nullptr) && ((L * L) % 32 == 0);
+  const bool z2_pos = FK == 1 && (f.field_mode == 1) && (f.zpos != nullptr) && ((L * L) % 32 == 0);
   R wp_hi, wp_lo, wm_hi, wm_lo;
   split<R>(f.w_plus, wp_hi, wp_lo);
   split<R>(f.w_minus, wm_hi, wm_lo);
@@ -1278,7 +1281,7 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
           const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
           x[xx] = scale_w_zpos<R, PK>(f.zpos, site0 + xx * L * L, up, x[xx]);
         }
-      } else {
+      } else if constexpr (FK == 2) {
 #pragma unroll
         for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
       }
@@ -1368,8 +1371,12 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   else if constexpr (KIND == 10) kern = fused_step_bulk_kernel<R, L, C, false, false, true>;
   else if constexpr (KIND == 7) kern = fused_step_kernel<R, L, C, false, false>;
   else if constexpr (KIND == 8) kern = fused_step_kernel<R, L, C, true, false>;
-  else if constexpr (KIND == 11) kern = fused_step_async_kernel<R, L, C, false>;
-  else if constexpr (KIND == 12) kern = fused_step_async_kernel<R, L, C, true>;
+  else if constexpr (KIND == 11 || KIND == 12) {
+    // the instance of the field's class: Z2 (bits, with or without a
+    // position factor) or any other field
+    const bool z2 = f.field_mode == 1 && (L * L) % 32 == 0 && (f.pos == nullptr || f.zpos != nullptr);
+    kern = z2 ? fused_step_async_kernel<R, L, C, KIND == 12, 1> : fused_step_async_kernel<R, L, C, KIND == 12, 2>;
+  }
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   if (e != cudaSuccess) return check_cuda(ctx, e, "fused_step: smem attribute");

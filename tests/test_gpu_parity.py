@@ -758,30 +758,43 @@ def test_synchronize_reports_no_timeout(ctx):
 # every fused kernel with mbarrier waits: peer access with a staged slab (0,
 # also as a one-CTA cluster), lane split (1), bulk exchange staged (2) and via
 # L2 (3), st.async write-backs (11)
-_WAITING_VARIANTS = [(0, "f32", 32, 8), (0, "f32", 16, 1), (1, "f32", 32, 8), (2, "f32", 32, 8), (3, "f32", 32, 8),
-                     (3, "f64", 32, 16), (11, "f32", 32, 8), (11, "f64", 32, 16), (11, "f32", 48, 12)]
+_WAITING_VARIANTS = [(0, "f32", 32, 8, "z2"), (0, "f32", 16, 1, "z2"), (1, "f32", 32, 8, "z2"),
+                     (2, "f32", 32, 8, "z2"), (3, "f32", 32, 8, "z2"), (3, "f64", 32, 16, "z2"),
+                     (11, "f32", 32, 8, "z2"), (11, "f64", 32, 16, "z2"), (11, "f32", 48, 12, "z2"),
+                     (11, "f32", 32, 8, "gauss"), (12, "f32", 32, 8, "gauss")]
 
 
-@pytest.mark.parametrize("kind,precision,L,cluster", _WAITING_VARIANTS)
-def test_fused_wait_time_out_is_reported_and_context_survives(ctx, kind, precision, L, cluster):
+@pytest.mark.parametrize("kind,precision,L,cluster,field", _WAITING_VARIANTS)
+def test_fused_wait_time_out_is_reported_and_context_survives(ctx, kind, precision, L, cluster, field):
     """A wait that runs out: the first wait of CTA 0 of cluster 0 is made on
     an mbarrier nothing arrives on (a stand-in for a copy that never lands),
     with a 2 ms limit.  Its cluster leaves the orbital loop together, the
     launch ends in milliseconds, nrcps_synchronize reports TIMEOUT, and the
-    next step on the same context is bit-identical to a clean run."""
+    next step on the same context is bit-identical to a clean run.  Kinds
+    11/12 have one instance per field class: a Gaussian field runs the
+    other one."""
     import time
     psi, kinv, bits = _random_step_inputs(ctx, L, 3, 5, precision, seed=8)
+    if field == "gauss":
+        phi, _ = nb.draw_fields("RANLXS2", 3, "GAUSS", L ** 3, 3, 0, ctx)
+        fld = {"field": phi, "a": 0.3, "field_mode": 2}
+    else:
+        fld = {"field": bits, "a": 0.5}
+
+    def step(q):
+        nb.propagate(q, 5, kinv, fld["field"], fld["a"], field_mode=fld.get("field_mode", 1), ctx=ctx)
+
     try:
         ctx.set_option("fused.kind", kind)
         ctx.set_option("fused.cluster", cluster)
         ref = psi.clone()
-        nb.propagate(ref, 5, kinv, bits, 0.5, ctx=ctx)
+        step(ref)
         ctx.synchronize()
         ctx.set_option("fused.wait_ns", 2_000_000)
         ctx.set_option("fused.stall_test", 1)
         bad = psi.clone()
         t0 = time.perf_counter()
-        nb.propagate(bad, 5, kinv, bits, 0.5, ctx=ctx)
+        step(bad)
         with pytest.raises(nb.NrcpsError) as err:
             ctx.synchronize()
         assert err.value.status == 7  # NRCPS_ERR_TIMEOUT
@@ -789,7 +802,7 @@ def test_fused_wait_time_out_is_reported_and_context_survives(ctx, kind, precisi
         ctx.set_option("fused.stall_test", 0)
         ctx.set_option("fused.wait_ns", 2_000_000_000)
         again = psi.clone()
-        nb.propagate(again, 5, kinv, bits, 0.5, ctx=ctx)
+        step(again)
         ctx.synchronize()
         assert torch.equal(again, ref)
     finally:

@@ -967,7 +967,12 @@ def run_trapped(a):
     import nrcps_b200 as nb
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    line = trapped_core(nb.Context(0), a.trapped_configs, a.steps, a.warmup, 0 if a.no_cpu_baseline else 4)
+    ctx = nb.Context(0)
+    if a.cluster:
+        ctx.set_option("fused.cluster", a.cluster)
+    if a.kind >= 0:
+        ctx.set_option("fused.kind", a.kind)
+    line = trapped_core(ctx, a.trapped_configs, a.steps, a.warmup, 0 if a.no_cpu_baseline else 4)
     line.update({"n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                  "data": "synthetic (device-drawn fields, SHO sources)"})
     print(json.dumps(line))

@@ -235,7 +235,6 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
       for (int a = 0; a < PB; ++a)
 #pragma unroll
         for (int b = 0; b < PB; ++b) r[a][b][0] = r[a][b][1] = (R)0;
-#pragma unroll(sizeof(R) == 4 ? 4 : 1)
       for (int slot = g; slot < 2 * ts; slot += groups) {
         cplx<R> av[PB], bv[PB];
 #pragma unroll

@@ -77,60 +77,6 @@ constexpr CS unit_root(long k, long n) {
   return CS{c, s};
 }
 
-// ---------------------------------------------- FP32 roots of unity
-// An FP32 twiddle pair (c, s) rounded component-wise has c^2 + s^2 = 1 + e
-// with |e| up to ~1e-7.  Forward and backward transforms use conjugate
-// pairs, so their phase errors cancel while e does not: every F.B round trip
-// would scale each non-zero momentum by the same (1 + e) product, step after
-// step.  unit_root_f32 picks, among the floats within two ulps of (c, s),
-// the pair whose squared norm is closest to 1.  (Round trips of plane
-// waves are then exact; the remaining rounding of general data is
-// unbiased.)
-constexpr double cabs_(double v) { return v < 0 ? -v : v; }
-constexpr double pow2_(int e) {
-  double r = 1.0;
-  for (int i = 0; i < (e < 0 ? -e : e); ++i) r = e < 0 ? r / 2 : r * 2;
-  return r;
-}
-constexpr double float_ulp(double v) {  // spacing of floats near |v| (v != 0)
-  double a = cabs_(v);
-  int e = 0;
-  while (a >= 2.0) {
-    a /= 2;
-    ++e;
-  }
-  while (a < 1.0) {
-    a *= 2;
-    --e;
-  }
-  return pow2_(e - 23);
-}
-struct CSf {
-  float c, s;
-};
-constexpr CSf unit_root_f32(long k, long n) {
-  CS w = unit_root(k, n);
-  double c0 = (double)(float)w.c, s0 = (double)(float)w.s;
-  double uc = c0 != 0.0 ? float_ulp(c0) : 0.0, us = s0 != 0.0 ? float_ulp(s0) : 0.0;
-  double best_c = c0, best_s = s0;
-  double best_e = cabs_(c0 * c0 + s0 * s0 - 1.0);
-  double best_a = cabs_(c0 - w.c) + cabs_(s0 - w.s);
-  for (int dc = -2; dc <= 2; ++dc)
-    for (int ds = -2; ds <= 2; ++ds) {
-      double c = c0 + dc * uc, s = s0 + ds * us;
-      if ((double)(float)c != c || (double)(float)s != s) continue;
-      double e = cabs_(c * c + s * s - 1.0);
-      double a = cabs_(c - w.c) + cabs_(s - w.s);
-      if (e < best_e || (e == best_e && a < best_a)) {
-        best_e = e;
-        best_a = a;
-        best_c = c;
-        best_s = s;
-      }
-    }
-  return CSf{(float)best_c, (float)best_s};
-}
-
 // x * W_N^K with W_N = exp(SIGN 2 pi i / N); exact for multiples of N/4.
 template <int N, int K, int SIGN, typename R>
 __device__ __forceinline__ cplx<R> twiddle(cplx<R> x) {

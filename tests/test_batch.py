@@ -95,6 +95,31 @@ def test_device_batch_uneven_shapes_fp32_vs_fp64():
 
 
 @pytest.mark.gpu
+def test_device_batch_fp32_vs_fp64_at_the_largest_uneven_shapes():
+    """FP32 orbitals at the uneven workload's largest shapes -- L=48, N=33,
+    T=128 and L=24, N=19, T=64, 8 configurations each, Gaussian fields
+    a=0.3 -- against the FP64 batch on the same stream, both re-orthonormalised
+    every 8 slices (the FP64 QR keeps every determinant exact and the long
+    T=128 runs well conditioned): <|det S_m(tau)|^2> per minor and slice."""
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    shell = {19: 2.5, 33: 4.5}
+    spec = [(48, 128, 33), (24, 64, 19)]
+    jobs = [nb.BatchJob(L=L, T=T, n_conf=8, fermi_energy=0.5 * (2 * np.pi / L) ** 2 * shell[N]) for L, T, N in spec]
+    out = {}
+    for prec in ("f32", "f64"):
+        b = nb.Batch(jobs, seed=99, field="GAUSS", a=0.3, precision=prec, qr_period=8, ctx=ctx)
+        assert b.n_orb == [N for _, _, N in spec]
+        out[prec] = [(np.abs(d.cpu().numpy()) ** 2).mean(0) for d in b.run()]
+        b.close()
+    for (L, T, N), a, r in zip(spec, out["f32"], out["f64"]):
+        err = np.max(np.abs(a - r) / np.abs(r), axis=tuple(range(1, a.ndim)))
+        print(f"L={L} N={N} T={T}: FP32 vs FP64 max rel err of <|det|^2> per tau: " +
+              " ".join(f"{v:.1e}" for v in err))
+        assert err.max() < 1e-4, (L, err.max())
+
+
+@pytest.mark.gpu
 def test_device_batch_fp64_at_the_largest_uneven_shapes(golden):
     """The uneven workload's largest shapes -- one L=48, N=33, T=128 job, one
     L=24, N=19, T=64 job and two L=16, N=7, T=32 configurations, Gaussian

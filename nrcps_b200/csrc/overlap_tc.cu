@@ -42,7 +42,6 @@ namespace tc {
 constexpr int BN = 128;                        // orbitals (n) per tile
 constexpr int BN2 = 2 * BN;                    // MMA N: [B_hi; B_lo] rows = accumulator columns per buffer
 constexpr int BK = 32;                         // floats of K per stage: one 128-byte swizzle row
-constexpr int STAGES = 3;
 constexpr int CHUNK = 8;                       // k-blocks (256 floats of K) per FP32 accumulation in TMEM
 constexpr uint32_t RAW_BYTES = BN * BK * 4;    // 16 KB: raw psi tile
 constexpr uint32_t BP_BYTES = 2 * RAW_BYTES;   // 32 KB: [B_hi; B_lo], 256 rows
@@ -51,10 +50,15 @@ constexpr uint32_t A_BYTES = 2 * AH_BYTES;     // 16 KB: [A_hi; A_lo], 128 rows
 constexpr uint32_t STAGE_BYTES = A_BYTES + BP_BYTES;  // 48 KB, 1024-aligned pieces
 constexpr uint32_t TX_BYTES = RAW_BYTES + A_BYTES;
 constexpr int ACC_LD = BN + 1;                 // padded row: lane i's row starts 2 banks after lane i-1's
-constexpr uint32_t ACC_BYTES = ((64 * ACC_LD * 8 + 1023) / 1024) * 1024;  // FP64 running sums of the 64 result rows
+// FP64 running sums of `rows` result rows (2 ns of them are used)
+constexpr uint32_t acc_bytes(int rows) { return ((rows * ACC_LD * 8 + 1023) / 1024) * 1024; }
 constexpr int THREADS = 320;
 constexpr uint32_t TMEM_COLS = 2 * BN2;        // two accumulator buffers
-constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + ACC_BYTES + 1024 /* alignment */ + 256 /* barriers */;
+// STG stages and ACCR FP64 result rows: 3 and 64 in general; 4 and 32 when
+// 2 ns <= 32 (the smaller sum buffer leaves room for one more stage in flight)
+constexpr size_t smem_bytes(int stg, int accr) {
+  return (size_t)stg * STAGE_BYTES + acc_bytes(accr) + 1024 /* alignment */ + 256 /* barriers */;
+}
 constexpr int MAX_NS_BLOCK = 32;               // 2 ns <= 64 accumulator rows per half
 
 // instruction descriptor: D F32, A/B TF32, both K-major, N = 256, M = 128
@@ -164,6 +168,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+template <int STAGES, int ACCR>
 __global__ void __launch_bounds__(THREADS, 1)
     overlap_tc_kernel(const __grid_constant__ CUtensorMap map_psi, const __grid_constant__ CUtensorMap map_ahi,
                       const __grid_constant__ CUtensorMap map_alo, Args g) {
@@ -171,7 +176,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   // 1024-byte aligned stage area (the swizzle atoms repeat every 1024 bytes)
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  double* acc = reinterpret_cast<double*>(base + (size_t)STAGES * STAGE_BYTES);  // [64][ACC_LD] FP64 sums
+  constexpr uint32_t ACC_BYTES = acc_bytes(ACCR);
+  double* acc = reinterpret_cast<double*>(base + (size_t)STAGES * STAGE_BYTES);  // [ACCR][ACC_LD] FP64 sums
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + (size_t)STAGES * STAGE_BYTES + ACC_BYTES);
   uint64_t* full = bars;                  // TMA landed (raw psi + A)
   uint64_t* conv = bars + STAGES;         // operand tile split (4 converter warps)
@@ -209,7 +215,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  for (int i = threadIdx.x; i < 64 * ACC_LD; i += THREADS) acc[i] = 0.0;
+  for (int i = threadIdx.x; i < ACCR * ACC_LD; i += THREADS) acc[i] = 0.0;
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
                  "r"(TMEM_COLS)
@@ -466,8 +472,12 @@ nrcps_status overlap_tc(nrcps_context* ctx, const float* split, int ns, const vo
   static bool attr_set[16] = {false};
   if (!attr_set[ctx->device & 15]) {
     NRCPS_TRY(check_cuda(ctx,
-                         cudaFuncSetAttribute(tc::overlap_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)tc::SMEM),
+                         cudaFuncSetAttribute(tc::overlap_tc_kernel<3, 64>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::smem_bytes(3, 64)),
+                         "overlap_tc: smem attribute"));
+    NRCPS_TRY(check_cuda(ctx,
+                         cudaFuncSetAttribute(tc::overlap_tc_kernel<4, 32>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::smem_bytes(4, 32)),
                          "overlap_tc: smem attribute"));
     attr_set[ctx->device & 15] = true;
   }
@@ -523,8 +533,12 @@ nrcps_status overlap_tc(nrcps_context* ctx, const float* split, int ns, const vo
     a.atomic_out = splits > 1;
     a.S = S;
     a.err = ctx->dev_err;
-    tc::overlap_tc_kernel<<<dim3((unsigned)tiles, (unsigned)splits), tc::THREADS, tc::SMEM, ctx->stream>>>(mpsi, mhi,
-                                                                                                           mlo, a);
+    if (2 * nsb <= 32)
+      tc::overlap_tc_kernel<4, 32><<<dim3((unsigned)tiles, (unsigned)splits), tc::THREADS, tc::smem_bytes(4, 32),
+                                     ctx->stream>>>(mpsi, mhi, mlo, a);
+    else
+      tc::overlap_tc_kernel<3, 64><<<dim3((unsigned)tiles, (unsigned)splits), tc::THREADS, tc::smem_bytes(3, 64),
+                                     ctx->stream>>>(mpsi, mhi, mlo, a);
     ctx->launches++;
     NRCPS_TRY(check_launch(ctx, "overlap_tc_kernel"));
   }

@@ -13,10 +13,11 @@
 // and the four products are formed by ONE M=128, N=256, K=8 MMA per k-step:
 // the A tile stacks [A_hi; A_lo] (rows 0-63, 64-127) and the B tile stacks
 // [B_hi; B_lo] (rows 0-127, 128-255), so the FP32 accumulator holds A_x B_y^T
-// in its four quadrants.  The tensor core accumulates in FP32 for 256 floats
-// of K only (a chunk); each chunk's accumulator is drained into FP64 sums
-// in shared memory while the next chunk accumulates in the second TMEM
-// buffer, so the result carries FP64 accumulation across K.
+// in its four quadrants (the drain adds hi hi + hi lo in FP32 and lo hi;
+// lo lo, 2^-44 of a product, is dropped).  The tensor core accumulates in
+// FP32 for 256 floats of K only (a chunk); each chunk's accumulator is
+// drained into FP64 sums in shared memory while the next chunk accumulates
+// in the second TMEM buffer, so the result carries FP64 accumulation across K.
 //
 // One CTA per (128 orbitals, K range); 10 warps:
 //   warp 0      TMA producer: the raw FP32 psi tile (128 x 32 floats, into the
@@ -331,11 +332,20 @@ __global__ void __launch_bounds__(THREADS, 1)
           double* arow = acc + (size_t)(row & 63) * ACC_LD;
 #pragma unroll 1
           for (int c0 = 0; c0 < BN; c0 += 32) {
-            float u[32], v[32];
+            float u[32];
             tmem_ld32(t0 + (uint32_t)c0, u);
-            tmem_ld32(t0 + (uint32_t)(c0 + BN), v);
+            if (q < 2) {
+              // A_hi rows: hi*hi + hi*lo, added in FP32 (one rounding, below
+              // the error of the chunk's own FP32 accumulation), one conversion
+              float v[32];
+              tmem_ld32(t0 + (uint32_t)(c0 + BN), v);
 #pragma unroll
-            for (int k = 0; k < 32; ++k) arow[c0 + k] += (double)u[k] + (double)v[k];
+              for (int k = 0; k < 32; ++k) arow[c0 + k] += (double)(u[k] + v[k]);
+            } else {
+              // A_lo rows: lo*hi; lo*lo (2^-44 of the product) is dropped
+#pragma unroll
+              for (int k = 0; k < 32; ++k) arow[c0 + k] += (double)u[k];
+            }
           }
         }
         asm volatile("bar.sync 1, 128;" ::: "memory");

@@ -11,7 +11,7 @@ forward, backward and Adam), and enters the estimator
 
 with <g> from many extra field draws (fields only: no propagation), and
 c(tau) fixed from the training pairs, so the estimator stays unbiased: E[g_i]
-= E[<g>].  The plain estimator mean_i C_i(tau) is the fallback and the judge
+= E[<g>].  The plain estimator mean_i C_i(tau) is the fallback and the yardstick
 of the variance reduction.
 
 No counterpart in the reference (its drivers write plain block averages:

@@ -3,7 +3,7 @@
 
 Tolerances: RNG and field integers bit-exact; FP64 propagation, overlaps and
 determinants within 1e-12 relative; FP32 propagation within 1e-5 relative on
-the correlators (the BASELINE target for the fast mode).
+the correlators (the accuracy target of the fast mode).
 """
 import ctypes
 import json

@@ -431,6 +431,27 @@ def test_trapped_workload_fp32_vs_fp64_full_shape(golden, ctx):
     assert err.max() < FP32_REL, err.max()
 
 
+def test_full_size_batch_matches_a_two_configuration_run(ctx):
+    """The batched workload's size: 4096 configurations x 19 orbitals of 32^3
+    sites (2.55 G complex FP32 values, 20.4 GB; offsets past 2^31 in every
+    kernel of the step and the measurement).  The last two configurations'
+    determinants equal, bit for bit, a separate run of just those two
+    configurations (same fields: configuration c reads its own stream
+    window), for 8 slices with a re-orthonormalisation after 4."""
+    idx, _, _ = nb.momenta((32, 32, 32), "PERFECT", 1.0, 0.045, 2.0)
+    assert len(idx) == 19
+    job = nb.EnsembleJob(L=32, T=8, n_conf=4096, seed=7, precision="f32", fermi_energy=0.045, qr_period=4)
+    ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
+    big = ens.run(0)[-2:].clone()
+    ens.close()
+    torch.cuda.empty_cache()
+    job.n_conf = 2
+    ens = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
+    small = ens.run(4094).clone()
+    ens.close()
+    assert torch.equal(big, small)
+
+
 def test_ensemble_fp32_config1(golden, ctx):
     """FP32 propagation: every per-configuration determinant within 5e-5 of
     the reference (FP32 rounding random-walks through 32 steps of six FFT

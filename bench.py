@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--cv-extra", type=int, default=1 << 20, help="cv: extra field draws for <g>")
     ap.add_argument("--cv-epochs", type=int, default=6)
     ap.add_argument("--jobs", type=int, default=512, help="jobs of the uneven workload")
+    ap.add_argument("--real-weights", type=int, default=1, choices=[0, 1],
+                    help="uneven, FP32: 1 steps on one FP32 weight per site made once per run, 0 forms "
+                         "(1 + a phi)/V from phi per site and orbital")
     ap.add_argument("--uneven-groups", action="store_true",
                     help="uneven: also time every (L, N) group alone and the field draw alone")
     ap.add_argument("--precision-configs", type=int, default=64,
@@ -870,7 +873,10 @@ def run_uneven(a):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
     ctx = nb.Context(0)
+    ctx.set_option("batch.real_weights", a.real_weights)
     line = uneven_core(ctx, a.jobs, a.steps, a.warmup, a.precision)
+    line["config"]["field_weights"] = ("one FP32 weight per site, made once per run"
+                                       if a.real_weights and a.precision == "f32" else "formed from phi per site")
     if a.uneven_groups:
         line["breakdown"] = uneven_breakdown(ctx, a.jobs, a.precision)
     line.update({"n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

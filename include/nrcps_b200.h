@@ -117,6 +117,12 @@ const char *nrcps_version(void);
  *   "qr.gram_tc"       1: the Gram matrices of the re-orthonormalisation of
  *                      FP32 orbitals (N <= 32) on the tcgen05 tensor cores
  *                      (TF32 hi/lo); 0 (default): the CUDA-core kernel;
+ *   "batch.real_weights" 1 (default): a batch created afterwards with FP32
+ *                      orbitals and a real Gaussian field turns each run's
+ *                      field into one FP32 weight per site, (1 + a phi)/V
+ *                      rounded once, which the fused step stages in shared
+ *                      memory; 0: the step forms the weight from phi per
+ *                      site and orbital (split into two FP32 parts);
  *   "lu.warp"          1 (default): leading-minor determinants with one warp
  *                      per minor in shared memory (N <= 64); 0: one thread
  *                      per minor with global scratch;

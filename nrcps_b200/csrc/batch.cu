@@ -87,6 +87,23 @@ __global__ void batch_gather_dets_kernel(const double* __restrict__ dets, int N,
   }
 }
 
+// One FP32 weight per site of a real Gaussian field, (1 + a phi)/V with the
+// V of the site's job (the same double expression the fused step forms per
+// site), rounded to FP32 once per run.  start[j]: the first site of job j.
+__global__ void real_weights_kernel(float* __restrict__ w, const double2* __restrict__ phi,
+                                    const uint64_t* __restrict__ start, const double* __restrict__ inv_vol,
+                                    int njobs, double a, uint64_t sites) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < sites; e += (uint64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = njobs - 1;  // the last job that starts at or before e
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(start + mid) <= e) lo = mid;
+      else hi = mid - 1;
+    }
+    w[e] = (float)((1.0 + a * __ldg(phi + e).x) * __ldg(inv_vol + lo));
+  }
+}
+
 }  // namespace
 }  // namespace nrcps
 
@@ -99,6 +116,10 @@ struct nrcps_batch {
   uint64_t sites = 0;              // field sites of one run
   double* phi = nullptr;           // Gaussian / Z3 fields, interleaved complex
   uint32_t* bits = nullptr;        // Z2 fields
+  float* wtab = nullptr;           // FP32 orbitals, real Gaussian fields: one weight per site
+  uint64_t* job_start = nullptr;   // first field site of every job (device)
+  double* job_inv_vol = nullptr;   // 1 / V of every job (device)
+  int njobs = 0;
   uint64_t stream_pos = 0;         // generator position (uniforms) of the next run
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -140,8 +161,8 @@ static nrcps_status record_batch(nrcps_batch* b, double* out) {
       if (t + 1 >= g.Tmax) break;
       const int nn = g.nact[t + 1];  // configurations measured again at t + 1
       nrcps_position_factor pf{};
-      pf.field_mode = b->bits ? 1 : 2;
-      pf.dev_field = b->bits ? (const void*)b->bits : (const void*)b->phi;
+      pf.field_mode = b->bits ? 1 : b->wtab ? 3 : 2;
+      pf.dev_field = b->bits ? (const void*)b->bits : b->wtab ? (const void*)b->wtab : (const void*)b->phi;
       pf.bit0 = (uint64_t)t * g.V;
       pf.conf_stride = 0;
       pf.dev_conf_base = g.conf_base;
@@ -185,8 +206,9 @@ extern "C" nrcps_status nrcps_batch_destroy(nrcps_batch* b) {
     if (g.done) cudaEventDestroy(g.done);
     if (g.stream) cudaStreamDestroy(g.stream);
   }
-  if (b->phi) cudaFree(b->phi);
-  if (b->bits) cudaFree(b->bits);
+  void* fields[] = {b->phi, b->bits, b->wtab, b->job_start, b->job_inv_vol};
+  for (void* p : fields)
+    if (p) cudaFree(p);
   delete b;
   return NRCPS_OK;
 }
@@ -312,6 +334,19 @@ extern "C" nrcps_status nrcps_batch_create(nrcps_context* ctx, const nrcps_batch
   } else {
     if ((st = check_cuda(ctx, cudaMalloc((void**)&b->phi, 16 * (size_t)b->sites), "cudaMalloc(phi)")))
       return fail(st);
+    if (params->field_kind == NRCPS_FIELD_GAUSS && params->precision == NRCPS_F32 && ctx->batch_real_weights) {
+      std::vector<double> iv(njobs);
+      for (int j = 0; j < njobs; ++j) iv[j] = 1.0 / ((double)jobs[j].L * jobs[j].L * jobs[j].L);
+      b->njobs = njobs;
+      if ((st = check_cuda(ctx, cudaMalloc((void**)&b->wtab, 4 * (size_t)b->sites), "cudaMalloc(weights)")) ||
+          (st = check_cuda(ctx, cudaMalloc((void**)&b->job_start, 8 * (size_t)njobs), "cudaMalloc(job starts)")) ||
+          (st = check_cuda(ctx, cudaMalloc((void**)&b->job_inv_vol, 8 * (size_t)njobs), "cudaMalloc(job 1/V)")) ||
+          (st = check_cuda(ctx, cudaMemcpy(b->job_start, base.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice),
+                           "cudaMemcpy(job starts)")) ||
+          (st = check_cuda(ctx, cudaMemcpy(b->job_inv_vol, iv.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice),
+                           "cudaMemcpy(job 1/V)")))
+        return fail(st);
+    }
   }
   *out = b;
   return NRCPS_OK;
@@ -342,6 +377,13 @@ extern "C" nrcps_status nrcps_batch_run(nrcps_batch* b, double* dev_out) {
   } else {
     NRCPS_TRY(nrcps_draw_fields(ctx, b->params.rng_kind, b->params.seed, b->params.field_kind, (long)b->sites, 1,
                                 &b->stream_pos, b->phi));
+    if (b->wtab) {
+      real_weights_kernel<<<grid_for((long)b->sites, 256, (long)ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+          b->wtab, reinterpret_cast<const double2*>(b->phi), b->job_start, b->job_inv_vol, b->njobs, b->params.a,
+          b->sites);
+      ctx->launches++;
+      NRCPS_TRY(check_launch(ctx, "real_weights_kernel"));
+    }
   }
   if (b->exec && b->out_captured != dev_out) {
     cudaGraphExecDestroy(b->exec);

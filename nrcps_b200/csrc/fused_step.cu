@@ -42,7 +42,7 @@ struct FusedArgs {
   const double* pos;      // optional P(x)
   const void* zpos;       // Z2 fields with P(x): per site the weights (1 + a) P(x)/V and (1 - a) P(x)/V,
                           // split (hi, lo, hi, lo) as float4 for R = float, (plus, minus) double2 for double
-  int field_mode;         // 1 bits, 2 complex phi, 0 complex fld
+  int field_mode;         // 1 bits, 2 complex phi, 0 complex fld, 3 real FP32 weights (FP32 orbitals)
   const void* field;
   uint64_t off0;          // element/bit offset of configuration 0
   uint64_t conf_stride;
@@ -61,6 +61,10 @@ template <typename R>
 __device__ __forceinline__ cplx<R> apply_w_general(const FusedArgs& f, uint64_t kb, int site, cplx<R> x) {
   double wr, wi;
   const uint64_t k = kb + (uint64_t)site;
+  if (sizeof(R) == 4 && f.field_mode == 3) {  // the site's weight, made once per run
+    const R w = (R)__ldg(reinterpret_cast<const float*>(f.field) + k);
+    return cplx<R>{x.re * w, x.im * w};
+  }
   if (f.field_mode == 1) {
     uint32_t word = __ldg(reinterpret_cast<const uint32_t*>(f.field) + (k >> 5));
     wr = ((word >> (k & 31)) & 1u) ? f.w_plus : f.w_minus;
@@ -1087,12 +1091,19 @@ __device__ __forceinline__ void st_async(uint32_t addr, cplx<R> v, uint32_t bar)
 // Shared memory of the st.async kernel: the padded slab, the mbarriers and
 // abort words, and (when the CTA's rows of an x-plane fill whole 32-bit
 // words) the orbital's Z2 field words, fetched during pass 1 for pass 3.
-template <typename R, int L, int C>
+// The general-field instance (FK = 2) instead stages the CTA's rows of a run's
+// real FP32 weight table (field mode 3): S L floats of every x-plane.
+template <typename R, int L, int C, int FK = 1>
 struct AsyncShape {
   using Base = FusedShape<R, L, C>;
   static constexpr bool FW = (Base::S * L) % 32 == 0 && (L * L) % 32 == 0;
   static constexpr int W = FW ? Base::S * L / 32 : 0;  // words per x-plane of the CTA's rows
-  static constexpr size_t SMEM = PullShape<R, L, C, false>::SMEM + (size_t)(4 * L * W + 15) / 16 * 16;
+  // FK 2 with FP32 orbitals: room for a real weight table's rows, copied in
+  // 16-byte pieces (rows of whole pieces, planes on 4 floats, an aligned start)
+  static constexpr bool WT = FK == 2 && sizeof(R) == 4 && (Base::S * L) % 4 == 0 && L % 2 == 0 &&
+                             (sizeof(cplx<R>) * Base::WORK + 32) % 16 == 0;
+  static constexpr size_t EXTRA = WT ? (size_t)4 * Base::S * L * L : (size_t)(4 * L * W + 15) / 16 * 16;
+  static constexpr size_t SMEM = PullShape<R, L, C, false>::SMEM + EXTRA;
 };
 
 // FK: 1 = compiled for Z2 fields only (with or without a position factor),
@@ -1117,8 +1128,9 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
   // with parity p and p + 1 and read only after the latter: every CTA sees
   // the same words and leaves at the same barrier.
   int* abort_words = reinterpret_cast<int*>(bar + 2);
-  using AS = AsyncShape<R, L, C>;
+  using AS = AsyncShape<R, L, C, FK>;
   uint32_t* fw = reinterpret_cast<uint32_t*>(bar + 4);  // [L][AS::W]: the orbital's field words (Z2)
+  float* wbuf = reinterpret_cast<float*>(bar + 4);      // FK 2, [L][S L]: the CTA's rows of the weight table
 
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
@@ -1170,6 +1182,23 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
         for (int e = tid; e < L * AS::W; e += Sh::THREADS) fw[e] = __ldg(words + (e / AS::W) * (L * L / 32) + e % AS::W);
       }
     }
+    // a real weight table (field mode 3): the CTA's rows of every x-plane,
+    // S L floats each, copied by cp.async while pass 1 runs (16-byte pieces:
+    // the configuration's table must start on 4 floats)
+    const bool wt = AS::WT && f.field_mode == 3 && (kb & 3) == 0;
+    if constexpr (AS::WT) {
+      if (wt) {
+        constexpr int CH = S * L / 4;  // 16-byte pieces per x-plane
+        const float* tab = reinterpret_cast<const float*>(f.field) + kb + (size_t)c * S * L;
+        for (int e = tid; e < L * CH; e += Sh::THREADS) {
+          const int xx = e / CH, j = e - xx * CH;
+          const uint32_t d = smem_u32(wbuf + xx * S * L + 4 * j);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(tab + (size_t)xx * L * L + 4 * j)
+                       : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      }
+    }
     // ---- 1. k(p), forward DFT along y from the slab (L2): thread -> (xl, z)
     {
       const int z = tid % L, xl = tid / L;
@@ -1190,6 +1219,9 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
       fft::dft<L, -1, R, PK>(x);
 #pragma unroll
       for (int y = 0; y < L; ++y) sm[off(y / S, xl, y % S, z)] = x[y];
+    }
+    if constexpr (AS::WT) {
+      if (wt) asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's weight pieces have landed
     }
     __syncthreads();
     // ---- 2. forward DFT along z in place: thread -> (xl, y)
@@ -1282,8 +1314,14 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
           x[xx] = scale_w_zpos<R, PK>(f.zpos, site0 + xx * L * L, up, x[xx]);
         }
       } else if constexpr (FK == 2) {
+        if (AS::WT && wt) {
+          // the weights of this thread's pencil, from the staged rows
 #pragma unroll
-        for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
+          for (int xx = 0; xx < L; ++xx) x[xx] = scale_w1<R, PK>(x[xx], (R)wbuf[xx * S * L + yl * L + z]);
+        } else {
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
+        }
       }
       fft::dft<L, +1, R, PK>(x);
       const uint32_t my_bar = smem_u32(bar);
@@ -1354,10 +1392,10 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
   static_assert(KIND < 4 || KIND == 7 || KIND == 11 || sizeof(R) == 4,
                 "packed transforms and the resident k(p) slab are FP32");
   constexpr int THREADS = KIND == 1 ? SplitShape<R, L, C>::THREADS : Sh::THREADS;
-  constexpr size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
+  size_t SMEM = (KIND == 2 || KIND == 5)   ? BulkShape<R, L, C, true>::SMEM
                           : (KIND == 3 || KIND == 6) ? BulkShape<R, L, C, false>::SMEM
                           : (KIND == 9 || KIND == 10) ? BulkShape<R, L, C, false, true>::SMEM
-                          : (KIND >= 11) ? AsyncShape<R, L, C>::SMEM
+                          : (KIND >= 11) ? AsyncShape<R, L, C, 1>::SMEM
                           : (KIND == 7 || KIND == 8) ? PullShape<R, L, C, false>::SMEM
                                                      : Sh::SMEM;
   void (*kern)(FusedArgs);
@@ -1376,6 +1414,7 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
     // position factor) or any other field
     const bool z2 = f.field_mode == 1 && (L * L) % 32 == 0 && (f.pos == nullptr || f.zpos != nullptr);
     kern = z2 ? fused_step_async_kernel<R, L, C, KIND == 12, 1> : fused_step_async_kernel<R, L, C, KIND == 12, 2>;
+    if (!z2) SMEM = AsyncShape<R, L, C, 2>::SMEM;
   }
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
@@ -1684,6 +1723,8 @@ nrcps_status fused_choice(nrcps_context* ctx, nrcps_precision prec, int L, int* 
 nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const void* kin_table,
                         nrcps_precision prec, const nrcps_position_factor* w, int cluster, const void* zpos) {
   if (!fused_supported(prec, d)) return NRCPS_ERR_UNSUPPORTED;
+  // FP32 weight tables carry the whole factor: FP32 orbitals, no position factor
+  if (w->field_mode == 3 && (prec != NRCPS_F32 || w->dev_pos)) return NRCPS_ERR_UNSUPPORTED;
   FusedArgs f;
   f.psi = psi;
   f.n_orb_total = (long)batch * nconf;

@@ -26,7 +26,7 @@ struct PencilGeom {
 enum PencilOp { OP_NONE = 0, OP_PRE_MUL = 1, OP_POST_MUL = 2, OP_MID_FIELD = 3 };
 
 struct FieldArgs {
-  int mode;              // 0 complex fld, 1 Z2 bits, 2 interleaved complex phi
+  int mode;              // 0 complex fld, 1 Z2 bits, 2 interleaved complex phi, 3 real FP32 weights
   const void* field;
   uint64_t bit0;         // element (mode 0/2) or bit (mode 1) offset of configuration 0
   uint64_t conf_stride;  // elements or bits between configurations
@@ -48,6 +48,8 @@ __device__ __forceinline__ cplx<R> field_factor(const FieldArgs& f, long conf, l
     uint32_t word = reinterpret_cast<const uint32_t*>(f.field)[k >> 5];
     double phi = ((word >> (k & 31)) & 1u) ? 1.0 : -1.0;
     w = cplx<R>{(R)((1.0 + f.a * phi) / f.vol), (R)0};
+  } else if (f.mode == 3) {
+    w = cplx<R>{(R)reinterpret_cast<const float*>(f.field)[k], (R)0};
   } else {
     double2 phi = reinterpret_cast<const double2*>(f.field)[k];
     w = cplx<R>{(R)((1.0 + f.a * phi.x) / f.vol), (R)((f.a * phi.y) / f.vol)};

@@ -140,3 +140,36 @@ def test_device_batch_fp64_at_the_largest_uneven_shapes(golden):
         ref = g[f"dets{i}"]
         assert d.shape == ref.shape
         assert _rel(d, ref) < FP64_REL, (i, _rel(d, ref))
+
+
+@pytest.mark.gpu
+def test_device_batch_fp32_real_weight_table():
+    """FP32 batches with a real Gaussian field step on one FP32 weight per
+    site ("batch.real_weights" 1, the default), staged into shared memory by
+    the st.async fused step (kind 11): the same determinants, bit for bit, as
+    the kind-7 step reading the same table per site (L = 32, 48, the sizes
+    with a kind-7 variant), and within 1e-5 of the step that forms
+    (1 + a phi)/V per site from phi (option 0)."""
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    shell = {7: 1.5, 19: 2.5}
+    spec = [(48, 6, 7), (32, 8, 19), (24, 5, 7), (16, 8, 19)]
+    jobs = [nb.BatchJob(L=L, T=T, n_conf=2, fermi_energy=0.5 * (2 * np.pi / L) ** 2 * shell[N]) for L, T, N in spec]
+
+    def run(kind, table):
+        ctx.set_option("fused.kind", kind)
+        ctx.set_option("batch.real_weights", table)
+        try:
+            b = nb.Batch(jobs, seed=99, field="GAUSS", a=0.3, precision="f32", ctx=ctx)
+            out = [d.cpu().numpy() for d in b.run()]
+            b.close()
+        finally:
+            ctx.set_option("fused.kind", -1)
+            ctx.set_option("batch.real_weights", 1)
+        return out
+
+    staged, per_site, from_phi = run(11, 1), run(7, 1), run(11, 0)
+    for (L, T, N), s, p, g in zip(spec, staged, per_site, from_phi):
+        if L >= 32:
+            assert np.array_equal(s, p), (L, N)
+        assert _rel(s, g) < 1e-5, (L, N, _rel(s, g))

@@ -26,7 +26,7 @@
 
 namespace nrcps {
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
-                       const double* w, const int* opp, nrcps_precision prec, double* phi, bool opp_checked);
+                       const double* w, const int* opp, nrcps_precision prec, double* phi, int props);
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
                             const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec,
                             const void* zpos);
@@ -111,7 +111,7 @@ struct nrcps_branch {
   double* pos = nullptr;
   double* w = nullptr;
   int* opp = nullptr;
-  bool opp_involution = false;  // opp checked on the host: an involution of the sites
+  int pair_props = 3;  // the pair table's properties, checked on the host (pair_table_props)
   double* src2 = nullptr;
   double* phi = nullptr;         // nmax x 2 x 2 complex
   uint64_t* base = nullptr;
@@ -173,7 +173,7 @@ extern "C" nrcps_status nrcps_branch_create(nrcps_context* ctx, const nrcps_bran
     const float hi = (float)kinv[i];
     kf[i] = make_float2(hi, (float)(kinv[i] - (double)hi));
   }
-  b->opp_involution = is_involution(opposite, V);
+  b->pair_props = pair_table_props(opposite, w, V);
   nrcps_status st;
   if ((st = alloc(&b->psi[0], es * 2 * (size_t)b->nmax * V)) || (st = alloc(&b->psi[1], es * 2 * (size_t)b->nmax * V)) ||
       (st = alloc((void**)&b->kinv, 8 * V)) || (st = up(b->kinv, kinv.data(), 8 * V)) ||
@@ -247,7 +247,7 @@ extern "C" nrcps_status nrcps_branch_run(nrcps_branch* b, double* dev_corr) {
     const double inv_norm = 1.0 / std::pow((double)B, (double)(d + 1));
     for (int s = 0; s < p.steps; ++s) {
       const int t = d * p.steps + s;
-      NRCPS_TRY(pair_impl(ctx, b->psi[cur], b->psi[cur], 2, (int)nn, V, b->w, b->opp, prec, b->phi, b->opp_involution));
+      NRCPS_TRY(pair_impl(ctx, b->psi[cur], b->psi[cur], 2, (int)nn, V, b->w, b->opp, prec, b->phi, b->pair_props));
       branch_reduce_kernel<<<1, 256, 0, ctx->stream>>>(b->phi, nn, inv_norm, dev_corr + 2L * t);
       ctx->launches++;
       NRCPS_TRY(check_launch(ctx, "branch_reduce_kernel"));

@@ -142,11 +142,17 @@ nrcps_status overlap_tc_prepare(nrcps_context* ctx, const double* src, int ns, l
 nrcps_status overlap_tc(nrcps_context* ctx, const float* split, int ns, const void* psi, int nt, int nconf, long vol,
                         double* S);
 
-// true when opp (host) is an involution of [0, vol), as TwoBody's parity mirror is
-inline bool is_involution(const int* opp, long vol) {
-  for (long i = 0; i < vol; ++i)
-    if (opp[i] < 0 || opp[i] >= vol || opp[opp[i]] != i) return false;
-  return true;
+// The pair kernels' view of a TwoBody table (host copies): bit 0 set unless
+// opp is an involution of [0, vol) (TwoBody's parity mirror is), bit 1 set
+// unless also w(opp(i)) = w(i) for every site (TwoBody's weights are)
+inline int pair_table_props(const int* opp, const double* w, long vol) {
+  int props = 0;
+  for (long i = 0; i < vol; ++i) {
+    if (opp[i] < 0 || opp[i] >= vol) return 3;
+    if (opp[opp[i]] != i) props |= 1;
+    if (w[opp[i]] != w[i]) props |= 2;
+  }
+  return props & 1 ? 3 : props;
 }
 
 inline unsigned grid_for(long n, int block, long cap = 148L * 64) {

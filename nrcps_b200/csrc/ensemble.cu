@@ -25,7 +25,7 @@ nrcps_status overlap_impl(nrcps_context* ctx, const double* src, int ns, const v
 nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const void* psi, int nt, int nconf, long vol,
                          nrcps_precision prec, double* S);
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
-                       const double* w, const int* opp, nrcps_precision prec, double* phi, bool opp_checked);
+                       const double* w, const int* opp, nrcps_precision prec, double* phi, int props);
 nrcps_status propagate_impl(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const double* kin,
                             const float2* kin_f32, const nrcps_position_factor* w, nrcps_precision prec,
                             const void* zpos);
@@ -53,7 +53,7 @@ struct nrcps_ensemble {
   double* itab = nullptr;
   double* w = nullptr;
   int* opp = nullptr;
-  bool opp_involution = false;  // opp checked on the host: an involution of the sites
+  int pair_props = 3;  // the pair table's properties, checked on the host (pair_table_props)
   uint32_t* bits = nullptr;   // Z2 fields of a run
   double* phi = nullptr;      // other fields of a run (interleaved complex)
   double* fld = nullptr;      // non-local interaction factor of one slice
@@ -161,7 +161,7 @@ static nrcps_status record_time_loop(nrcps_ensemble* e, double* dets) {
       if (e->qr_logR && t >= j.qr_period)
         NRCPS_TRY(rescale_dets(ctx, dets, e->qr_logR, N, nc, 2L * T * e->nmeas, 2L * t * e->nmeas, 0));
     } else {
-      NRCPS_TRY(pair_impl(ctx, e->psi, e->psi, N, nc, vol, e->w, e->opp, prec, e->S, e->opp_involution));
+      NRCPS_TRY(pair_impl(ctx, e->psi, e->psi, N, nc, vol, e->w, e->opp, prec, e->S, e->pair_props));
       if (e->pw_index) NRCPS_TRY(gather_impl(ctx, e->pw_index, N, e->psi, N, nc, vol, prec, e->P1));
       else if (e->src_split) NRCPS_TRY(overlap_tc(ctx, e->src_split, N, e->psi, N, nc, vol, e->P1));
       else NRCPS_TRY(overlap_impl(ctx, e->src, N, e->psi, N, nc, vol, prec, e->P1));
@@ -283,7 +283,7 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   if (job->mode == 1) {
     if ((st = dalloc(ctx, &e->w, 8 * V)) || (st = upload(ctx, e->w, w, 8 * V))) return fail(st);
     if ((st = dalloc(ctx, &e->opp, 4 * V)) || (st = upload(ctx, e->opp, opposite, 4 * V))) return fail(st);
-    e->opp_involution = is_involution(opposite, V);
+    e->pair_props = pair_table_props(opposite, w, V);
     if ((st = dalloc(ctx, &e->P1, 16 * (size_t)nc * N * N))) return fail(st);
   }
   const uint64_t sites = (uint64_t)nc * job->T * V;

@@ -141,6 +141,11 @@ __global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1
 // slots of every tile, in R within a tile and in FP64 across tiles; the
 // groups are summed in shared memory and the cluster's CTAs in rank order
 // through distributed shared memory: the result does not depend on timing.
+//
+// With psi1 = psi2 and a weight even under the pairing (w(opp(i)) = w(i),
+// TwoBody's tables), the pair of terms of i and opp(i) is symmetric in
+// (s, t), so phi is: only the blocks on and above the diagonal are summed
+// and each is written to both triangles.
 constexpr int PAIR_THREADS = 256;
 constexpr int PAIR_MAXN = 32;
 constexpr int PB = 2;                // register block: PB x PB complex pair-matrix entries per thread
@@ -164,11 +169,71 @@ struct PairShape {
   }
 };
 
+// Block blk of the upper triangle (row-major, bi <= bj) or of the full
+// nb x nb grid
+__device__ __forceinline__ void pair_block(int blk, int nb, bool sym, int& bi, int& bj) {
+  if (!sym) {
+    bi = blk / nb;
+    bj = blk % nb;
+    return;
+  }
+  bi = 0;
+  while (blk >= nb - bi) {
+    blk -= nb - bi;
+    ++bi;
+  }
+  bj = bi + blk;
+}
+
+// The end of a tiled pair kernel: the groups of every block summed in shared
+// memory (fixed order), then the cluster's CTAs in rank order through
+// distributed shared memory, written by rank 0 (to both triangles for the
+// symmetric form).
+__device__ __forceinline__ void pair_reduce_store(const double (&acc)[PB][PB][2], unsigned char* smem, int n,
+                                                  int nb, bool sym, int nblk, int groups, int g, int blk,
+                                                  bool active, long conf, double* __restrict__ phi) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int split = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
+  __syncthreads();
+  double* red = reinterpret_cast<double*>(smem);  // [nblk][PAIR_E], over the staged tiles
+  for (int gg = 0; gg < groups; ++gg) {
+    if (active && g == gg) {
+#pragma unroll
+      for (int a = 0; a < PB; ++a)
+#pragma unroll
+        for (int b = 0; b < PB; ++b)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const int e = blk * PAIR_E + (a * PB + b) * 2 + c;
+            red[e] = (gg == 0 ? 0.0 : red[e]) + acc[a][b][c];
+          }
+    }
+    __syncthreads();
+  }
+  cluster.sync();  // every CTA's sums are in its shared memory
+  if (rank == 0) {
+    for (int e = threadIdx.x; e < nblk * PAIR_E; e += PAIR_THREADS) {
+      double v = 0.0;
+      for (int r2 = 0; r2 < split; ++r2) v += cluster.map_shared_rank(red, r2)[e];
+      const int k = e % PAIR_E;
+      int bi, bj;
+      pair_block(e / PAIR_E, nb, sym, bi, bj);
+      const int s = PB * bi + (k / 2) / PB, t = PB * bj + (k / 2) % PB;
+      // (the symmetric form writes each entry with s <= t to both places)
+      if (s < n && t < n && (!sym || s <= t)) {
+        phi[2 * ((conf * n + s) * (long)n + t) + (k & 1)] = v;
+        if (sym && s != t) phi[2 * ((conf * n + t) * (long)n + s) + (k & 1)] = v;
+      }
+    }
+  }
+  cluster.sync();  // peers keep their shared memory until rank 0 has read it
+}
+
 template <typename R>
 __global__ void __launch_bounds__(PAIR_THREADS, 4)
     pair_tile_kernel(const void* __restrict__ psi1, const void* __restrict__ psi2, int n, long vol,
-                     const double* __restrict__ w, const int* __restrict__ opp, const int* __restrict__ bad_opp,
-                     int ts, double* __restrict__ phi) {
+                     const double* __restrict__ w, const int* __restrict__ opp, const int* __restrict__ flags,
+                     int host_flags, int ts, double* __restrict__ phi) {
   extern __shared__ __align__(16) unsigned char pair_smem[];
   const int LD = 2 * ts + 1;
   const int nb = (n + PB - 1) / PB, rows = nb * PB;
@@ -179,16 +244,22 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
   const long conf = blockIdx.x / split;
   const cplx<R>* p1 = reinterpret_cast<const cplx<R>*>(psi1) + (size_t)conf * n * vol;
   const cplx<R>* p2 = reinterpret_cast<const cplx<R>*>(psi2) + (size_t)conf * n * vol;
-  const bool paired = !(bad_opp && *bad_opp);
+  // the table's properties: bit 0 opp is no involution, bit 1 w is not even
+  // under opp (from the device check when there is one)
+  const int fl = flags ? *flags : host_flags;
+  const bool paired = !(fl & 1);
+  const bool sym = paired && !(fl & 2) && psi1 == psi2;
   // staging: thread -> (slot q of the tile, orbital lane)
   const int q = threadIdx.x % ts, olane = threadIdx.x / ts, ostride = PAIR_THREADS / ts;
   // accumulation: thread -> (PB x PB block, group), blocks fastest: the
   // lanes of a warp read one slot of at most 2 nb rows, in distinct banks
-  const int nblk = nb * nb;
+  const int nblk = sym ? nb * (nb + 1) / 2 : nb * nb;
   const int groups = PAIR_THREADS / nblk;  // >= 1 for n <= 32
   const int g = threadIdx.x / nblk, blk = threadIdx.x % nblk;
   const bool active = g < groups;
-  const int abase = (active ? blk / nb : 0) * PB * LD, bbase = (active ? blk % nb : 0) * PB * LD;
+  int bi = 0, bj = 0;
+  if (active) pair_block(blk, nb, sym, bi, bj);
+  const int abase = bi * PB * LD, bbase = bj * PB * LD;
   for (int e = threadIdx.x; e < (rows - n) * LD; e += PAIR_THREADS) {  // the padding row stays zero
     A[n * LD + e] = cplx<R>{(R)0, (R)0};
     B[n * LD + e] = cplx<R>{(R)0, (R)0};
@@ -261,42 +332,21 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
         }
     }
   }
-  // sum the groups of every block in shared memory (fixed order), then the
-  // cluster's CTAs in rank order
-  __syncthreads();
-  double* red = reinterpret_cast<double*>(pair_smem);  // [nblk][PAIR_E], over the staged tiles
-  for (int gg = 0; gg < groups; ++gg) {
-    if (active && g == gg) {
-#pragma unroll
-      for (int a = 0; a < PB; ++a)
-#pragma unroll
-        for (int b = 0; b < PB; ++b)
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            const int e = blk * PAIR_E + (a * PB + b) * 2 + c;
-            red[e] = (gg == 0 ? 0.0 : red[e]) + acc[a][b][c];
-          }
-    }
-    __syncthreads();
-  }
-  cluster.sync();  // every CTA's sums are in its shared memory
-  if (rank == 0) {
-    for (int e = threadIdx.x; e < nblk * PAIR_E; e += PAIR_THREADS) {
-      double v = 0.0;
-      for (int r2 = 0; r2 < split; ++r2) v += cluster.map_shared_rank(red, r2)[e];
-      const int b = e / PAIR_E, k = e % PAIR_E;
-      const int s = PB * (b / nb) + (k / 2) / PB, t = PB * (b % nb) + (k / 2) % PB;
-      if (s < n && t < n) phi[2 * ((conf * n + s) * (long)n + t) + (k & 1)] = v;
-    }
-  }
-  cluster.sync();  // peers keep their shared memory until rank 0 has read it
+  pair_reduce_store(acc, pair_smem, n, nb, sym, nblk, groups, g, blk, active, conf, phi);
 }
 
-// *bad = 1 unless opp is an involution of [0, vol) (TwoBody's parity mirror is)
-__global__ void opp_involution_check_kernel(const int* __restrict__ opp, long vol, int* bad) {
+// *flags |= 1 unless opp is an involution of [0, vol) (TwoBody's parity
+// mirror is), |= 2 unless w(opp(i)) = w(i) for every i
+__global__ void opp_involution_check_kernel(const int* __restrict__ opp, const double* __restrict__ w, long vol,
+                                            int* flags) {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < vol; i += (long)gridDim.x * blockDim.x) {
     const int j = opp[i];
-    if (j < 0 || j >= vol || opp[j] != i) *bad = 1;
+    if (j < 0 || j >= vol) {
+      atomicOr(flags, 3);
+    } else {
+      if (opp[j] != i) atomicOr(flags, 1);
+      if (w[j] != w[i]) atomicOr(flags, 2);
+    }
   }
 }
 
@@ -735,7 +785,8 @@ nrcps_status gather_impl(nrcps_context* ctx, const int* index, int ns, const voi
 
 template <typename R>
 static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf,
-                                     long vol, const double* w, const int* opp, const int* bad_opp, double* phi) {
+                                     long vol, const double* w, const int* opp, const int* flags, int host_flags,
+                                     double* phi) {
   using Sh = PairShape<R>;
   const int ts = Sh::ts(n);
   const size_t smem = Sh::smem(n);
@@ -767,28 +818,30 @@ static nrcps_status launch_pair_tile(nrcps_context* ctx, const void* psi1, const
   cfg.stream = ctx->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, pair_tile_kernel<R>, psi1, psi2, n, vol, w, opp, bad_opp, ts, phi);
+  cudaError_t e =
+      cudaLaunchKernelEx(&cfg, pair_tile_kernel<R>, psi1, psi2, n, vol, w, opp, flags, host_flags, ts, phi);
   ctx->launches++;
   return check_cuda(ctx, e, "pair_tile_kernel launch");
 }
 
-// opp_checked: the caller has checked on the host that opp is an
-// involution of [0, vol); otherwise the device checks it before the tiles.
+// props: the table's properties as the caller checked them on the host
+// (pair_table_props), or -1: the device checks them before the tiles.
 nrcps_status pair_impl(nrcps_context* ctx, const void* psi1, const void* psi2, int n, int nconf, long vol,
-                       const double* w, const int* opp, nrcps_precision prec, double* phi, bool opp_checked) {
+                       const double* w, const int* opp, nrcps_precision prec, double* phi, int props) {
   long blocks = (long)nconf * n * n;
   if (blocks == 0) return NRCPS_OK;
   if (n <= PAIR_MAXN && ctx->pair_tile && (long)nconf * 8 < (1L << 31)) {
-    const int* bad = nullptr;
-    if (!opp_checked) {
+    const int* flags = nullptr;
+    if (props < 0) {
       NRCPS_TRY(check_cuda(ctx, cudaMemsetAsync(ctx->dev_pair_flag, 0, sizeof(int), ctx->stream), "pair flag"));
-      opp_involution_check_kernel<<<grid_for(vol, 256), 256, 0, ctx->stream>>>(opp, vol, ctx->dev_pair_flag);
+      opp_involution_check_kernel<<<grid_for(vol, 256), 256, 0, ctx->stream>>>(opp, w, vol, ctx->dev_pair_flag);
       ctx->launches++;
       NRCPS_TRY(check_launch(ctx, "opp_involution_check_kernel"));
-      bad = ctx->dev_pair_flag;
+      flags = ctx->dev_pair_flag;
     }
-    if (prec == NRCPS_F64) return launch_pair_tile<double>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
-    return launch_pair_tile<float>(ctx, psi1, psi2, n, nconf, vol, w, opp, bad, phi);
+    if (prec == NRCPS_F64)
+      return launch_pair_tile<double>(ctx, psi1, psi2, n, nconf, vol, w, opp, flags, props, phi);
+    return launch_pair_tile<float>(ctx, psi1, psi2, n, nconf, vol, w, opp, flags, props, phi);
   }
   if (prec == NRCPS_F64) pair_kernel<double><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
   else pair_kernel<float><<<(unsigned)blocks, 256, 0, ctx->stream>>>(psi1, psi2, n, vol, w, opp, phi);
@@ -841,7 +894,7 @@ extern "C" nrcps_status nrcps_pair_matrix(nrcps_context* ctx, const void* dev_ps
   NRCPS_REQUIRE(ctx, n >= 0 && nconf >= 0 && vol > 0, "nrcps_pair_matrix: bad arguments");
   if ((long)n * nconf == 0) return NRCPS_OK;
   NRCPS_REQUIRE(ctx, dev_psi1 && dev_psi2 && dev_w && dev_opposite && dev_phi, "nrcps_pair_matrix: null pointer");
-  return pair_impl(ctx, dev_psi1, dev_psi2, n, nconf, vol, dev_w, dev_opposite, prec, dev_phi, false);
+  return pair_impl(ctx, dev_psi1, dev_psi2, n, nconf, vol, dev_w, dev_opposite, prec, dev_phi, -1);
 }
 
 extern "C" nrcps_status nrcps_shifted_pair_matrix(nrcps_context* ctx, const void* dev_psi1, const void* dev_psi2,

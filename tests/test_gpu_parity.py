@@ -244,6 +244,39 @@ def test_pair_matrix_tiles_match_oracle(ctx, n, dims, nconf):
                 ctx.set_option("pair.tile", 1)
 
 
+@pytest.mark.parametrize("n,dims,nconf,even", [(1, (8, 8, 8), 3, True), (10, (12, 12, 12), 300, True),
+                                               (19, (8, 8, 8), 2, True), (32, (8, 8, 8), 3, True),
+                                               (10, (8, 8, 8), 3, False)])
+def test_pair_matrix_of_one_set_of_orbitals(ctx, n, dims, nconf, even):
+    """psi1 = psi2 (the ensemble's pair sink) with TwoBody's weights, even
+    under the pairing: the tiled kernel sums only the blocks on and above the
+    diagonal and mirrors them; with weights that are not even (random) the
+    device check turns that off.  Against the oracle: FP64 within 1e-12, FP32
+    orbitals within 1e-6."""
+    rs = np.random.default_rng(n + nconf + 7)
+    vol = int(np.prod(dims))
+    psi = rs.standard_normal((nconf, n, vol)) + 1j * rs.standard_normal((nconf, n, vol))
+    tb = nb.TwoBody(dims, "TGND", "STANDARD", 1.0, 0.176776695, 0.99999, ctx)
+    w = tb.w_host if even else rs.uniform(0.0, 1.0, vol)
+    assert np.array_equal(w[tb.opp_host], w) == even
+    wd = torch.from_numpy(np.ascontiguousarray(w)).to(ctx.device)
+    od = torch.from_numpy(np.ascontiguousarray(tb.opp_host.astype(np.int32))).to(ctx.device)
+    for dt, tol, prec in ((torch.complex128, FP64_REL, C.F64), (torch.complex64, 1e-6, C.F32)):
+        p = torch.from_numpy(psi).to(ctx.device).to(dt)
+        out = torch.empty((nconf, n, n), dtype=torch.complex128, device=ctx.device)
+        ctx.check(nb.lib().nrcps_pair_matrix(ctx.handle, ctypes.c_void_p(p.data_ptr()), ctypes.c_void_p(p.data_ptr()),
+                                             n, nconf, vol, ctypes.c_void_p(wd.data_ptr()),
+                                             ctypes.c_void_p(od.data_ptr()), prec, ctypes.c_void_p(out.data_ptr())),
+                  "pair_matrix")
+        got = out.cpu().numpy()
+        for c in sorted({0, nconf - 1}):
+            pc = p[c].cpu().numpy().astype(np.complex128)
+            r = O.pair_matrix(pc, pc, w, tb.opp_host)
+            assert max_norm_err(got[c], r) < tol, (dt, c)
+            if even:
+                assert np.array_equal(got[c], got[c].T)
+
+
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 def test_pair_matrix_with_a_table_that_is_no_involution(ctx, precision):
     """The tiled kernel pairs each site with its opposite (opp(opp(i)) = i,

@@ -246,13 +246,16 @@ nrcps_status nrcps_interaction_evolve(nrcps_context *ctx, void *psi, int batch, 
  * conf*conf_stride + site):
  *   0: complex FP64 fld (Interaction::Initialize output), element k of dev_field;
  *   1: Z2 bits: fld = (1 + a*phi)/V with phi = +1 when bit k of dev_field is set;
- *   2: interleaved complex FP64 phi (Lattice::Get layout), fld = (1 + a*phi)/V.
+ *   2: interleaved complex FP64 phi (Lattice::Get layout), fld = (1 + a*phi)/V;
+ *   3: one real FP32 weight per site, element k of dev_field (float), the
+ *      whole factor (a and P unused: dev_pos must be NULL); for a real
+ *      field made once per run, as nrcps_batch does for FP32 orbitals.
  * Mathematically identical to the reference's sequence (F*B = V). */
 typedef struct {
   int field_mode;
   const void *dev_field;
-  uint64_t bit0;        /* element (mode 0/2) or bit (mode 1) offset of configuration 0 */
-  uint64_t conf_stride; /* elements (mode 0/2) or bits (mode 1) between configurations */
+  uint64_t bit0;        /* element (mode 0/2/3) or bit (mode 1) offset of configuration 0 */
+  uint64_t conf_stride; /* elements (mode 0/2/3) or bits (mode 1) between configurations */
   double a;
   const double *dev_pos; /* may be NULL */
   /* may be NULL; else a device array of nconf offsets that replaces

@@ -416,7 +416,8 @@ extern "C" nrcps_status nrcps_propagate(nrcps_context* ctx, void* psi, int batch
   if (!ctx) return NRCPS_ERR_INVALID_ARGUMENT;
   NRCPS_REQUIRE(ctx, (psi || nconf == 0) && dims && dev_kin && w && w->dev_field && batch > 0 && nconf >= 0,
                 "nrcps_propagate: bad arguments");
-  NRCPS_REQUIRE(ctx, w->field_mode >= 0 && w->field_mode <= 2, "nrcps_propagate: bad field_mode");
+  NRCPS_REQUIRE(ctx, w->field_mode >= 0 && w->field_mode <= 3, "nrcps_propagate: bad field_mode");
+  NRCPS_REQUIRE(ctx, w->field_mode != 3 || !w->dev_pos, "nrcps_propagate: field_mode 3 carries the whole factor");
   NRCPS_TRY(check_dims(ctx, dims));
   if (nconf == 0) return NRCPS_OK;
   return propagate_impl(ctx, psi, batch, nconf, dims, dev_kin, nullptr, w, prec, nullptr);

@@ -65,11 +65,14 @@ def bench_step(ctx: Context, L: int, orbitals: int, precision: str, kind: int, c
                       device=ctx.device)
     kinv = torch.from_numpy(1.0 / kinetic_table(dims, "PERFECT", 1.0, 0.5, 2.0)).to(ctx.device)
     pf = C.PositionFactor()
-    if field == "gauss":  # Gaussian phi, a = 0.3: the general position-factor path
+    if field in ("gauss", "wtab"):  # Gaussian phi, a = 0.3: the general position-factor path
         from .api import draw_fields
         fld, _ = draw_fields("RANLXS2", 7, "GAUSS", L ** 3, nconf, 0, ctx)
         pf.field_mode, pf.dev_field, pf.bit0, pf.conf_stride = 2, fld.data_ptr(), 0, L ** 3
         pf.a, pf.dev_pos = 0.3, None
+        if field == "wtab":  # the same field as one FP32 weight (1 + a phi)/V per site
+            fld = ((1.0 + 0.3 * fld.reshape(-1, 2)[:, 0]) / L ** 3).to(torch.float32).contiguous()
+            pf.field_mode, pf.dev_field = 3, fld.data_ptr()
     else:
         fld = draw_z2_bits("RANLXS2", 7, 0, nconf * L ** 3, ctx)
         pf.field_mode, pf.dev_field, pf.bit0, pf.conf_stride = 1, fld.data_ptr(), 0, L ** 3
@@ -191,7 +194,8 @@ def main(argv=None) -> int:
     ap.add_argument("what", choices=["step", "overlap", "dets", "cv", "qr", "rng", "pair"])
     ap.add_argument("--gram-tc", type=int, default=0)
     ap.add_argument("--pair-tile", type=int, default=1)
-    ap.add_argument("--field", default="z2", choices=["z2", "gauss"], help="step: Z2 bits or Gaussian phi")
+    ap.add_argument("--field", default="z2", choices=["z2", "gauss", "wtab"],
+                    help="step: Z2 bits, Gaussian phi, or the Gaussian field as FP32 weights per site")
     ap.add_argument("--L", type=int, default=32)
     ap.add_argument("--orbitals", type=int, default=19456)
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])

@@ -549,6 +549,24 @@ def _random_step_inputs(ctx, L, nconf, batch, precision, seed=0):
     return torch.from_numpy(psi).to(dt).to(ctx.device), kinv, bits
 
 
+@pytest.mark.parametrize("L,precision", [(16, "f32"), (24, "f32"), (32, "f32"), (48, "f32"), (12, "f32"),
+                                         (16, "f64")])
+def test_real_weight_table_field(ctx, L, precision):
+    """Field mode 3: the Gaussian field as one FP32 weight (1 + a phi)/V per
+    site, against mode 2 forming it from phi per site: within 2e-6 of the
+    orbitals' norm after one step (the weight rounded to FP32 once), in the
+    fused step (FP32; staged in shared memory by kind 11) and in the pencil
+    passes (L = 12, and FP64)."""
+    nconf, batch = 3, 2
+    psi, kinv, _ = _random_step_inputs(ctx, L, nconf, batch, precision, seed=3)
+    phi, _ = nb.draw_fields("RANLXS2", 11, "GAUSS", L ** 3, nconf, 0, ctx)
+    wt = ((1.0 + 0.3 * phi[..., 0]) / L ** 3).to(torch.float32).contiguous()
+    a, b = psi.clone(), psi.clone()
+    nb.propagate(a, batch, kinv, phi, 0.3, field_mode=2, ctx=ctx)
+    nb.propagate(b, batch, kinv, wt, 0.0, field_mode=3, ctx=ctx)
+    assert max_norm_err(b.cpu().numpy(), a.cpu().numpy()) < 2e-6
+
+
 @pytest.mark.parametrize("L,precision", [(8, "f32"), (16, "f32"), (24, "f32"), (32, "f32"), (48, "f32"),
                                          (8, "f64"), (16, "f64"), (24, "f64"), (32, "f64")])
 def test_fused_step_matches_pencil_passes(ctx, L, precision):

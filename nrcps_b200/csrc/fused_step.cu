@@ -1184,8 +1184,10 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
     }
     // a real weight table (field mode 3): the CTA's rows of every x-plane,
     // S L floats each, copied by cp.async while pass 1 runs (16-byte pieces:
-    // the configuration's table must start on 4 floats)
-    const bool wt = AS::WT && f.field_mode == 3 && (kb & 3) == 0;
+    // the table must start on 16 bytes and the configuration's part of it on
+    // 4 floats; otherwise pass 3 reads the weights per site)
+    const bool wt = AS::WT && f.field_mode == 3 && (kb & 3) == 0 &&
+                    (reinterpret_cast<uintptr_t>(f.field) & 15) == 0;
     if constexpr (AS::WT) {
       if (wt) {
         constexpr int CH = S * L / 4;  // 16-byte pieces per x-plane

@@ -555,8 +555,9 @@ def test_real_weight_table_field(ctx, L, precision):
     """Field mode 3: the Gaussian field as one FP32 weight (1 + a phi)/V per
     site, against mode 2 forming it from phi per site: within 2e-6 of the
     orbitals' norm after one step (the weight rounded to FP32 once), in the
-    fused step (FP32; staged in shared memory by kind 11) and in the pencil
-    passes (L = 12, and FP64)."""
+    fused step (FP32; staged in shared memory by kind 11, or read per site
+    from a table that is not 16-byte aligned) and in the pencil passes
+    (L = 12, and FP64)."""
     nconf, batch = 3, 2
     psi, kinv, _ = _random_step_inputs(ctx, L, nconf, batch, precision, seed=3)
     phi, _ = nb.draw_fields("RANLXS2", 11, "GAUSS", L ** 3, nconf, 0, ctx)
@@ -565,6 +566,14 @@ def test_real_weight_table_field(ctx, L, precision):
     nb.propagate(a, batch, kinv, phi, 0.3, field_mode=2, ctx=ctx)
     nb.propagate(b, batch, kinv, wt, 0.0, field_mode=3, ctx=ctx)
     assert max_norm_err(b.cpu().numpy(), a.cpu().numpy()) < 2e-6
+    # a table that starts 4 bytes past a 16-byte boundary: the weights are
+    # read per site instead of staged, the same products
+    buf = torch.zeros(wt.numel() + 1, dtype=torch.float32, device=ctx.device)
+    buf[1:] = wt.reshape(-1)
+    c = psi.clone()
+    nb.propagate(c, batch, kinv, buf[1:], 0.0, field_mode=3, ctx=ctx)
+    assert buf[1:].data_ptr() % 16 == 4
+    assert torch.equal(c, b)
 
 
 @pytest.mark.parametrize("L,precision", [(8, "f32"), (16, "f32"), (24, "f32"), (32, "f32"), (48, "f32"),

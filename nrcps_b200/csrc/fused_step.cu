@@ -1725,6 +1725,10 @@ nrcps_status fused_choice(nrcps_context* ctx, nrcps_precision prec, int L, int* 
 nrcps_status fused_step(nrcps_context* ctx, void* psi, int batch, int nconf, const int d[3], const void* kin_table,
                         nrcps_precision prec, const nrcps_position_factor* w, int cluster, const void* zpos) {
   if (!fused_supported(prec, d)) return NRCPS_ERR_UNSUPPORTED;
+  // the bulk-copy kinds move slabs of psi in 16-byte units: a psi that does
+  // not start on 16 bytes (a caller's view at an odd FP32 element) takes the
+  // pencil passes
+  if (reinterpret_cast<uintptr_t>(psi) & 15) return NRCPS_ERR_UNSUPPORTED;
   // FP32 weight tables carry the whole factor: FP32 orbitals, no position factor
   if (w->field_mode == 3 && (prec != NRCPS_F32 || w->dev_pos)) return NRCPS_ERR_UNSUPPORTED;
   FusedArgs f;

@@ -576,6 +576,27 @@ def test_real_weight_table_field(ctx, L, precision):
     assert torch.equal(c, b)
 
 
+@pytest.mark.parametrize("L", [8, 16, 32])
+def test_orbitals_off_a_16_byte_boundary_take_the_pencil_passes(ctx, L):
+    """FP32 orbitals whose array starts 8 bytes past a 16-byte boundary (a
+    view at an odd element): the fused kinds that move slabs by bulk copy
+    need 16-byte starts, so such a call takes the pencil passes -- the same
+    values as the pencil passes on an aligned copy."""
+    psi, kinv, bits = _random_step_inputs(ctx, L, 2, 3, "f32", seed=4)
+    buf = torch.zeros(psi.numel() + 1, dtype=psi.dtype, device=ctx.device)
+    buf[1:] = psi.reshape(-1)
+    view = buf[1:].view(psi.shape)
+    assert view.data_ptr() % 16 == 8
+    nb.propagate(view, 3, kinv, bits, 0.5, ctx=ctx)
+    ref = psi.clone()
+    ctx.set_option("propagate.fused", 0)
+    try:
+        nb.propagate(ref, 3, kinv, bits, 0.5, ctx=ctx)
+    finally:
+        ctx.set_option("propagate.fused", 1)
+    assert torch.equal(view, ref)
+
+
 @pytest.mark.parametrize("L,precision", [(8, "f32"), (16, "f32"), (24, "f32"), (32, "f32"), (48, "f32"),
                                          (8, "f64"), (16, "f64"), (24, "f64"), (32, "f64")])
 def test_fused_step_matches_pencil_passes(ctx, L, precision):

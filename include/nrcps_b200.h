@@ -281,7 +281,9 @@ nrcps_status nrcps_overlap_planewave(nrcps_context *ctx, const int *dev_index, i
                                      const void *dev_psi, int nt, int nconf, long vol,
                                      nrcps_precision prec, double *dev_S);
 /* TwoBody::Run (src/two_body/noarch/two_body_run.C:16-43): phi[c][s][t] =
- * sum_i w_i psi1_{c,s}(i) psi2_{c,t}(opp(i)), no conjugation. */
+ * sum_i w_i psi1_{c,s}(i) psi2_{c,t}(opp(i)), no conjugation.  A site whose
+ * opp(i) lies outside [0, vol) contributes nothing (the reference's tables
+ * have none). */
 nrcps_status nrcps_pair_matrix(nrcps_context *ctx, const void *dev_psi1, const void *dev_psi2, int n,
                                int nconf, long vol, const double *dev_w, const int *dev_opposite,
                                nrcps_precision prec, double *dev_phi);

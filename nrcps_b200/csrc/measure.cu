@@ -97,7 +97,9 @@ __global__ void __launch_bounds__(256) pair_kernel(const void* __restrict__ psi1
   const char* b = reinterpret_cast<const char*>(psi2) + (size_t)(conf * n + t) * vol * 2 * sizeof(R);
   double re = 0.0, im = 0.0;
   for (long i = threadIdx.x; i < vol; i += blockDim.x) {
-    cplx<R> x = ld<R>(a, i), y = ld<R>(b, opp[i]);
+    const int j = opp[i];
+    if (j < 0 || j >= vol) continue;  // a partner outside the lattice contributes nothing
+    cplx<R> x = ld<R>(a, i), y = ld<R>(b, j);
     double wi = w[i];
     re += ((double)x.re * y.re - (double)x.im * y.im) * wi;
     im += ((double)x.re * y.im + (double)x.im * y.re) * wi;
@@ -274,7 +276,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     const long i = tile * ts + q;
     const bool valid = i < vol;
     const long j = valid ? (long)__ldg(opp + i) : 0;
-    const bool take = valid && (!paired || i <= j);
+    // (the plain gather skips a partner outside the lattice; a paired table
+    // has none)
+    const bool take = valid && (paired ? i <= j : (j >= 0 && j < vol));
     const bool second = paired && valid && i < j;
     // also the barrier after the previous tile's accumulation
     if (!__syncthreads_or(take)) continue;
@@ -371,7 +375,9 @@ __global__ void __launch_bounds__(256) shifted_pair_kernel(const void* __restric
     const int* sh = shift + (size_t)l * vol;
     const double* w = wl + (size_t)l * vol;
     for (long i = threadIdx.x; i < vol; i += blockDim.x) {
-      cplx<R> x = ld<R>(a, sh[i]), y = ld<R>(b, opp[i]);
+      const int si = sh[i], j = opp[i];
+      if (si < 0 || si >= vol || j < 0 || j >= vol) continue;  // outside the lattice: no term
+      cplx<R> x = ld<R>(a, si), y = ld<R>(b, j);
       const double wi = w[i];
       re += ((double)x.re * y.re - (double)x.im * y.im) * wi;
       im += ((double)x.re * y.im + (double)x.im * y.re) * wi;

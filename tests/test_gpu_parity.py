@@ -308,6 +308,44 @@ def test_pair_matrix_with_a_table_that_is_no_involution(ctx, precision):
         assert max_norm_err(got[c], r) < tol
 
 
+@pytest.mark.parametrize("tile", [1, 0])
+def test_pair_matrix_skips_partners_outside_the_lattice(ctx, tile):
+    """nrcps_pair_matrix with an opposite-site table holding indices outside
+    [0, vol) (-1 and vol): those sites contribute nothing, in the tiled and
+    the per-pair kernels, and nothing is read out of bounds."""
+    rs = np.random.default_rng(5)
+    dims, n, nconf = (8, 8, 8), 6, 2
+    vol = int(np.prod(dims))
+    psi1 = rs.standard_normal((nconf, n, vol)) + 1j * rs.standard_normal((nconf, n, vol))
+    psi2 = rs.standard_normal((nconf, n, vol)) + 1j * rs.standard_normal((nconf, n, vol))
+    w = rs.uniform(0.0, 1.0, vol)
+    opp = rs.permutation(vol).astype(np.int32)
+    bad = rs.choice(vol, 20, replace=False)
+    opp[bad[:10]] = -1
+    opp[bad[10:]] = vol
+    p1 = torch.from_numpy(psi1).to(ctx.device)
+    p2 = torch.from_numpy(psi2).to(ctx.device)
+    out = torch.empty((nconf, n, n), dtype=torch.complex128, device=ctx.device)
+    wd = torch.from_numpy(w).to(ctx.device)
+    od = torch.from_numpy(opp).to(ctx.device)
+    ctx.set_option("pair.tile", tile)
+    try:
+        ctx.check(nb.lib().nrcps_pair_matrix(ctx.handle, ctypes.c_void_p(p1.data_ptr()),
+                                             ctypes.c_void_p(p2.data_ptr()), n, nconf, vol,
+                                             ctypes.c_void_p(wd.data_ptr()), ctypes.c_void_p(od.data_ptr()), C.F64,
+                                             ctypes.c_void_p(out.data_ptr())),
+                  "pair_matrix")
+        ctx.synchronize()
+    finally:
+        ctx.set_option("pair.tile", 1)
+    keep = (opp >= 0) & (opp < vol)
+    w0 = np.where(keep, w, 0.0)
+    opp0 = np.where(keep, opp, 0)
+    got = out.cpu().numpy()
+    for c in range(nconf):
+        assert max_norm_err(got[c], O.pair_matrix(psi1[c], psi2[c], w0, opp0)) < FP64_REL
+
+
 def test_lu_cases_match_reference(golden, ctx):
     """Determinants against ludcmp: 1e-12 relative, or 1e-13 of the Hadamard
     bound (product of row norms) for the deliberately near-singular cases,

@@ -276,7 +276,8 @@ nrcps_status nrcps_propagate(nrcps_context *ctx, void *psi, int batch, int nconf
 nrcps_status nrcps_overlap(nrcps_context *ctx, const double *dev_src, int ns, const void *dev_psi,
                            int nt, int nconf, long vol, nrcps_precision prec, double *dev_S);
 /* Plane-wave sources (OneBody::Set(n1,n2,n3), src/one_body/one_body.C:215-228):
- * S[c][s][t] = psi_{c,t}(p_s), an exact gather; dev_index = ns lattice indices. */
+ * S[c][s][t] = psi_{c,t}(p_s), an exact gather; dev_index = ns lattice indices
+ * (an index outside [0, vol) gives zeros). */
 nrcps_status nrcps_overlap_planewave(nrcps_context *ctx, const int *dev_index, int ns,
                                      const void *dev_psi, int nt, int nconf, long vol,
                                      nrcps_precision prec, double *dev_S);

@@ -78,7 +78,9 @@ __global__ void gather_kernel(const int* __restrict__ index, int ns, const void*
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
     long conf = e / ((long)ns * nt);
     int s = (int)((e / nt) % ns), t = (int)(e % nt);
-    cplx<R> q = ld<R>(psi, ((conf * nt + t) * vol) + index[s]);
+    const int p = index[s];
+    // a lattice index outside [0, vol) has no overlap with the orbitals
+    cplx<R> q = (p >= 0 && p < vol) ? ld<R>(psi, ((conf * nt + t) * vol) + p) : cplx<R>{(R)0, (R)0};
     S[2 * e] = (double)q.re;
     S[2 * e + 1] = (double)q.im;
   }

@@ -229,15 +229,23 @@ def generate_pairs(L: int, T: int, fermi_energy: float, seed: int, n_conf: int, 
     idx, _, _ = momenta((L, L, L), "PERFECT", 1.0, fermi_energy, 2.0)
     V = L ** 3
     Xs, Cs = [], []
-    for c0 in range(first_conf, first_conf + n_conf, chunk):
-        m = min(chunk, first_conf + n_conf - c0)
-        ens = Ensemble(EnsembleJob(L=L, T=T, n_conf=m, seed=seed, precision=precision, fermi_energy=fermi_energy,
-                                   qr_period=qr_period), plane_wave_index=idx, ctx=ctx)
-        d = ens.run(c0)
-        Cs.append((d[:, :, -1].abs() ** 2).to(torch.float64))
-        ens.close()
-        bits = draw_z2_bits("RANLXS2", seed, c0 * T * V, m * T * V, ctx)
-        Xs.append(coarse_fields(bits, 0, L, T, G, m, ctx))
+    ens = None  # one ensemble per chunk size, run at each chunk's first configuration
+    try:
+        for c0 in range(first_conf, first_conf + n_conf, chunk):
+            m = min(chunk, first_conf + n_conf - c0)
+            if ens is None or ens.job.n_conf != m:
+                if ens is not None:
+                    ens.close()
+                ens = Ensemble(EnsembleJob(L=L, T=T, n_conf=m, seed=seed, precision=precision,
+                                           fermi_energy=fermi_energy, qr_period=qr_period),
+                               plane_wave_index=idx, ctx=ctx)
+            d = ens.run(c0)
+            Cs.append((d[:, :, -1].abs() ** 2).to(torch.float64))  # a copy: the next run reuses d
+            bits = draw_z2_bits("RANLXS2", seed, c0 * T * V, m * T * V, ctx)
+            Xs.append(coarse_fields(bits, 0, L, T, G, m, ctx))
+    finally:
+        if ens is not None:
+            ens.close()
     return torch.cat(Xs), torch.cat(Cs)
 
 

@@ -391,6 +391,12 @@ nrcps_status nrcps_ensemble_set_sources(nrcps_ensemble *ens, const double *sourc
 nrcps_status nrcps_ensemble_destroy(nrcps_ensemble *ens);
 /* Kernel launches issued by the last run (for launch accounting). */
 nrcps_status nrcps_ensemble_launches(const nrcps_ensemble *ens, long *launches);
+/* Z2 fields: *dev_bits receives the device array of the last run's field
+ * bits (slice t of configuration c at bit (c T + t) V), valid until the
+ * next run or destroy; NULL for other fields.  No counterpart in the
+ * reference (its Lattice keeps one slice); lets a caller reuse the run's
+ * fields (the control variate's features) instead of drawing them again. */
+nrcps_status nrcps_ensemble_field_bits(const nrcps_ensemble *ens, const uint32_t **dev_bits);
 
 /* --------------------------------------------------------------- batch
  * Jobs of different lattice size, particle number and time extent advanced

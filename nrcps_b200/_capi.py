@@ -112,6 +112,7 @@ SIGNATURES = {
     "nrcps_ensemble_set_sources": ([_P, _DP, _IP], _I),
     "nrcps_ensemble_destroy": ([_P], _I),
     "nrcps_ensemble_launches": ([_P, _LP], _I),
+    "nrcps_ensemble_field_bits": ([_P, ctypes.POINTER(ctypes.c_void_p)], _I),
     "nrcps_accumulate": ([_P, _P, _I, _I, _I, _I, _I, _P, _P], _I),
     "nrcps_batch_create": ([_P, _P, _P, _I, ctypes.POINTER(_P)], _I),
     "nrcps_batch_output_size": ([_P, _LP, _LP], _I),

@@ -837,6 +837,14 @@ class Ensemble:
         self.ctx.check(lib().nrcps_ensemble_launches(self.handle, ctypes.byref(n)), "ensemble_launches")
         return n.value
 
+    def field_bits_ptr(self) -> Optional[int]:
+        """Device address of the last run's Z2 field bits (configuration c,
+        slice t at bit (c T + t) V), valid until the next run; None for other
+        fields."""
+        p = ctypes.c_void_p()
+        self.ctx.check(lib().nrcps_ensemble_field_bits(self.handle, ctypes.byref(p)), "ensemble_field_bits")
+        return p.value
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             lib().nrcps_ensemble_destroy(self.handle)

@@ -406,6 +406,12 @@ extern "C" nrcps_status nrcps_ensemble_launches(const nrcps_ensemble* e, long* l
   return NRCPS_OK;
 }
 
+extern "C" nrcps_status nrcps_ensemble_field_bits(const nrcps_ensemble* e, const uint32_t** dev_bits) {
+  if (!e || !dev_bits) return NRCPS_ERR_INVALID_ARGUMENT;
+  *dev_bits = e->job.field_kind == NRCPS_FIELD_ZTWO ? e->bits : nullptr;
+  return NRCPS_OK;
+}
+
 extern "C" nrcps_status nrcps_ensemble_destroy(nrcps_ensemble* e) {
   if (!e) return NRCPS_OK;
   if (e->ctx) cudaStreamSynchronize(e->ctx->stream);

@@ -201,11 +201,13 @@ class ControlVariateNet:
 
 
 # ------------------------------------------------------------------ data
-def coarse_fields(bits: torch.Tensor, bit0: int, L: int, T: int, G: int, n: int, ctx: Context) -> torch.Tensor:
+def coarse_fields(bits, bit0: int, L: int, T: int, G: int, n: int, ctx: Context) -> torch.Tensor:
     """Block means [n, T, G^3] BF16 of the Z2 fields of n configurations whose
-    slice t of configuration c is bits bit0 + (c T + t) L^3 ..."""
+    slice t of configuration c is bits bit0 + (c T + t) L^3 ... (bits: a
+    device tensor or a device address)."""
     x = torch.empty((n, T, G ** 3), dtype=torch.bfloat16, device=ctx.device)
-    ctx.check(lib().nrcps_cv_coarse_z2(ctx.handle, _p(bits), bit0, L, T, G, n, _p(x)), "cv coarse")
+    b = ctypes.c_void_p(bits) if isinstance(bits, int) else _p(bits)
+    ctx.check(lib().nrcps_cv_coarse_z2(ctx.handle, b, bit0, L, T, G, n, _p(x)), "cv coarse")
     return x
 
 
@@ -241,8 +243,8 @@ def generate_pairs(L: int, T: int, fermi_energy: float, seed: int, n_conf: int, 
                                plane_wave_index=idx, ctx=ctx)
             d = ens.run(c0)
             Cs.append((d[:, :, -1].abs() ** 2).to(torch.float64))  # a copy: the next run reuses d
-            bits = draw_z2_bits("RANLXS2", seed, c0 * T * V, m * T * V, ctx)
-            Xs.append(coarse_fields(bits, 0, L, T, G, m, ctx))
+            # the features from the run's own fields (the same stream window)
+            Xs.append(coarse_fields(ens.field_bits_ptr(), 0, L, T, G, m, ctx))
     finally:
         if ens is not None:
             ens.close()

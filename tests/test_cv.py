@@ -77,6 +77,40 @@ def test_device_forward_and_gradients_match_reference():
 
 
 @pytest.mark.gpu
+def test_run_field_bits_are_the_stream_window():
+    """nrcps_ensemble_field_bits: after a run at configuration c0 the
+    ensemble's bits are the RANLXS2 window of configurations c0.. (the
+    control variate takes its features from them): the same words as a fresh
+    draw of that window, and the same block means."""
+    import torch
+    import nrcps_b200 as nb
+    from nrcps_b200 import cv
+    ctx = nb.default_context()
+    L, T, m, seed, c0 = 8, 6, 5, 1234, 7
+    V = L ** 3
+    idx, _, _ = nb.momenta((L,) * 3, "PERFECT", 1.0, 0.35, 2.0)
+    ens = nb.Ensemble(nb.EnsembleJob(L=L, T=T, n_conf=m, seed=seed, precision="f64", fermi_energy=0.35),
+                      plane_wave_index=idx, ctx=ctx)
+    try:
+        ens.run(c0)
+        ptr = ens.field_bits_ptr()
+        assert ptr
+        ref = nb.draw_z2_bits("RANLXS2", seed, c0 * T * V, m * T * V, ctx)
+        nwords = (m * T * V) // 32
+
+        class _Words:  # the ensemble's device words as a tensor view
+            __cuda_array_interface__ = {"shape": (nwords,), "typestr": "<i4", "data": (ptr, True), "version": 3}
+
+        got = torch.as_tensor(_Words(), device=ctx.device)
+        assert torch.equal(got, ref.view(torch.int32)[:nwords])
+        xa = cv.coarse_fields(ptr, 0, L, T, 4, m, ctx)
+        xb = cv.coarse_fields(ref, 0, L, T, 4, m, ctx)
+        assert torch.equal(xa, xb)
+    finally:
+        ens.close()
+
+
+@pytest.mark.gpu
 def test_training_and_control_variate_on_a_small_ensemble():
     """L=8, T=12, N=7, Z2 a=0.5: train on 3072 configurations, calibrate c on
     1024 more, estimate <C_N(tau)> from 2048 fresh configurations with <g> from

@@ -99,7 +99,7 @@ def test_run_field_bits_are_the_stream_window():
         nwords = (m * T * V) // 32
 
         class _Words:  # the ensemble's device words as a tensor view
-            __cuda_array_interface__ = {"shape": (nwords,), "typestr": "<i4", "data": (ptr, True), "version": 3}
+            __cuda_array_interface__ = {"shape": (nwords,), "typestr": "<i4", "data": (ptr, False), "version": 3}
 
         got = torch.as_tensor(_Words(), device=ctx.device)
         assert torch.equal(got, ref.view(torch.int32)[:nwords])

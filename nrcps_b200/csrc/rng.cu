@@ -562,10 +562,10 @@ extern "C" nrcps_status nrcps_draw_fields(nrcps_context* ctx, int kind, long see
   long done = 0;
   while (done < need_total) {
     long need = need_total - done;
-    // pairs per round: acceptance pi/4 = 0.785; up to 32 M pairs (0.9 GB of
+    // pairs per round: acceptance pi/4 = 0.785; up to 128 M pairs (3.5 GB of
     // working memory), so a large draw takes few host round trips
     long npairs = (long)(need * 1.35) + 4096;
-    if (npairs > 32L * 1024 * 1024) npairs = 32L * 1024 * 1024;
+    if (npairs > 128L * 1024 * 1024) npairs = 128L * 1024 * 1024;
     const long ntiles_max = (npairs + 1023) / 1024;
     size_t bytes_u = sizeof(double) * 2 * npairs;
     size_t bytes_i = sizeof(int) * (3 * npairs + ntiles_max + 16);

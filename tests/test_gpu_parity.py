@@ -90,16 +90,17 @@ def test_gauss_fields_stream_exact(ctx, field):
 
 
 def test_gauss_fields_large_draw_is_one_stream(ctx):
-    """A draw larger than one round of the Gaussian sampler (32 M candidate
+    """A draw larger than one round of the Gaussian sampler (128 M candidate
     pairs, so this one takes two rounds and a host read of the consumed
     stream length between them) equals the same stream drawn slice by slice,
     and ends at the same stream position."""
-    vol, slices = 48 ** 3, 240  # 26.5 M values
+    vol, slices = 48 ** 3, 1000  # 110.6 M values
     big, off = nb.draw_fields("RANLXS2", 5, "GAUSS", vol, slices, 0, ctx)
     pos = 0
-    for t0 in range(0, slices, 60):
-        part, pos = nb.draw_fields("RANLXS2", 5, "GAUSS", vol, 60, pos, ctx)
-        assert torch.equal(part, big[t0:t0 + 60])
+    for t0 in range(0, slices, 250):
+        part, pos = nb.draw_fields("RANLXS2", 5, "GAUSS", vol, 250, pos, ctx)
+        assert torch.equal(part, big[t0:t0 + 250])
+        del part
     assert pos == off
     del big
 

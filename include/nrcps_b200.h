@@ -123,6 +123,11 @@ const char *nrcps_version(void);
  *                      rounded once, which the fused step stages in shared
  *                      memory; 0: the step forms the weight from phi per
  *                      site and orbital (split into two FP32 parts);
+ *   "batch.prefetch_fields" 1 (default): such a batch (FP32 weights) draws
+ *                      the next run's fields on a side stream while a run's
+ *                      graph executes, into a second weight buffer (the same
+ *                      stream windows, the same results); 0: each run draws
+ *                      its own fields before its graph;
  *   "lu.warp"          1 (default): leading-minor determinants with one warp
  *                      per minor in shared memory (N <= 64); 0: one thread
  *                      per minor with global scratch;

@@ -116,20 +116,29 @@ struct nrcps_batch {
   uint64_t sites = 0;              // field sites of one run
   double* phi = nullptr;           // Gaussian / Z3 fields, interleaved complex
   uint32_t* bits = nullptr;        // Z2 fields
-  float* wtab = nullptr;           // FP32 orbitals, real Gaussian fields: one weight per site
+  float* wt[2] = {nullptr, nullptr};  // FP32 orbitals, real Gaussian fields: one weight per site (two
+                                      // buffers when the next run's fields are drawn during this run)
   uint64_t* job_start = nullptr;   // first field site of every job (device)
   double* job_inv_vol = nullptr;   // 1 / V of every job (device)
   int njobs = 0;
   uint64_t stream_pos = 0;         // generator position (uniforms) of the next run
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph[2] = {nullptr, nullptr};  // one time loop per weight buffer
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
   double* out_captured = nullptr;
   long launches_per_run = 0;
+  // drawing the next run's fields on a side stream while a run's graph runs
+  bool prefetch = false;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ready[2] = {nullptr, nullptr};  // buffer j's fields drawn
+  cudaEvent_t used[2] = {nullptr, nullptr};   // the graph that read buffer j is done
+  bool prepared[2] = {false, false};
+  bool used_recorded[2] = {false, false};
+  int next = 0;  // buffer of the next run
 };
 
 namespace nrcps {
 
-static nrcps_status record_batch(nrcps_batch* b, double* out) {
+static nrcps_status record_batch(nrcps_batch* b, double* out, const float* wtab) {
   nrcps_context* ctx = b->ctx;
   const nrcps_precision prec = (nrcps_precision)b->params.precision;
   const long n0 = ctx->launches;
@@ -161,8 +170,8 @@ static nrcps_status record_batch(nrcps_batch* b, double* out) {
       if (t + 1 >= g.Tmax) break;
       const int nn = g.nact[t + 1];  // configurations measured again at t + 1
       nrcps_position_factor pf{};
-      pf.field_mode = b->bits ? 1 : b->wtab ? 3 : 2;
-      pf.dev_field = b->bits ? (const void*)b->bits : b->wtab ? (const void*)b->wtab : (const void*)b->phi;
+      pf.field_mode = b->bits ? 1 : wtab ? 3 : 2;
+      pf.dev_field = b->bits ? (const void*)b->bits : wtab ? (const void*)wtab : (const void*)b->phi;
       pf.bit0 = (uint64_t)t * g.V;
       pf.conf_stride = 0;
       pf.dev_conf_base = g.conf_base;
@@ -195,8 +204,14 @@ using namespace nrcps;
 extern "C" nrcps_status nrcps_batch_destroy(nrcps_batch* b) {
   if (!b) return NRCPS_OK;
   if (b->ctx) cudaStreamSynchronize(b->ctx->stream);
-  if (b->exec) cudaGraphExecDestroy(b->exec);
-  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->side) cudaStreamSynchronize(b->side);
+  for (int j = 0; j < 2; ++j) {
+    if (b->exec[j]) cudaGraphExecDestroy(b->exec[j]);
+    if (b->graph[j]) cudaGraphDestroy(b->graph[j]);
+    if (b->ready[j]) cudaEventDestroy(b->ready[j]);
+    if (b->used[j]) cudaEventDestroy(b->used[j]);
+  }
+  if (b->side) cudaStreamDestroy(b->side);
   for (Group& g : b->groups) {
     if (g.stream) cudaStreamSynchronize(g.stream);
     void* bufs[] = {g.psi, g.kinv, g.kinv_f, g.pw_index, g.conf_base, g.out_off, g.conf_T,
@@ -206,7 +221,7 @@ extern "C" nrcps_status nrcps_batch_destroy(nrcps_batch* b) {
     if (g.done) cudaEventDestroy(g.done);
     if (g.stream) cudaStreamDestroy(g.stream);
   }
-  void* fields[] = {b->phi, b->bits, b->wtab, b->job_start, b->job_inv_vol};
+  void* fields[] = {b->phi, b->bits, b->wt[0], b->wt[1], b->job_start, b->job_inv_vol};
   for (void* p : fields)
     if (p) cudaFree(p);
   delete b;
@@ -338,7 +353,7 @@ extern "C" nrcps_status nrcps_batch_create(nrcps_context* ctx, const nrcps_batch
       std::vector<double> iv(njobs);
       for (int j = 0; j < njobs; ++j) iv[j] = 1.0 / ((double)jobs[j].L * jobs[j].L * jobs[j].L);
       b->njobs = njobs;
-      if ((st = check_cuda(ctx, cudaMalloc((void**)&b->wtab, 4 * (size_t)b->sites), "cudaMalloc(weights)")) ||
+      if ((st = check_cuda(ctx, cudaMalloc((void**)&b->wt[0], 4 * (size_t)b->sites), "cudaMalloc(weights)")) ||
           (st = check_cuda(ctx, cudaMalloc((void**)&b->job_start, 8 * (size_t)njobs), "cudaMalloc(job starts)")) ||
           (st = check_cuda(ctx, cudaMalloc((void**)&b->job_inv_vol, 8 * (size_t)njobs), "cudaMalloc(job 1/V)")) ||
           (st = check_cuda(ctx, cudaMemcpy(b->job_start, base.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice),
@@ -346,6 +361,16 @@ extern "C" nrcps_status nrcps_batch_create(nrcps_context* ctx, const nrcps_batch
           (st = check_cuda(ctx, cudaMemcpy(b->job_inv_vol, iv.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice),
                            "cudaMemcpy(job 1/V)")))
         return fail(st);
+      if (ctx->batch_prefetch_fields) {
+        b->prefetch = true;
+        if ((st = check_cuda(ctx, cudaMalloc((void**)&b->wt[1], 4 * (size_t)b->sites), "cudaMalloc(weights)")) ||
+            (st = check_cuda(ctx, cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking), "stream")))
+          return fail(st);
+        for (int j = 0; j < 2; ++j)
+          if ((st = check_cuda(ctx, cudaEventCreateWithFlags(&b->ready[j], cudaEventDisableTiming), "event")) ||
+              (st = check_cuda(ctx, cudaEventCreateWithFlags(&b->used[j], cudaEventDisableTiming), "event")))
+            return fail(st);
+      }
     }
   }
   *out = b;
@@ -366,52 +391,95 @@ extern "C" nrcps_status nrcps_batch_output_size(const nrcps_batch* b, long* doub
   return NRCPS_OK;
 }
 
+namespace nrcps {
+
+// One run's fields, the next window of the stream, on the context's current
+// stream: Z2 bits, or phi and (FP32, real Gaussian) weight buffer j.
+static nrcps_status draw_run_fields(nrcps_batch* b, int j) {
+  nrcps_context* ctx = b->ctx;
+  if (b->params.field_kind == NRCPS_FIELD_ZTWO) {
+    NRCPS_TRY(nrcps_draw_z2_bits(ctx, b->params.rng_kind, b->params.seed, b->stream_pos, b->sites, b->bits));
+    b->stream_pos += b->sites;
+    return NRCPS_OK;
+  }
+  NRCPS_TRY(nrcps_draw_fields(ctx, b->params.rng_kind, b->params.seed, b->params.field_kind, (long)b->sites, 1,
+                              &b->stream_pos, b->phi));
+  if (b->wt[j]) {
+    real_weights_kernel<<<grid_for((long)b->sites, 256, (long)ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+        b->wt[j], reinterpret_cast<const double2*>(b->phi), b->job_start, b->job_inv_vol, b->njobs, b->params.a,
+        b->sites);
+    ctx->launches++;
+    NRCPS_TRY(check_launch(ctx, "real_weights_kernel"));
+  }
+  return NRCPS_OK;
+}
+
+// The time loop of weight buffer j captured into graph j.
+static nrcps_status capture_batch(nrcps_batch* b, double* dev_out, int j) {
+  nrcps_context* ctx = b->ctx;
+  NRCPS_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "sync before capture"));
+  cudaStream_t cap = ctx->stream;
+  bool own = false;
+  if (cap == nullptr) {
+    NRCPS_TRY(check_cuda(ctx, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream create"));
+    own = true;
+  }
+  cudaStream_t saved = ctx->stream;
+  ctx->stream = cap;
+  nrcps_status rs = check_cuda(ctx, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+  if (rs == NRCPS_OK) {
+    rs = record_batch(b, dev_out, b->wt[j]);
+    cudaError_t ce = cudaStreamEndCapture(cap, &b->graph[j]);
+    if (rs == NRCPS_OK) rs = check_cuda(ctx, ce, "end capture");
+  }
+  ctx->stream = saved;
+  if (rs == NRCPS_OK) rs = check_cuda(ctx, cudaGraphInstantiate(&b->exec[j], b->graph[j], 0), "graph instantiate");
+  if (own) cudaStreamDestroy(cap);
+  return rs;
+}
+
+}  // namespace nrcps
+
 extern "C" nrcps_status nrcps_batch_run(nrcps_batch* b, double* dev_out) {
   if (!b) return NRCPS_ERR_INVALID_ARGUMENT;
   nrcps_context* ctx = b->ctx;
   NRCPS_REQUIRE(ctx, dev_out, "nrcps_batch_run: null output");
-  // ---- this run's fields: the next window of the one stream
-  if (b->params.field_kind == NRCPS_FIELD_ZTWO) {
-    NRCPS_TRY(nrcps_draw_z2_bits(ctx, b->params.rng_kind, b->params.seed, b->stream_pos, b->sites, b->bits));
-    b->stream_pos += b->sites;
+  const int j = b->prefetch ? b->next : 0;  // this run's weight buffer
+  // ---- this run's fields: the next window of the one stream (drawn during
+  // the previous run when prefetching)
+  if (b->prefetch && b->prepared[j]) {
+    NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(ctx->stream, b->ready[j], 0), "wait fields"));
+    b->prepared[j] = false;
   } else {
-    NRCPS_TRY(nrcps_draw_fields(ctx, b->params.rng_kind, b->params.seed, b->params.field_kind, (long)b->sites, 1,
-                                &b->stream_pos, b->phi));
-    if (b->wtab) {
-      real_weights_kernel<<<grid_for((long)b->sites, 256, (long)ctx->sm_count * 16), 256, 0, ctx->stream>>>(
-          b->wtab, reinterpret_cast<const double2*>(b->phi), b->job_start, b->job_inv_vol, b->njobs, b->params.a,
-          b->sites);
-      ctx->launches++;
-      NRCPS_TRY(check_launch(ctx, "real_weights_kernel"));
+    NRCPS_TRY(draw_run_fields(b, j));
+  }
+  const int ngraphs = b->prefetch ? 2 : 1;
+  if (b->out_captured != dev_out) {
+    for (int i = 0; i < 2; ++i) {
+      if (b->exec[i]) cudaGraphExecDestroy(b->exec[i]);
+      if (b->graph[i]) cudaGraphDestroy(b->graph[i]);
+      b->exec[i] = nullptr;
+      b->graph[i] = nullptr;
     }
-  }
-  if (b->exec && b->out_captured != dev_out) {
-    cudaGraphExecDestroy(b->exec);
-    cudaGraphDestroy(b->graph);
-    b->exec = nullptr;
-    b->graph = nullptr;
-  }
-  if (!b->exec) {
     b->out_captured = dev_out;
-    NRCPS_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "sync before capture"));
-    cudaStream_t cap = ctx->stream;
-    bool own = false;
-    if (cap == nullptr) {
-      NRCPS_TRY(check_cuda(ctx, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream create"));
-      own = true;
-    }
-    cudaStream_t saved = ctx->stream;
-    ctx->stream = cap;
-    nrcps_status rs = check_cuda(ctx, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
-    if (rs == NRCPS_OK) {
-      rs = record_batch(b, dev_out);
-      cudaError_t ce = cudaStreamEndCapture(cap, &b->graph);
-      if (rs == NRCPS_OK) rs = check_cuda(ctx, ce, "end capture");
-    }
-    ctx->stream = saved;
-    if (rs == NRCPS_OK) rs = check_cuda(ctx, cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiate");
-    if (own) cudaStreamDestroy(cap);
-    if (rs != NRCPS_OK) return rs;
   }
-  return check_cuda(ctx, cudaGraphLaunch(b->exec, ctx->stream), "graph launch");
+  for (int i = 0; i < ngraphs; ++i)
+    if (!b->exec[i]) NRCPS_TRY(capture_batch(b, dev_out, i));
+  NRCPS_TRY(check_cuda(ctx, cudaGraphLaunch(b->exec[j], ctx->stream), "graph launch"));
+  if (!b->prefetch) return NRCPS_OK;
+  // ---- the next run's fields into the other buffer, on the side stream,
+  // once the graph that last read that buffer is done
+  NRCPS_TRY(check_cuda(ctx, cudaEventRecord(b->used[j], ctx->stream), "record used"));
+  b->used_recorded[j] = true;
+  const int o = j ^ 1;
+  if (b->used_recorded[o]) NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(b->side, b->used[o], 0), "wait used"));
+  cudaStream_t main = ctx->stream;
+  ctx->stream = b->side;
+  const nrcps_status st = draw_run_fields(b, o);
+  ctx->stream = main;
+  NRCPS_TRY(st);
+  NRCPS_TRY(check_cuda(ctx, cudaEventRecord(b->ready[o], b->side), "record ready"));
+  b->prepared[o] = true;
+  b->next = o;
+  return NRCPS_OK;
 }

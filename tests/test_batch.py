@@ -173,3 +173,32 @@ def test_device_batch_fp32_real_weight_table():
         if L >= 32:
             assert np.array_equal(s, p), (L, N)
         assert _rel(s, g) < 1e-5, (L, N, _rel(s, g))
+
+
+@pytest.mark.gpu
+def test_device_batch_field_prefetch_is_the_same_stream():
+    """"batch.prefetch_fields" 1 (the default) draws the next run's fields on a
+    side stream during a run, into a second weight buffer: three consecutive
+    runs give bit for bit the determinants of three runs that draw their own
+    fields first (option 0)."""
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    shell = {7: 1.5, 19: 2.5}
+    spec = [(32, 6, 19), (16, 9, 7), (24, 4, 7)]
+    jobs = [nb.BatchJob(L=L, T=T, n_conf=2, fermi_energy=0.5 * (2 * np.pi / L) ** 2 * shell[N]) for L, T, N in spec]
+
+    def runs(prefetch):
+        ctx.set_option("batch.prefetch_fields", prefetch)
+        try:
+            b = nb.Batch(jobs, seed=31, field="GAUSS", a=0.3, precision="f32", ctx=ctx)
+            out = [[d.cpu().numpy() for d in b.run()] for _ in range(3)]
+            b.close()
+        finally:
+            ctx.set_option("batch.prefetch_fields", 1)
+        return out
+
+    with_prefetch, without = runs(1), runs(0)
+    for r in range(3):
+        for a, b in zip(with_prefetch[r], without[r]):
+            assert np.array_equal(a, b), r
+    assert not np.array_equal(with_prefetch[0][0], with_prefetch[1][0])

@@ -131,6 +131,7 @@ struct nrcps_batch {
   cudaStream_t side = nullptr;
   cudaEvent_t ready[2] = {nullptr, nullptr};  // buffer j's fields drawn
   cudaEvent_t used[2] = {nullptr, nullptr};   // the graph that read buffer j is done
+  cudaEvent_t before = nullptr;               // the work issued before a run's graph
   bool prepared[2] = {false, false};
   bool used_recorded[2] = {false, false};
   int next = 0;  // buffer of the next run
@@ -211,6 +212,7 @@ extern "C" nrcps_status nrcps_batch_destroy(nrcps_batch* b) {
     if (b->ready[j]) cudaEventDestroy(b->ready[j]);
     if (b->used[j]) cudaEventDestroy(b->used[j]);
   }
+  if (b->before) cudaEventDestroy(b->before);
   if (b->side) cudaStreamDestroy(b->side);
   for (Group& g : b->groups) {
     if (g.stream) cudaStreamSynchronize(g.stream);
@@ -370,6 +372,8 @@ extern "C" nrcps_status nrcps_batch_create(nrcps_context* ctx, const nrcps_batch
           if ((st = check_cuda(ctx, cudaEventCreateWithFlags(&b->ready[j], cudaEventDisableTiming), "event")) ||
               (st = check_cuda(ctx, cudaEventCreateWithFlags(&b->used[j], cudaEventDisableTiming), "event")))
             return fail(st);
+        if ((st = check_cuda(ctx, cudaEventCreateWithFlags(&b->before, cudaEventDisableTiming), "event")))
+          return fail(st);
       }
     }
   }
@@ -465,6 +469,9 @@ extern "C" nrcps_status nrcps_batch_run(nrcps_batch* b, double* dev_out) {
   }
   for (int i = 0; i < ngraphs; ++i)
     if (!b->exec[i]) NRCPS_TRY(capture_batch(b, dev_out, i));
+  // the side draw below starts after everything issued before this graph
+  // (it may share the context's scratch and generator arguments with it)
+  if (b->prefetch) NRCPS_TRY(check_cuda(ctx, cudaEventRecord(b->before, ctx->stream), "record before"));
   NRCPS_TRY(check_cuda(ctx, cudaGraphLaunch(b->exec[j], ctx->stream), "graph launch"));
   if (!b->prefetch) return NRCPS_OK;
   // ---- the next run's fields into the other buffer, on the side stream,
@@ -473,12 +480,18 @@ extern "C" nrcps_status nrcps_batch_run(nrcps_batch* b, double* dev_out) {
   b->used_recorded[j] = true;
   const int o = j ^ 1;
   if (b->used_recorded[o]) NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(b->side, b->used[o], 0), "wait used"));
+  NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(b->side, b->before, 0), "wait before"));
+  if (ctx->side_pending) NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(b->side, ctx->side_done, 0), "wait side"));
   cudaStream_t main = ctx->stream;
   ctx->stream = b->side;
   const nrcps_status st = draw_run_fields(b, o);
   ctx->stream = main;
   NRCPS_TRY(st);
   NRCPS_TRY(check_cuda(ctx, cudaEventRecord(b->ready[o], b->side), "record ready"));
+  if (!ctx->side_done)
+    NRCPS_TRY(check_cuda(ctx, cudaEventCreateWithFlags(&ctx->side_done, cudaEventDisableTiming), "event"));
+  NRCPS_TRY(check_cuda(ctx, cudaEventRecord(ctx->side_done, b->side), "record side"));
+  ctx->side_pending = true;
   b->prepared[o] = true;
   b->next = o;
   return NRCPS_OK;

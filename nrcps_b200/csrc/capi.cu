@@ -30,6 +30,13 @@ nrcps_status check_launch(nrcps_context* ctx, const char* what) {
 
 void* scratch(nrcps_context* ctx, size_t bytes, nrcps_status* st) {
   *st = NRCPS_OK;
+  // a side-stream field draw may still be using the scratch (no scratch
+  // user runs inside a graph capture, where an outside event cannot be waited)
+  if (ctx->side_pending) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->stream, &cs);
+    if (cs == cudaStreamCaptureStatusNone) cudaStreamWaitEvent(ctx->stream, ctx->side_done, 0);
+  }
   if (bytes <= ctx->scratch_bytes) return ctx->scratch;
   if (ctx->scratch) {
     cudaStreamSynchronize(ctx->stream);
@@ -77,6 +84,8 @@ extern "C" nrcps_status nrcps_create(int device, nrcps_context** out) {
 extern "C" nrcps_status nrcps_destroy(nrcps_context* ctx) {
   if (!ctx) return NRCPS_OK;
   cudaStreamSynchronize(ctx->stream);
+  cudaDeviceSynchronize();  // side-stream draws included
+  if (ctx->side_done) cudaEventDestroy(ctx->side_done);
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->gen_args) cudaFree(ctx->gen_args);
   if (ctx->kin_f32) cudaFree(ctx->kin_f32);

@@ -87,6 +87,11 @@ struct Context {
   // Scratch owned by the context (grown on demand, never shrunk).
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
+  // The last field draw issued on a side stream (a batch drawing its next
+  // run's fields during a run); work on the context's stream that uses the
+  // shared scratch waits for it, and each side draw waits for the previous.
+  cudaEvent_t side_done = nullptr;
+  bool side_pending = false;
   long launches = 0;  // kernels queued through this context
   // Device copy of the ranlux generation arguments for (gen_kind, gen_seed).
   void* gen_args = nullptr;

@@ -320,7 +320,9 @@ nrcps_status ranlux_generate(nrcps_context* ctx, int kind, long seed, uint64_t u
     if (!ctx->gen_args) {
       NRCPS_TRY(check_cuda(ctx, cudaMalloc(&ctx->gen_args, sizeof(GenArgs)), "cudaMalloc(GenArgs)"));
     }
-    NRCPS_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "sync before GenArgs update"));
+    // every stream's draws (a batch's side stream included) are done with
+    // the old arguments before they are replaced
+    NRCPS_TRY(check_cuda(ctx, cudaDeviceSynchronize(), "sync before GenArgs update"));
     cudaError_t e = cudaMemcpy(ctx->gen_args, h, sizeof(GenArgs), cudaMemcpyHostToDevice);
     delete h;
     NRCPS_TRY(check_cuda(ctx, e, "cudaMemcpy(GenArgs)"));

@@ -202,3 +202,34 @@ def test_device_batch_field_prefetch_is_the_same_stream():
         for a, b in zip(with_prefetch[r], without[r]):
             assert np.array_equal(a, b), r
     assert not np.array_equal(with_prefetch[0][0], with_prefetch[1][0])
+
+
+@pytest.mark.gpu
+def test_device_batch_field_prefetch_with_other_draws_in_between():
+    """While a prefetching batch's next fields are drawn on its side stream,
+    the context draws another Gaussian field with another seed (the shared
+    scratch and generator arguments): both the batch's next run and that
+    draw are what they are without the overlap."""
+    import torch
+    import nrcps_b200 as nb
+    ctx = nb.default_context()
+    jobs = [nb.BatchJob(L=32, T=5, n_conf=3, fermi_energy=0.5 * (2 * np.pi / 32) ** 2 * 2.5),
+            nb.BatchJob(L=16, T=7, n_conf=2, fermi_energy=0.5 * (2 * np.pi / 16) ** 2 * 1.5)]
+    b = nb.Batch(jobs, seed=31, field="GAUSS", a=0.3, precision="f32", ctx=ctx)
+    first = [d.cpu().numpy() for d in b.run()]
+    other, _ = nb.draw_fields("RANLXS2", 77, "GAUSS", 32 ** 3, 40, 0, ctx)  # during the side draw
+    second = [d.cpu().numpy() for d in b.run()]
+    other = other.cpu()
+    b.close()
+    ctx.set_option("batch.prefetch_fields", 0)
+    try:
+        ref = nb.Batch(jobs, seed=31, field="GAUSS", a=0.3, precision="f32", ctx=ctx)
+        want = [[d.cpu().numpy() for d in ref.run()] for _ in range(2)]
+        ref.close()
+    finally:
+        ctx.set_option("batch.prefetch_fields", 1)
+    for got, w in zip((first, second), want):
+        for a, c in zip(got, w):
+            assert np.array_equal(a, c)
+    again, _ = nb.draw_fields("RANLXS2", 77, "GAUSS", 32 ** 3, 40, 0, ctx)
+    assert torch.equal(other, again.cpu())

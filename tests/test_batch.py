@@ -262,4 +262,4 @@ def test_ensemble_field_prefetch_is_the_same_stream(precision, mode):
         return out
 
     for a, b in zip(runs(1), runs(0)):
-        assert np.array_equal(a, b, equal_nan=True)
+        assert np.array_equal(a, b)

@@ -128,12 +128,6 @@ const char *nrcps_version(void);
  *                      graph executes, into a second weight buffer (the same
  *                      stream windows, the same results); 0: each run draws
  *                      its own fields before its graph;
- *   "ensemble.prefetch_fields" 1 (default): an ensemble created afterwards
- *                      with Z2 fields draws, while a run's graph executes,
- *                      the fields of the configurations after it on a side
- *                      stream into a second bit buffer; a run at any other
- *                      first configuration draws its own (the same fields
- *                      either way); 0: every run draws its own fields;
  *   "lu.warp"          1 (default): leading-minor determinants with one warp
  *                      per minor in shared memory (N <= 64); 0: one thread
  *                      per minor with global scratch;

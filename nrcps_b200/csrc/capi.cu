@@ -144,8 +144,6 @@ extern "C" nrcps_status nrcps_set_option(nrcps_context* ctx, const char* name, l
     ctx->batch_real_weights = value != 0;
   } else if (n == "batch.prefetch_fields") {
     ctx->batch_prefetch_fields = value != 0;
-  } else if (n == "ensemble.prefetch_fields") {
-    ctx->ensemble_prefetch_fields = value != 0;
   } else {
     return set_error(ctx, NRCPS_ERR_INVALID_ARGUMENT, "unknown option %s", name);
   }

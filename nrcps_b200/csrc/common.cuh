@@ -109,7 +109,6 @@ struct Context {
   int qr_gram_tc = 0;     // 1: QR Gram matrices of FP32 orbitals on the tensor cores (N <= 32); 0: CUDA cores
   int batch_real_weights = 1;  // 1: FP32 batches with real Gaussian fields step on one FP32 weight per site
   int batch_prefetch_fields = 1;  // 1: such batches draw the next run's fields during a run (two weight buffers)
-  int ensemble_prefetch_fields = 1;  // 1: Z2 ensembles draw the next configurations' fields during a run
   // TF32 hi / lo split of the sources for nrcps_overlap's tensor-core path (grown on demand)
   void* tc_split = nullptr;
   size_t tc_split_bytes = 0;

@@ -54,8 +54,7 @@ struct nrcps_ensemble {
   double* w = nullptr;
   int* opp = nullptr;
   int pair_props = 3;  // the pair table's properties, checked on the host (pair_table_props)
-  uint32_t* bits = nullptr;   // Z2 fields of a run (one of bitbuf)
-  uint32_t* bitbuf[2] = {nullptr, nullptr};  // two when the next run's fields are drawn during a run
+  uint32_t* bits = nullptr;   // Z2 fields of a run
   double* phi = nullptr;      // other fields of a run (interleaved complex)
   double* fld = nullptr;      // non-local interaction factor of one slice
   double* S = nullptr;
@@ -63,19 +62,8 @@ struct nrcps_ensemble {
   double* lu_scr = nullptr;
   double* qr_G = nullptr;     // Gram matrices / R^-1 of a re-orthonormalisation
   double* qr_logR = nullptr;  // running sum of log R_ii per configuration and orbital
-  cudaGraph_t graph[2] = {nullptr, nullptr};  // one time loop per Z2 field buffer
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
-  // Z2 fields of the next run (first_conf + n_conf) drawn on a side stream
-  // while a run's graph executes
-  bool prefetch = false;
-  cudaStream_t side = nullptr;
-  cudaEvent_t ready[2] = {nullptr, nullptr};  // buffer k's fields drawn
-  cudaEvent_t used[2] = {nullptr, nullptr};   // the graph that read buffer k is done
-  cudaEvent_t before = nullptr;               // the work issued before a run's graph
-  bool prepared[2] = {false, false};
-  bool used_recorded[2] = {false, false};
-  uint64_t predicted[2] = {0, 0};  // first configuration of the fields in buffer k
-  int next = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
   uint64_t gauss_offset = 0;    // stream position of the next configuration (Gaussian fields)
   uint64_t gauss_next_conf = 0;
   long launches_per_run = 0;
@@ -300,19 +288,7 @@ extern "C" nrcps_status nrcps_ensemble_create(nrcps_context* ctx, const nrcps_jo
   }
   const uint64_t sites = (uint64_t)nc * job->T * V;
   if (fk == NRCPS_FIELD_ZTWO) {
-    if ((st = dalloc(ctx, &e->bitbuf[0], 4 * ((sites + 31) / 32 + 1)))) return fail(st);
-    e->bits = e->bitbuf[0];
-    if (ctx->ensemble_prefetch_fields) {
-      e->prefetch = true;
-      if ((st = dalloc(ctx, &e->bitbuf[1], 4 * ((sites + 31) / 32 + 1))) ||
-          (st = check_cuda(ctx, cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking), "stream")) ||
-          (st = check_cuda(ctx, cudaEventCreateWithFlags(&e->before, cudaEventDisableTiming), "event")))
-        return fail(st);
-      for (int k = 0; k < 2; ++k)
-        if ((st = check_cuda(ctx, cudaEventCreateWithFlags(&e->ready[k], cudaEventDisableTiming), "event")) ||
-            (st = check_cuda(ctx, cudaEventCreateWithFlags(&e->used[k], cudaEventDisableTiming), "event")))
-          return fail(st);
-    }
+    if ((st = dalloc(ctx, &e->bits, 4 * ((sites + 31) / 32 + 1)))) return fail(st);
     if (job->use_potential && job->local_interaction) {
       // the fused step's per-site weights (1 +- a) P/V, P = h (the squared,
       // scaled potential above): the products the general path forms per site
@@ -355,16 +331,8 @@ extern "C" nrcps_status nrcps_ensemble_run(nrcps_ensemble* e, uint64_t first_con
   const uint64_t sites = (uint64_t)j.n_conf * per_conf;
   long n0 = ctx->launches;
   // ---- fields of configurations [first_conf, first_conf + n_conf)
-  const int kb = e->prefetch ? e->next : 0;  // this run's Z2 field buffer
   if (j.field_kind == NRCPS_FIELD_ZTWO) {
-    if (e->prefetch && e->prepared[kb]) {
-      // drawn during the previous run (for the configurations after it)
-      NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(ctx->stream, e->ready[kb], 0), "wait fields"));
-    }
-    if (!(e->prefetch && e->prepared[kb] && e->predicted[kb] == first_conf))
-      NRCPS_TRY(nrcps_draw_z2_bits(ctx, j.rng_kind, j.seed, first_conf * per_conf, sites, e->bitbuf[kb]));
-    e->prepared[kb] = false;
-    e->bits = e->bitbuf[kb];
+    NRCPS_TRY(nrcps_draw_z2_bits(ctx, j.rng_kind, j.seed, first_conf * per_conf, sites, e->bits));
   } else if (j.field_kind == NRCPS_FIELD_ZTHREE) {
     uint64_t off = first_conf * per_conf;
     NRCPS_TRY(nrcps_draw_fields(ctx, j.rng_kind, j.seed, j.field_kind, e->vol, (long)j.n_conf * j.T, &off, e->phi));
@@ -380,20 +348,15 @@ extern "C" nrcps_status nrcps_ensemble_run(nrcps_ensemble* e, uint64_t first_con
     e->gauss_next_conf += j.n_conf;
   }
   long gen_launches = ctx->launches - n0;
-  // ---- the time loop, captured once per output buffer (and Z2 field
-  // buffer) and replayed
-  const bool z2_prefetch = e->prefetch && j.field_kind == NRCPS_FIELD_ZTWO;
-  if (e->dets_captured != dev_dets) {
-    for (int k = 0; k < 2; ++k) {
-      if (e->exec[k]) cudaGraphExecDestroy(e->exec[k]);
-      if (e->graph[k]) cudaGraphDestroy(e->graph[k]);
-      e->exec[k] = nullptr;
-      e->graph[k] = nullptr;
-    }
-    e->dets_captured = dev_dets;
+  // ---- the time loop, captured once per output buffer and replayed
+  if (e->exec && e->dets_captured != dev_dets) {
+    cudaGraphExecDestroy(e->exec);
+    cudaGraphDestroy(e->graph);
+    e->exec = nullptr;
+    e->graph = nullptr;
   }
-  for (int k = 0; k < (z2_prefetch ? 2 : 1); ++k) {
-    if (e->exec[k]) continue;
+  if (!e->exec) {
+    e->dets_captured = dev_dets;
     NRCPS_TRY(check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "sync before capture"));
     cudaStream_t cap = ctx->stream;
     bool own = false;
@@ -403,51 +366,20 @@ extern "C" nrcps_status nrcps_ensemble_run(nrcps_ensemble* e, uint64_t first_con
     }
     cudaStream_t saved = ctx->stream;
     ctx->stream = cap;
-    if (e->bitbuf[k]) e->bits = e->bitbuf[k];
-    nrcps_status rs = check_cuda(ctx, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
-    if (rs == NRCPS_OK) {
-      rs = record_time_loop(e, dev_dets);
-      cudaError_t ce = cudaStreamEndCapture(cap, &e->graph[k]);
-      if (rs == NRCPS_OK) rs = check_cuda(ctx, ce, "end capture");
-    }
+    NRCPS_TRY(check_cuda(ctx, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture"));
+    nrcps_status rs = record_time_loop(e, dev_dets);
+    cudaError_t ce = cudaStreamEndCapture(cap, &e->graph);
     ctx->stream = saved;
-    if (e->bitbuf[kb]) e->bits = e->bitbuf[kb];
-    if (rs == NRCPS_OK) rs = check_cuda(ctx, cudaGraphInstantiate(&e->exec[k], e->graph[k], 0), "graph instantiate");
+    if (rs != NRCPS_OK) {
+      if (own) cudaStreamDestroy(cap);
+      return rs;
+    }
+    NRCPS_TRY(check_cuda(ctx, ce, "end capture"));
+    NRCPS_TRY(check_cuda(ctx, cudaGraphInstantiate(&e->exec, e->graph, 0), "graph instantiate"));
     if (own) cudaStreamDestroy(cap);
-    if (rs != NRCPS_OK) return rs;
   }
-  const long loop_launches = e->launches_per_run;
-  if (z2_prefetch) NRCPS_TRY(check_cuda(ctx, cudaEventRecord(e->before, ctx->stream), "record before"));
-  NRCPS_TRY(check_cuda(ctx, cudaGraphLaunch(e->exec[kb], ctx->stream), "graph launch"));
-  long side_launches = 0;
-  if (z2_prefetch) {
-    // ---- the next configurations' fields into the other buffer, on the
-    // side stream, after the work issued before this graph, earlier side
-    // draws, and the graph that last read that buffer
-    NRCPS_TRY(check_cuda(ctx, cudaEventRecord(e->used[kb], ctx->stream), "record used"));
-    e->used_recorded[kb] = true;
-    const int o = kb ^ 1;
-    if (e->used_recorded[o]) NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(e->side, e->used[o], 0), "wait used"));
-    NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(e->side, e->before, 0), "wait before"));
-    if (ctx->side_pending) NRCPS_TRY(check_cuda(ctx, cudaStreamWaitEvent(e->side, ctx->side_done, 0), "wait side"));
-    const uint64_t nxt = first_conf + j.n_conf;
-    const long s0 = ctx->launches;
-    cudaStream_t main = ctx->stream;
-    ctx->stream = e->side;
-    const nrcps_status st = nrcps_draw_z2_bits(ctx, j.rng_kind, j.seed, nxt * per_conf, sites, e->bitbuf[o]);
-    ctx->stream = main;
-    NRCPS_TRY(st);
-    side_launches = ctx->launches - s0;
-    NRCPS_TRY(check_cuda(ctx, cudaEventRecord(e->ready[o], e->side), "record ready"));
-    if (!ctx->side_done)
-      NRCPS_TRY(check_cuda(ctx, cudaEventCreateWithFlags(&ctx->side_done, cudaEventDisableTiming), "event"));
-    NRCPS_TRY(check_cuda(ctx, cudaEventRecord(ctx->side_done, e->side), "record side"));
-    ctx->side_pending = true;
-    e->prepared[o] = true;
-    e->predicted[o] = nxt;
-    e->next = o;
-  }
-  ctx->launches = n0 + gen_launches + loop_launches + side_launches;
+  NRCPS_TRY(check_cuda(ctx, cudaGraphLaunch(e->exec, ctx->stream), "graph launch"));
+  ctx->launches = n0 + gen_launches + e->launches_per_run;
   return NRCPS_OK;
 }
 
@@ -483,17 +415,10 @@ extern "C" nrcps_status nrcps_ensemble_field_bits(const nrcps_ensemble* e, const
 extern "C" nrcps_status nrcps_ensemble_destroy(nrcps_ensemble* e) {
   if (!e) return NRCPS_OK;
   if (e->ctx) cudaStreamSynchronize(e->ctx->stream);
-  if (e->side) cudaStreamSynchronize(e->side);
-  for (int k = 0; k < 2; ++k) {
-    if (e->exec[k]) cudaGraphExecDestroy(e->exec[k]);
-    if (e->graph[k]) cudaGraphDestroy(e->graph[k]);
-    if (e->ready[k]) cudaEventDestroy(e->ready[k]);
-    if (e->used[k]) cudaEventDestroy(e->used[k]);
-  }
-  if (e->before) cudaEventDestroy(e->before);
-  if (e->side) cudaStreamDestroy(e->side);
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
   void* bufs[] = {e->psi, e->src, e->src_split, e->pw_index, e->kinv, e->kinv_f, e->pos, e->zpos, e->itab, e->w, e->opp,
-                  e->bitbuf[0], e->bitbuf[1], e->phi, e->fld, e->S, e->P1, e->lu_scr, e->qr_G, e->qr_logR};
+                  e->bits, e->phi, e->fld, e->S, e->P1, e->lu_scr, e->qr_G, e->qr_logR};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete e;

@@ -233,33 +233,3 @@ def test_device_batch_field_prefetch_with_other_draws_in_between():
             assert np.array_equal(a, c)
     again, _ = nb.draw_fields("RANLXS2", 77, "GAUSS", 32 ** 3, 40, 0, ctx)
     assert torch.equal(other, again.cpu())
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("precision,mode", [("f32", "slater"), ("f64", "slater"), ("f32", "slater2")])
-def test_ensemble_field_prefetch_is_the_same_stream(precision, mode):
-    """"ensemble.prefetch_fields" 1 (the default): a Z2 ensemble draws the
-    fields of the configurations after a run on a side stream during that
-    run.  Runs at 0, n, 2n (prefetched), then at 7 and 2 (not the predicted
-    configurations: drawn by the run) give the determinants of an ensemble
-    that draws every run's fields itself, bit for bit."""
-    import nrcps_b200 as nb
-    ctx = nb.default_context()
-    L, T, n = 8, 6, 4
-    idx, _, _ = nb.momenta((L,) * 3, "PERFECT", 1.0, 0.35, 2.0)
-    job = nb.EnsembleJob(L=L, T=T, n_conf=n, seed=77, precision=precision, fermi_energy=0.35, mode=mode,
-                         qr_period=4 if precision == "f32" else 0)
-    firsts = [0, n, 2 * n, 7, 2]
-
-    def runs(prefetch):
-        ctx.set_option("ensemble.prefetch_fields", prefetch)
-        try:
-            e = nb.Ensemble(job, plane_wave_index=idx, ctx=ctx)
-            out = [e.run(c).cpu().numpy() for c in firsts]
-            e.close()
-        finally:
-            ctx.set_option("ensemble.prefetch_fields", 1)
-        return out
-
-    for a, b in zip(runs(1), runs(0)):
-        assert np.array_equal(a, b)

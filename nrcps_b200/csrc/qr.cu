@@ -12,11 +12,7 @@
 //   det S_n(Psi) = det S_n(Q) * prod_{i <= n} R_ii.
 // The running sum of log R_ii per orbital is kept per configuration and the
 // measured determinants are rescaled by exp(sum_{i<=n} log R_ii).
-#include <cooperative_groups.h>
-
 #include "common.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace nrcps {
 
@@ -227,21 +223,14 @@ __global__ void chol_inv_kernel(double* __restrict__ G, int N, int nconf, double
 // the NG = 16 site groups of a pair (16 adjacent lanes of one warp) are
 // summed by shuffles in FP64 at the end.
 // Tile rows N .. 19 are zero, so partial blocks need no special case.
-// A configuration is one cluster of G4_SPLIT CTAs, CTA r taking tiles r,
-// r + G4_SPLIT, ..: twice the CTAs of one per configuration, so the last
-// wave of a large batch is short; rank 0 adds the CTAs' sums in rank order
-// (a fixed split: the sums do not depend on the batch size).
 constexpr int G4_ROWS = 20;  // 5 row blocks of 4
 constexpr int G4_NG = 16;    // site groups per block pair
-constexpr int G4_SPLIT = 2;  // CTAs per configuration
 __global__ void __launch_bounds__(256, 2) gram4_kernel(const void* __restrict__ psi, int N, long vol,
                                                   double* __restrict__ G) {
   extern __shared__ __align__(16) unsigned char gsm[];
   float2* tiles = reinterpret_cast<float2*>(gsm);  // [2][G4_ROWS][GT + 1]
   constexpr int TS = G4_ROWS * (GT + 1);
-  cg::cluster_group cluster = cg::this_cluster();
-  const int rank = (int)cluster.block_rank();
-  const long c = blockIdx.x / G4_SPLIT;
+  const long c = blockIdx.x;
   const float2* base = reinterpret_cast<const float2*>(psi) + (size_t)c * N * vol;
   const int nb = (N + 3) / 4, npairs = nb * (nb + 1) / 2;
   const int g = threadIdx.x % G4_NG, pair = threadIdx.x / G4_NG;
@@ -272,14 +261,12 @@ __global__ void __launch_bounds__(256, 2) gram4_kernel(const void* __restrict__ 
   for (int k = 0; k < 32; ++k) acc[k] = 0.0;
 #pragma unroll
   for (int k = 0; k < 16; ++k) s[k] = make_float2(0.f, 0.f);
-  constexpr long STEP = (long)G4_SPLIT * GT;  // this CTA's tiles: rank, rank + G4_SPLIT, ..
-  if ((long)rank * GT < vol) fill((long)rank * GT, tiles);
-  else asm volatile("cp.async.commit_group;" ::: "memory");
+  fill(0, tiles);
   int buf = 0, ntile = 0;
-  for (long p0 = (long)rank * GT; p0 < vol; p0 += STEP, buf ^= 1, ++ntile) {
+  for (long p0 = 0; p0 < vol; p0 += GT, buf ^= 1, ++ntile) {
     const float2* tile = tiles + buf * TS;
     __syncthreads();  // every thread is done with the tile the next copies overwrite
-    if (p0 + STEP < vol) fill(p0 + STEP, tiles + (buf ^ 1) * TS);
+    if (p0 + GT < vol) fill(p0 + GT, tiles + (buf ^ 1) * TS);
     else asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("cp.async.wait_group 1;" ::: "memory");
     __syncthreads();
@@ -306,7 +293,7 @@ __global__ void __launch_bounds__(256, 2) gram4_kernel(const void* __restrict__ 
           }
         }
       }
-      if ((ntile & 3) == 3 || p0 + STEP >= vol) {
+      if ((ntile & 3) == 3 || p0 + GT >= vol) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
           acc[2 * k] += (double)s[k].x;
@@ -316,26 +303,11 @@ __global__ void __launch_bounds__(256, 2) gram4_kernel(const void* __restrict__ 
       }
     }
   }
-  // sum the 16 site groups of a pair (adjacent lanes), then the cluster's
-  // CTAs in rank order, and write the upper triangle
+  // sum the 16 site groups of a pair (adjacent lanes) and write the upper triangle
 #pragma unroll
   for (int k = 0; k < 32; ++k)
     for (int o = G4_NG / 2; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-  asm volatile("cp.async.wait_all;" ::: "memory");
-  __syncthreads();  // every thread is done with the tiles; their memory holds the sums now
-  double* red = reinterpret_cast<double*>(gsm);  // [npairs][32]
   if (active && g == 0)
-#pragma unroll
-    for (int k = 0; k < 32; ++k) red[pair * 32 + k] = acc[k];
-  cluster.sync();  // every CTA's sums are in its shared memory
-  if (rank == 0 && active && g == 0) {
-    for (int r2 = 1; r2 < G4_SPLIT; ++r2) {
-      const double* peer = cluster.map_shared_rank(red, r2);
-#pragma unroll
-      for (int k = 0; k < 32; ++k) acc[k] += peer[pair * 32 + k];
-    }
-  }
-  if (rank == 0 && active && g == 0)
     for (int u = 0; u < 4; ++u)
       for (int v = 0; v < 4; ++v) {
         const int i = 4 * bi + u, j = 4 * bj + v;
@@ -344,7 +316,6 @@ __global__ void __launch_bounds__(256, 2) gram4_kernel(const void* __restrict__ 
         out[0] = acc[2 * (4 * u + v)];
         out[1] = acc[2 * (4 * u + v) + 1];
       }
-  cluster.sync();  // peers keep their shared memory until rank 0 has read it
 }
 
 // psi_{c,t}(p) <- sum_{i <= t} psi_{c,i}(p) Rinv[i][t]; one thread per site,
@@ -491,19 +462,7 @@ nrcps_status qr_reorthonormalise(nrcps_context* ctx, void* psi, int N, long vol,
     } else if (N <= G4_ROWS) {
       const size_t sh4 = sizeof(float2) * 2 * G4_ROWS * (GT + 1);
       cudaFuncSetAttribute(gram4_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh4);
-      cudaLaunchConfig_t cfg = {};
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = G4_SPLIT;
-      attr[0].val.clusterDim.y = 1;
-      attr[0].val.clusterDim.z = 1;
-      cfg.gridDim = dim3((unsigned)((long)nconf * G4_SPLIT));
-      cfg.blockDim = dim3(256);
-      cfg.dynamicSmemBytes = sh4;
-      cfg.stream = ctx->stream;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      NRCPS_TRY(check_cuda(ctx, cudaLaunchKernelEx(&cfg, gram4_kernel, psi, N, vol, G), "gram4_kernel launch"));
+      gram4_kernel<<<(unsigned)nconf, 256, sh4, ctx->stream>>>(psi, N, vol, G);
     } else {
       if (N <= 22) launch(gram_tile_kernel<float, 2, true>);
       else if (N <= 32) launch(gram_tile_kernel<float, 3, true>);

@@ -923,7 +923,9 @@ def cv_core(ctx, a, cv_train: int, cv_eval: int, cv_extra: int, cv_epochs: int):
     c = cv.cv_coefficient(C[-n_cal:].cpu(), torch.exp(net.predict_logC(X[-n_cal:])))
     del X, Xs
     # evaluation block: a seed never used for training
-    (Xe, Ce), t_eval = timed(lambda: cv.generate_pairs(L, T, ef, 2000, cv_eval, chunk=1024, G=G,
+    # (4096 configurations per ensemble run, as the batched workload; each
+    # configuration's determinants do not depend on the chunking)
+    (Xe, Ce), t_eval = timed(lambda: cv.generate_pairs(L, T, ef, 2000, cv_eval, chunk=4096, G=G,
                                                        precision=a.precision, qr_period=qr_period(a), ctx=ctx))
     ge, t_inf = timed(lambda: torch.exp(net.predict_logC(Xe)))
     gm, gm_err, t_extra = cv.extra_fields_mean_g(net, L, 3000, 0, cv_extra, chunk=8192, ctx=ctx)

@@ -928,7 +928,7 @@ def cv_core(ctx, a, cv_train: int, cv_eval: int, cv_extra: int, cv_epochs: int):
     (Xe, Ce), t_eval = timed(lambda: cv.generate_pairs(L, T, ef, 2000, cv_eval, chunk=4096, G=G,
                                                        precision=a.precision, qr_period=qr_period(a), ctx=ctx))
     ge, t_inf = timed(lambda: torch.exp(net.predict_logC(Xe)))
-    gm, gm_err, t_extra = cv.extra_fields_mean_g(net, L, 3000, 0, cv_extra, chunk=8192, ctx=ctx)
+    gm, gm_err, t_extra = cv.extra_fields_mean_g(net, L, 3000, 0, cv_extra, chunk=32768, ctx=ctx)
     Ce = Ce.cpu()
     plain, plain_err, est, est_err = cv.estimators(Ce, ge, c, gm, gm_err)
     var_ratio = (Ce - c * ge).var(0) / Ce.var(0)

@@ -1100,15 +1100,16 @@ struct AsyncShape {
   static constexpr int W = FW ? Base::S * L / 32 : 0;  // words per x-plane of the CTA's rows
   // FK 2 with FP32 orbitals: room for a real weight table's rows, copied in
   // 16-byte pieces (rows of whole pieces, planes on 4 floats, an aligned start)
-  static constexpr bool WT = FK == 2 && sizeof(R) == 4 && (Base::S * L) % 4 == 0 && L % 2 == 0 &&
+  static constexpr bool WT = (FK == 2 || FK == 3) && sizeof(R) == 4 && (Base::S * L) % 4 == 0 && L % 2 == 0 &&
                              (sizeof(cplx<R>) * Base::WORK + 32) % 16 == 0;
   static constexpr size_t EXTRA = WT ? (size_t)4 * Base::S * L * L : (size_t)(4 * L * W + 15) / 16 * 16;
   static constexpr size_t SMEM = PullShape<R, L, C, false>::SMEM + EXTRA;
 };
 
 // FK: 1 = compiled for Z2 fields only (with or without a position factor),
-// 2 = for every other field only; one instance per field class keeps the
-// other class's code, and its registers, out of the kernel.
+// 2 = for every other field, 3 = for a real FP32 weight table only (field
+// mode 3, FP32); one instance per field class keeps the other classes' code,
+// and its registers, out of the kernel.
 template <typename R, int L, int C, bool PK = false, int FK = 1>
 __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<R, L, C, false>::MIN_BLOCKS)
     fused_step_async_kernel(FusedArgs f) {
@@ -1315,11 +1316,16 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
           const bool up = (__ldg(words + xx * (L * L / 32)) >> bit) & 1u;
           x[xx] = scale_w_zpos<R, PK>(f.zpos, site0 + xx * L * L, up, x[xx]);
         }
-      } else if constexpr (FK == 2) {
+      } else if constexpr (FK == 2 || FK == 3) {
         if (AS::WT && wt) {
           // the weights of this thread's pencil, from the staged rows
 #pragma unroll
           for (int xx = 0; xx < L; ++xx) x[xx] = scale_w1<R, PK>(x[xx], (R)wbuf[xx * S * L + yl * L + z]);
+        } else if constexpr (FK == 3) {
+          // a table that cannot be staged: the same weights per site
+          const float* tab = reinterpret_cast<const float*>(f.field) + kb + site0;
+#pragma unroll
+          for (int xx = 0; xx < L; ++xx) x[xx] = scale_w1<R, PK>(x[xx], (R)__ldg(tab + xx * L * L));
         } else {
 #pragma unroll
           for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);
@@ -1417,6 +1423,12 @@ static nrcps_status launch_fused(nrcps_context* ctx, const FusedArgs& f, int cta
     const bool z2 = f.field_mode == 1 && (L * L) % 32 == 0 && (f.pos == nullptr || f.zpos != nullptr);
     kern = z2 ? fused_step_async_kernel<R, L, C, KIND == 12, 1> : fused_step_async_kernel<R, L, C, KIND == 12, 2>;
     if (!z2) SMEM = AsyncShape<R, L, C, 2>::SMEM;
+    if constexpr (sizeof(R) == 4) {
+      if (f.field_mode == 3) {  // (FP32 only: the host sends mode 3 with FP32 orbitals alone)
+        kern = fused_step_async_kernel<R, L, C, KIND == 12, 3>;
+        SMEM = AsyncShape<R, L, C, 3>::SMEM;
+      }
+    }
   }
   else kern = fused_step_kernel<R, L, C>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);

@@ -62,8 +62,10 @@ __device__ __forceinline__ cplx<R> apply_w_general(const FusedArgs& f, uint64_t 
   double wr, wi;
   const uint64_t k = kb + (uint64_t)site;
   if (sizeof(R) == 4 && f.field_mode == 3) {  // the site's weight, made once per run
-    const R w = (R)__ldg(reinterpret_cast<const float*>(f.field) + k);
-    return cplx<R>{x.re * w, x.im * w};
+    const float w = __ldg(reinterpret_cast<const float*>(f.field) + k);
+    // rounded products (never fused into a following add): every kind gives
+    // the same values
+    return cplx<R>{(R)__fmul_rn((float)x.re, w), (R)__fmul_rn((float)x.im, w)};
   }
   if (f.field_mode == 1) {
     uint32_t word = __ldg(reinterpret_cast<const uint32_t*>(f.field) + (k >> 5));
@@ -1318,14 +1320,21 @@ __global__ void __launch_bounds__(PullShape<R, L, C, false>::THREADS, PullShape<
         }
       } else if constexpr (FK == 2 || FK == 3) {
         if (AS::WT && wt) {
-          // the weights of this thread's pencil, from the staged rows
+          // the weights of this thread's pencil, from the staged rows (rounded
+          // products, as apply_w_general forms them)
 #pragma unroll
-          for (int xx = 0; xx < L; ++xx) x[xx] = scale_w1<R, PK>(x[xx], (R)wbuf[xx * S * L + yl * L + z]);
+          for (int xx = 0; xx < L; ++xx) {
+            const float w = wbuf[xx * S * L + yl * L + z];
+            x[xx] = cplx<R>{(R)__fmul_rn((float)x[xx].re, w), (R)__fmul_rn((float)x[xx].im, w)};
+          }
         } else if constexpr (FK == 3) {
           // a table that cannot be staged: the same weights per site
           const float* tab = reinterpret_cast<const float*>(f.field) + kb + site0;
 #pragma unroll
-          for (int xx = 0; xx < L; ++xx) x[xx] = scale_w1<R, PK>(x[xx], (R)__ldg(tab + xx * L * L));
+          for (int xx = 0; xx < L; ++xx) {
+            const float w = __ldg(tab + xx * L * L);
+            x[xx] = cplx<R>{(R)__fmul_rn((float)x[xx].re, w), (R)__fmul_rn((float)x[xx].im, w)};
+          }
         } else {
 #pragma unroll
           for (int xx = 0; xx < L; ++xx) x[xx] = apply_w_general<R>(f, kb, site0 + xx * L * L, x[xx]);

@@ -17,6 +17,12 @@
 // draw them running the jobs one after another: job j, configuration k,
 // slice t reads sites [base_j + (k T_j + t) V_j, ... + V_j) of the stream,
 // base_j = sum_{i<j} n_conf_i T_i V_i.  Each run continues the stream.
+// With FP32 orbitals a real Gaussian field reaches the fused step as one
+// FP32 weight (1 + a phi)/V per site, made once per run; such a batch draws
+// the next run's fields on a side stream while the current run's graph
+// executes, into the second of two weight buffers (one captured graph per
+// buffer), so the stream order and the results are those of drawing them
+// at the start of each run.
 #include <algorithm>
 #include <cmath>
 #include <vector>

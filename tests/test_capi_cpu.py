@@ -79,6 +79,21 @@ def test_headline_and_trapped_shape_tables_bit_exact(golden):
         assert np.array_equal(got[::stride], t["sources_sample"][n]), n
 
 
+@pytest.mark.parametrize("dims,wavefunc,cutoff", [((48, 48, 48), "TGND", 0.99999), ((32, 32, 32), "TGND", 2.0),
+                                                   ((8, 6, 4), "TGND", 0.99999), ((16, 16, 16), "PAIR1", 0.99999)])
+def test_two_body_tables_are_paired_and_even(dims, wavefunc, cutoff):
+    """The pair kernels' preconditions on TwoBody's tables (host-built, as the
+    ensemble and the branching driver check them): the opposite-site index is
+    an involution of the lattice, so sites pair up and each orbital element is
+    read once, and the weight is even under it, w(opp(i)) = w(i), so one set
+    of orbitals gives a symmetric pair matrix (the upper triangle suffices)."""
+    w, opp = nb.two_body_tables(dims, wavefunc, "STANDARD", 1.0, 0.176776695, cutoff)
+    vol = int(np.prod(dims))
+    assert opp.min() >= 0 and opp.max() < vol
+    assert np.array_equal(opp[opp], np.arange(vol))
+    assert np.array_equal(w[opp], w)
+
+
 def test_momenta_errors():
     with pytest.raises(nb.NrcpsError):
         nb.momenta((16, 16, 16), "PERFECT", 1.0, -1.0, 2.0)  # nothing below the Fermi level
